@@ -1,0 +1,405 @@
+"""granite_b200 -- B200-native CCZ4 RHS + SSP-RK3 stage update for GRANITE blocks.
+
+Python mirror of the reference operator interface
+(include/granite/spacetime/ccz4.hpp:49-115 of GRANITE) over the C ABI in
+include/granite_ccz4.h (libgranite_ccz4.so, CUDA sm_100a). There is no CPU
+path: every operator runs the CUDA library and raises if it cannot.
+
+    from granite_b200 import GridBlock, CCZ4Params, CCZ4Evolution
+    grid = GridBlock(0, 0, (32, 32, 32), (-10, -10, -10), (10, 10, 10), 4, 22)
+    rhs = GridBlock(1, 0, (32, 32, 32), (-10, -10, -10), (10, 10, 10), 4, 22)
+    set_flat_spacetime(grid)
+    CCZ4Evolution(CCZ4Params(ko_sigma=0.0)).computeRHSVacuum(grid, rhs)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import build as _build
+
+NUM_SPACETIME_VARS = 22
+
+GRANITE_OK = 0
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+BC_REFERENCE = 0
+BC_PERIODIC = 1
+AMR_REFERENCE = 0
+AMR_GHOSTS = 1
+KERNEL_STAGE, KERNEL_GHOST, KERNEL_TRANSFER, KERNEL_CONSTRAINTS = 0, 1, 2, 3
+
+_ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "no sm_100 device", -4: "out of memory",
+           -5: "non-finite state", -6: "unsupported", -7: "timeout"}
+
+
+class GraniteError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_ERRORS.get(code, 'error')} ({code}): {msg}")
+        self.code = code
+
+
+class _Params(C.Structure):
+    _fields_ = [("kappa1", C.c_double), ("kappa2", C.c_double), ("eta", C.c_double),
+                ("ko_sigma", C.c_double), ("chi_blend_center", C.c_double),
+                ("chi_blend_width", C.c_double), ("fd_order", C.c_int), ("device", C.c_int)]
+
+
+class _BlockDesc(C.Structure):
+    _fields_ = [("ncells", C.c_int * 3), ("nghost", C.c_int), ("lo", C.c_double * 3),
+                ("hi", C.c_double * 3), ("level", C.c_int), ("id", C.c_int)]
+
+
+_LIB = None
+
+
+def library_path() -> str:
+    return _build.LIB
+
+
+def load_library(build_if_missing: bool = True) -> C.CDLL:
+    """Load libgranite_ccz4.so (building it with nvcc if it is missing or stale)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if build_if_missing and not _build.up_to_date():
+        _build.build()
+    if not os.path.exists(_build.LIB):
+        raise GraniteError(-6, f"{_build.LIB} is missing: build it with granite_b200/build.py")
+    lib = C.CDLL(_build.LIB)
+    vp = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    lib.granite_ccz4_create.argtypes = [C.POINTER(_Params), C.POINTER(vp)]
+    lib.granite_ccz4_destroy.argtypes = [vp]
+    lib.granite_ccz4_last_error.argtypes = [vp, C.c_char_p, C.c_size_t]
+    lib.granite_ccz4_sync.argtypes = [vp]
+    lib.granite_ccz4_compute_rhs_host.argtypes = [vp, C.POINTER(_BlockDesc), dp, dp, dp, dp, dp, dp,
+                                                  C.c_int]
+    lib.granite_ccz4_apply_dissipation_host.argtypes = [vp, C.POINTER(_BlockDesc), dp, dp]
+    lib.granite_ccz4_compute_constraints_host.argtypes = [vp, C.POINTER(_BlockDesc), dp, dp, dp]
+    lib.granite_ccz4_compute_rhs_device.argtypes = [vp, C.POINTER(_BlockDesc), vp, vp, vp, vp, vp,
+                                                    vp, C.c_int, vp]
+    lib.granite_ccz4_add_block.argtypes = [vp, C.POINTER(_BlockDesc), C.POINTER(C.c_int)]
+    lib.granite_ccz4_commit.argtypes = [vp]
+    lib.granite_ccz4_num_blocks.argtypes = [vp]
+    lib.granite_ccz4_arena_bytes.argtypes = [vp, C.POINTER(C.c_size_t)]
+    lib.granite_ccz4_upload_block.argtypes = [vp, C.c_int, dp]
+    lib.granite_ccz4_download_block.argtypes = [vp, C.c_int, dp]
+    lib.granite_ccz4_rk3_step.argtypes = [vp, C.c_int, C.c_double, C.c_int, C.c_int]
+    lib.granite_ccz4_hierarchy_step.argtypes = [vp, C.c_double, C.c_int, C.c_int]
+    lib.granite_ccz4_constraint_norms.argtypes = [vp, C.c_int, dp, dp]
+    lib.granite_ccz4_nonfinite_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    lib.granite_ccz4_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    lib.granite_ccz4_default_params.argtypes = [C.POINTER(_Params)]
+    lib.granite_ccz4_default_params.restype = None
+    lib.granite_ccz4_set_profiling.argtypes = [vp, C.c_int]
+    lib.granite_ccz4_profile_reset.argtypes = [vp]
+    lib.granite_ccz4_profile_get.argtypes = [vp, C.c_int, dp, C.POINTER(C.c_longlong)]
+    lib.granite_ccz4_get_stream.argtypes = [vp, C.POINTER(vp)]
+    _LIB = lib
+    return lib
+
+
+def _dp(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+# ---------------------------------------------------------------------------
+# GridBlock (include/granite/core/grid.hpp:44-162)
+# ---------------------------------------------------------------------------
+
+class GridBlock:
+    """Field-major block storage with the reference GridBlock layout.
+
+    ``array`` is a float64 numpy array of shape (num_vars, nz+2g, ny+2g, nx+2g);
+    its flat buffer is exactly GridBlock::flatBuffer() (grid.hpp:109-116).
+    """
+
+    def __init__(self, id: int, level: int, ncells, lo, hi, nghost: int = 4,
+                 num_vars: int = NUM_SPACETIME_VARS):
+        self.id = int(id)
+        self.level = int(level)
+        self.ncells = tuple(int(n) for n in ncells)
+        self.lo = tuple(float(x) for x in lo)
+        self.hi = tuple(float(x) for x in hi)
+        self.nghost = int(nghost)
+        self.num_vars = int(num_vars)
+        self.dx_ = tuple((self.hi[d] - self.lo[d]) / self.ncells[d] for d in range(3))  # grid.cpp:20-22
+        g = 2 * self.nghost
+        nx, ny, nz = self.ncells
+        self.array = np.zeros((self.num_vars, nz + g, ny + g, nx + g), dtype=np.float64)
+
+    # accessors mirroring the reference
+    def getId(self):
+        return self.id
+
+    def getLevel(self):
+        return self.level
+
+    def getNumGhost(self):
+        return self.nghost
+
+    def getNumVars(self):
+        return self.num_vars
+
+    def totalCells(self, d):
+        return self.ncells[d] + 2 * self.nghost
+
+    def totalSize(self):
+        return self.totalCells(0) * self.totalCells(1) * self.totalCells(2)
+
+    def dx(self, d):
+        return self.dx_[d]
+
+    def x(self, d, idx):
+        return self.lo[d] + (float(idx) - self.nghost + 0.5) * self.dx_[d]
+
+    def istart(self, d=0):
+        return self.nghost
+
+    def iend(self, d):
+        return self.nghost + self.ncells[d]
+
+    def data(self, var, i, j, k):
+        return self.array[var, k, j, i]
+
+    def set(self, var, i, j, k, value):
+        self.array[var, k, j, i] = value
+
+    def flatBuffer(self):
+        return self.array.reshape(-1)
+
+    def numCells(self):
+        return self.ncells
+
+    def lowerCorner(self):
+        return self.lo
+
+    def upperCorner(self):
+        return self.hi
+
+    def desc(self) -> _BlockDesc:
+        d = _BlockDesc()
+        for a in range(3):
+            d.ncells[a] = self.ncells[a]
+            d.lo[a] = self.lo[a]
+            d.hi[a] = self.hi[a]
+        d.nghost = self.nghost
+        d.level = self.level
+        d.id = self.id
+        return d
+
+    def interior(self):
+        g = self.nghost
+        nx, ny, nz = self.ncells
+        return (slice(None), slice(g, g + nz), slice(g, g + ny), slice(g, g + nx))
+
+
+def block_desc(ncells, lo, hi, level=0, id=0, nghost=4) -> _BlockDesc:
+    return GridBlock(id, level, ncells, lo, hi, nghost, 1).desc()
+
+
+# ---------------------------------------------------------------------------
+# CCZ4Evolution (include/granite/spacetime/ccz4.hpp:49-115)
+# ---------------------------------------------------------------------------
+
+@dataclass
+class CCZ4Params:
+    """CCZ4Params, ccz4.hpp:25-34."""
+
+    kappa1: float = 0.02
+    kappa2: float = 0.0
+    eta: float = 2.0
+    ko_sigma: float = 0.1
+    fd_order: int = 4
+    use_moving_puncture: bool = True
+    chi_blend_center: float = 0.05
+    chi_blend_width: float = 0.02
+    device: int = 0
+
+    def _c(self) -> _Params:
+        return _Params(self.kappa1, self.kappa2, self.eta, self.ko_sigma, self.chi_blend_center,
+                       self.chi_blend_width, self.fd_order, self.device)
+
+
+class _Context:
+    def __init__(self, params: CCZ4Params):
+        self.lib = load_library()
+        self.h = C.c_void_p()
+        self._p = params._c()
+        rc = self.lib.granite_ccz4_create(C.byref(self._p), C.byref(self.h))
+        if rc != GRANITE_OK:
+            raise GraniteError(rc, "granite_ccz4_create failed (no usable sm_100 GPU?)")
+
+    def check(self, rc: int):
+        if rc != GRANITE_OK:
+            buf = C.create_string_buffer(512)
+            self.lib.granite_ccz4_last_error(self.h, buf, 512)
+            raise GraniteError(rc, buf.value.decode())
+
+    def close(self):
+        if self.h:
+            self.lib.granite_ccz4_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _f64(a):
+    a = np.asarray(a)
+    if a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise TypeError("expected a C-contiguous float64 array")
+    return a
+
+
+class CCZ4Evolution:
+    """GPU CCZ4 operator with the reference's method names and semantics."""
+
+    def __init__(self, params: CCZ4Params | None = None, precision: int = PRECISION_FP64):
+        self.params_ = params or CCZ4Params()
+        self.precision = precision
+        self.ctx = _Context(self.params_)
+
+    def params(self):
+        return self.params_
+
+    def computeRHS(self, grid: GridBlock, rhs: GridBlock, rho_matter, Si_matter, Sij_matter,
+                   S_trace):
+        """ccz4.hpp:69-74. Matter arrays: rho[N], Si[N,3], Sij[N,6], S[N] (N = totalSize)."""
+        N = grid.totalSize()
+        rho = _f64(np.ascontiguousarray(rho_matter, dtype=np.float64).reshape(N))
+        Si = _f64(np.ascontiguousarray(Si_matter, dtype=np.float64).reshape(N * 3))
+        Sij = _f64(np.ascontiguousarray(Sij_matter, dtype=np.float64).reshape(N * 6))
+        S = _f64(np.ascontiguousarray(S_trace, dtype=np.float64).reshape(N))
+        self.ctx.check(self.ctx.lib.granite_ccz4_compute_rhs_host(
+            self.ctx.h, C.byref(grid.desc()), _dp(grid.array), _dp(rhs.array), _dp(rho), _dp(Si),
+            _dp(Sij), _dp(S), self.precision))
+
+    def computeRHSVacuum(self, grid: GridBlock, rhs: GridBlock):
+        """ccz4.hpp:81."""
+        self.ctx.check(self.ctx.lib.granite_ccz4_compute_rhs_host(
+            self.ctx.h, C.byref(grid.desc()), _dp(grid.array), _dp(rhs.array), None, None, None,
+            None, self.precision))
+
+    def applyDissipation(self, grid: GridBlock, rhs: GridBlock):
+        """ccz4.hpp:99."""
+        self.ctx.check(self.ctx.lib.granite_ccz4_apply_dissipation_host(
+            self.ctx.h, C.byref(grid.desc()), _dp(grid.array), _dp(rhs.array)))
+
+    def computeConstraints(self, grid: GridBlock):
+        """ccz4.hpp:90-92. Returns (ham[N], mom[N,3]) over the whole block, ghosts zero."""
+        N = grid.totalSize()
+        ham = np.zeros(N, dtype=np.float64)
+        mom = np.zeros((N, 3), dtype=np.float64)
+        self.ctx.check(self.ctx.lib.granite_ccz4_compute_constraints_host(
+            self.ctx.h, C.byref(grid.desc()), _dp(grid.array), _dp(ham), _dp(mom)))
+        return ham, mom
+
+
+# ---------------------------------------------------------------------------
+# Resident hierarchy + RK3 driver (main.cpp TimeIntegrator, amr.cpp subcycle)
+# ---------------------------------------------------------------------------
+
+class Evolver:
+    """Device-resident blocks advanced by the fused RK3 step.
+
+    add blocks, commit(), upload(), then rk3_step(level, dt) / hierarchy_step(dt).
+    """
+
+    def __init__(self, params: CCZ4Params | None = None):
+        self.params = params or CCZ4Params()
+        self.ctx = _Context(self.params)
+        self.blocks: list[GridBlock] = []
+        self.committed = False
+
+    def add_block(self, b: GridBlock) -> int:
+        idx = C.c_int()
+        self.ctx.check(self.ctx.lib.granite_ccz4_add_block(self.ctx.h, C.byref(b.desc()),
+                                                           C.byref(idx)))
+        self.blocks.append(b)
+        return idx.value
+
+    def commit(self):
+        self.ctx.check(self.ctx.lib.granite_ccz4_commit(self.ctx.h))
+        self.committed = True
+
+    def arena_bytes(self) -> int:
+        n = C.c_size_t()
+        self.ctx.check(self.ctx.lib.granite_ccz4_arena_bytes(self.ctx.h, C.byref(n)))
+        return n.value
+
+    def upload(self, idx: int | None = None, array=None):
+        items = range(len(self.blocks)) if idx is None else [idx]
+        for i in items:
+            a = self.blocks[i].array if array is None else _f64(array)
+            self.ctx.check(self.ctx.lib.granite_ccz4_upload_block(self.ctx.h, i, _dp(a)))
+
+    def download(self, idx: int | None = None, out=None):
+        items = range(len(self.blocks)) if idx is None else [idx]
+        for i in items:
+            a = self.blocks[i].array if out is None else _f64(out)
+            self.ctx.check(self.ctx.lib.granite_ccz4_download_block(self.ctx.h, i, _dp(a)))
+
+    def rk3_step(self, level: int, dt: float, precision: int = PRECISION_FP64,
+                 bc: int = BC_REFERENCE):
+        self.ctx.check(self.ctx.lib.granite_ccz4_rk3_step(self.ctx.h, level, dt, precision, bc))
+
+    def hierarchy_step(self, dt_coarse: float, precision: int = PRECISION_FP64,
+                       amr_mode: int = AMR_REFERENCE):
+        self.ctx.check(self.ctx.lib.granite_ccz4_hierarchy_step(self.ctx.h, dt_coarse, precision,
+                                                                amr_mode))
+
+    def sync(self):
+        self.ctx.check(self.ctx.lib.granite_ccz4_sync(self.ctx.h))
+
+    def constraint_norms(self, level: int = -1):
+        h = C.c_double()
+        m = C.c_double()
+        self.ctx.check(self.ctx.lib.granite_ccz4_constraint_norms(self.ctx.h, level, C.byref(h),
+                                                                  C.byref(m)))
+        return h.value, m.value
+
+    def nonfinite_count(self) -> int:
+        n = C.c_longlong()
+        self.ctx.check(self.ctx.lib.granite_ccz4_nonfinite_count(self.ctx.h, C.byref(n)))
+        return n.value
+
+    def launch_count(self) -> int:
+        n = C.c_longlong()
+        self.ctx.check(self.ctx.lib.granite_ccz4_launch_count(self.ctx.h, C.byref(n)))
+        return n.value
+
+    def set_profiling(self, on: bool):
+        self.ctx.check(self.ctx.lib.granite_ccz4_set_profiling(self.ctx.h, int(bool(on))))
+
+    def profile_reset(self):
+        self.ctx.check(self.ctx.lib.granite_ccz4_profile_reset(self.ctx.h))
+
+    def profile(self, kernel_class: int):
+        """(total device ms, launches) of a kernel class since the last reset."""
+        ms = C.c_double()
+        n = C.c_longlong()
+        self.ctx.check(self.ctx.lib.granite_ccz4_profile_get(self.ctx.h, kernel_class,
+                                                             C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def stream_handle(self) -> int:
+        s = C.c_void_p()
+        self.ctx.check(self.ctx.lib.granite_ccz4_get_stream(self.ctx.h, C.byref(s)))
+        return s.value or 0
+
+    def close(self):
+        self.ctx.close()
+
+
+from .initial_data import (  # noqa: E402
+    brill_lindquist, gauge_wave, set_flat_spacetime, set_gauge_wave_data)

@@ -1,0 +1,75 @@
+// ccz4_common.cuh -- device-side data layout shared by the CCZ4 kernels.
+//
+// A block's fields use the reference GridBlock layout (grid.hpp:109-116):
+// field-major, x fastest, 22 fields of double, nghost = 4. Every block of the
+// hierarchy owns three such buffers in one device arena: the evolved state
+// (slot 0) and two RK stage buffers (slots 1, 2) that the three stages
+// ping-pong through, so no stage reads a buffer that the same launch writes.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace granite_b200 {
+
+constexpr int NV = 22;
+constexpr int NG = 4;
+
+// SpacetimeVar order, types.hpp:104-130
+enum Var : int {
+    CHI = 0, GXX, GXY, GXZ, GYY, GYZ, GZZ, AXX, AXY, AXZ, AYY, AYZ, AZZ,
+    KTR, GHX, GHY, GHZ, THETA, ALPHA, BETAX, BETAY, BETAZ
+};
+
+// Block descriptor as the kernels see it (one per block, in device memory).
+struct DevBlock {
+    double* buf[3];      // state, stage A, stage B (slot 0/1/2)
+    int n[3];            // interior cells
+    int tx, ty, tz;      // cells incl. ghosts
+    long long stride;    // cells per field
+    double lo[3];
+    double dx[3];
+    double inv12h[3];    // 1/(12 dx)      first derivative (ccz4.cpp:72)
+    double inv12h2[3];   // 1/(12 dx^2)    second derivative (ccz4.cpp:158)
+    double inv4hh[3];    // 1/(4 dx_a dx_b) mixed (xy, xz, yz) (ccz4.cpp:188)
+    double kocf[3];      // sigma/(64 dx)  KO (ccz4.cpp:886-887)
+    int level;
+    int pad_;
+};
+
+// One unit of the batched work-list: a tile of interior points of a block.
+struct Tile {
+    int block;
+    int i0, j0, k0;  // interior-relative origin of the tile
+};
+
+// Arguments of one fused RHS launch.
+struct StageArgs {
+    int in_sel;      // buffer slot the stencils read
+    int n_sel;       // slot of u^n (pointwise, RK combine)
+    int out_sel;     // slot written
+    int final_stage; // 1: apply the algebraic constraints after the floors
+    double a1, a2, a3dt;  // out = a1 u^n + a2 u_in + a3dt L(u_in)
+    int ko_on;       // ko_sigma > 0
+    double chi_c, chi_w, kappa1, kappa2, eta;
+    // standalone RHS output (EPI_STORE): rhs base per block is given by rhs_ptr
+    double* rhs;     // single-block RHS destination (EPI_STORE only)
+    const double* rho; const double* Si; const double* Sij; const double* S;  // matter (nullable)
+    unsigned long long* nonfinite;  // floor hits on non-finite chi/alpha (nullable)
+};
+
+__host__ __device__ inline long long cell_index(const DevBlock& b, int i, int j, int k) {
+    return (long long)i + (long long)b.tx * ((long long)j + (long long)b.ty * k);
+}
+
+// Cell-centre coordinate without FMA contraction, grid.hpp:92-94.
+__device__ inline double coord(const DevBlock& b, int d, int idx) {
+    return __dadd_rn(b.lo[d], __dmul_rn(__dadd_rn((double)(idx - NG), 0.5), b.dx[d]));
+}
+
+// Asymptotic value of the 1/r falloff, main.cpp:382-394.
+__host__ __device__ inline double f_inf(int v) {
+    return (v == CHI || v == GXX || v == GYY || v == GZZ || v == ALPHA) ? 1.0 : 0.0;
+}
+
+}  // namespace granite_b200

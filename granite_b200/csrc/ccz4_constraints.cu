@@ -1,0 +1,261 @@
+// ccz4_constraints.cu -- Hamiltonian / momentum constraint monitor (FP64).
+//
+// CCZ4Evolution::computeConstraints (ccz4.cpp:941-1159): H = R + 2/3 K^2 -
+// A_ij A^ij (vacuum), M_i = gtu^{jk} D_j A_ki - 3/(2 chi) A_ij gtu^{jk} d_k chi
+// - 2/3 d_i K. chi is not clamped here (ccz4.cpp:963). The norms of
+// main.cpp:1216-1254 are sqrt(sum H^2 / N) over interior points; each CTA
+// writes its partial sums, and a single-CTA kernel adds the partials in a
+// fixed order, so the result does not depend on scheduling.
+#include "ccz4_common.cuh"
+#include "ccz4_kernels.h"
+#include "ccz4_stencil.cuh"
+
+namespace granite_b200 {
+
+namespace {
+
+__device__ void constraint_point(const DevBlock& B, const double* __restrict__ u, long long c, double& H,
+                                 double M[3]) {
+    using P = double;
+    const long long st = B.stride;
+    const double* __restrict__ uc = u + c;
+#define FP(v) (uc + (long long)(v) * st)
+    const double chi = __ldg(FP(CHI));
+    const double K = __ldg(FP(KTR));
+    double gt[6], At[6], Gh[3], gtu[6];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+        gt[a] = __ldg(FP(GXX + a));
+        At[a] = __ldg(FP(AXX + a));
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) Gh[a] = __ldg(FP(GHX + a));
+    {
+        const double det = gt[0] * (gt[3] * gt[5] - gt[4] * gt[4]) - gt[1] * (gt[1] * gt[5] - gt[4] * gt[2]) +
+            gt[2] * (gt[1] * gt[4] - gt[3] * gt[2]);
+        const double inv = 1.0 / (det + 1.0e-30);
+        gtu[0] = (gt[3] * gt[5] - gt[4] * gt[4]) * inv;
+        gtu[1] = (gt[2] * gt[4] - gt[1] * gt[5]) * inv;
+        gtu[2] = (gt[1] * gt[4] - gt[2] * gt[3]) * inv;
+        gtu[3] = (gt[0] * gt[5] - gt[2] * gt[2]) * inv;
+        gtu[4] = (gt[1] * gt[2] - gt[0] * gt[4]) * inv;
+        gtu[5] = (gt[0] * gt[3] - gt[1] * gt[1]) * inv;
+    }
+    const double beta0[3] = {0.0, 0.0, 0.0};
+    double dg[6][3], Rt[6];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+        FieldDer<P> fd = field_der<P, true>(B, FP(GXX + a), beta0, 0.0, false);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) dg[a][d] = fd.d[d];
+        Rt[a] = -0.5 * (gtu[0] * fd.h[0] + gtu[3] * fd.h[3] + gtu[5] * fd.h[5] +
+                        2.0 * (gtu[1] * fd.h[1] + gtu[2] * fd.h[2] + gtu[4] * fd.h[4]));
+    }
+    double G1[3][6], ch[3][6], Gc[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = i; j < 3; ++j)
+                G1[k][sy(i, j)] = 0.5 * (dg[sy(k, j)][i] + dg[sy(k, i)][j] - dg[sy(i, j)][k]);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int jk = 0; jk < 6; ++jk)
+            ch[i][jk] = gtu[sy(i, 0)] * G1[0][jk] + gtu[sy(i, 1)] * G1[1][jk] + gtu[sy(i, 2)] * G1[2][jk];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        Gc[k] = gtu[0] * ch[k][0] + gtu[3] * ch[k][3] + gtu[5] * ch[k][5] +
+            2.0 * (gtu[1] * ch[k][1] + gtu[2] * ch[k][2] + gtu[4] * ch[k][4]);
+    double dGh[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        FieldDer<P> fd = field_der<P, false>(B, FP(GHX + a), beta0, 0.0, false);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) dGh[a][d] = fd.d[d];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = i; j < 3; ++j) {
+            double t2 = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) t2 += gt[sy(k, i)] * dGh[k][j] + gt[sy(k, j)] * dGh[k][i];
+            Rt[sy(i, j)] += 0.5 * t2 + (Gh[0] - Gc[0]) * G1[0][sy(i, j)] + (Gh[1] - Gc[1]) * G1[1][sy(i, j)] +
+                (Gh[2] - Gc[2]) * G1[2][sy(i, j)];
+        }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double Gu[3][3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int l = 0; l < 3; ++l)
+                Gu[j][l] = gtu[sy(l, 0)] * G1[k][sy(j, 0)] + gtu[sy(l, 1)] * G1[k][sy(j, 1)] +
+                    gtu[sy(l, 2)] * G1[k][sy(j, 2)];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = i; j < 3; ++j) {
+                double t = 0.0;
+#pragma unroll
+                for (int l = 0; l < 3; ++l) t += ch[k][sy(l, i)] * Gu[j][l] + ch[k][sy(l, j)] * Gu[i][l];
+                Rt[sy(i, j)] += t;
+            }
+    }
+    FieldDer<P> fchi = field_der<P, true>(B, FP(CHI), beta0, 0.0, false);
+    const double c_half = 0.5 / (chi + 1e-30), c_quart = 0.25 / ((chi * chi) + 1e-30);
+    double DDchi[6];
+#pragma unroll
+    for (int ij = 0; ij < 6; ++ij)
+        DDchi[ij] = fchi.h[ij] - (ch[0][ij] * fchi.d[0] + ch[1][ij] * fchi.d[1] + ch[2][ij] * fchi.d[2]);
+    const double lapchi = gtu[0] * DDchi[0] + gtu[3] * DDchi[3] + gtu[5] * DDchi[5] +
+        2.0 * (gtu[1] * DDchi[1] + gtu[2] * DDchi[2] + gtu[4] * DDchi[4]);
+    double dchi2 = 0.0;
+#pragma unroll
+    for (int l = 0; l < 3; ++l)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) dchi2 += gtu[sy(l, m)] * fchi.d[l] * fchi.d[m];
+    double Rs = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int ij = sy(i, j);
+            const double rchi = c_half * (DDchi[ij] + gt[ij] * lapchi) -
+                c_quart * (fchi.d[i] * fchi.d[j] - 3.0 * gt[ij] * dchi2);
+            Rs += gtu[ij] * (Rt[ij] + rchi);
+        }
+    Rs *= chi;
+    double Am[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            Am[i][j] = gtu[sy(i, 0)] * At[sy(0, j)] + gtu[sy(i, 1)] * At[sy(1, j)] + gtu[sy(i, 2)] * At[sy(2, j)];
+    double AtAt = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) AtAt += Am[i][j] * Am[j][i];
+    H = Rs + (2.0 / 3.0) * K * K - AtAt;  // ccz4.cpp:1127 with rho = 0
+
+    // momentum constraint, ccz4.cpp:1138-1155
+    double dA[6][3], dK[3];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+        FieldDer<P> fd = field_der<P, false>(B, FP(AXX + a), beta0, 0.0, false);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) dA[a][d] = fd.d[d];
+    }
+    {
+        FieldDer<P> fd = field_der<P, false>(B, FP(KTR), beta0, 0.0, false);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) dK[d] = fd.d[d];
+    }
+    const double c3 = 3.0 / (2.0 * chi + 1e-30);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        double Mi = 0.0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double g_jk = gtu[sy(j, k)];
+                double DA = dA[sy(k, i)][j];
+#pragma unroll
+                for (int m = 0; m < 3; ++m) DA -= ch[m][sy(j, k)] * At[sy(m, i)] + ch[m][sy(j, i)] * At[sy(k, m)];
+                Mi += g_jk * DA - c3 * At[sy(i, j)] * g_jk * fchi.d[k];
+            }
+        M[i] = Mi - (2.0 / 3.0) * dK[i];
+    }
+#undef FP
+}
+
+constexpr int CT_X = 32, CT_Y = 4;
+
+__global__ void __launch_bounds__(CT_X* CT_Y)
+    constraints_kernel(const DevBlock* __restrict__ blocks, const Tile* __restrict__ tiles, int sel,
+                       double* __restrict__ ham, double* __restrict__ mom, double* __restrict__ partials) {
+    const Tile t = tiles[blockIdx.x];
+    const DevBlock& B = blocks[t.block];
+    const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y, k = t.k0 + threadIdx.z;
+    double h2 = 0.0, m2 = 0.0;
+    if (i < B.n[0] && j < B.n[1] && k < B.n[2]) {
+        const long long c = cell_index(B, i + NG, j + NG, k + NG);
+        double H, M[3];
+        constraint_point(B, B.buf[sel], c, H, M);
+        if (ham) ham[c] = H;
+        if (mom) {
+            mom[3 * c] = M[0];
+            mom[3 * c + 1] = M[1];
+            mom[3 * c + 2] = M[2];
+        }
+        h2 = H * H;
+        m2 = M[0] * M[0] + M[1] * M[1] + M[2] * M[2];
+    }
+    if (!partials) return;
+    // fixed-shape CTA reduction (warp shuffles, then smem across warps)
+    for (int o = 16; o > 0; o >>= 1) {
+        h2 += __shfl_down_sync(0xffffffffu, h2, o);
+        m2 += __shfl_down_sync(0xffffffffu, m2, o);
+    }
+    __shared__ double sh[2][CT_X * CT_Y / 32];
+    const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+    const int warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
+    if (lane == 0) {
+        sh[0][warp] = h2;
+        sh[1][warp] = m2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < CT_X * CT_Y / 32; ++w) {
+            a += sh[0][w];
+            b += sh[1][w];
+        }
+        partials[2 * blockIdx.x] = a;
+        partials[2 * blockIdx.x + 1] = b;
+    }
+}
+
+// One CTA; thread t sums partials t, t+T, ... in order, then a fixed tree.
+__global__ void sum_partials_kernel(const double* __restrict__ p, int n, double* out) {
+    __shared__ double sa[256], sb[256];
+    double a = 0.0, b = 0.0;
+    for (int x = threadIdx.x; x < n; x += blockDim.x) {
+        a += p[2 * x];
+        b += p[2 * x + 1];
+    }
+    sa[threadIdx.x] = a;
+    sb[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            sa[threadIdx.x] += sa[threadIdx.x + s];
+            sb[threadIdx.x] += sb[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = sa[0];
+        out[1] = sb[0];
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_constraints(const DevBlock* blocks, const Tile* tiles, int ntiles, int sel, double* ham,
+                               double* mom, double* partials, cudaStream_t stream) {
+    if (ntiles <= 0) return cudaSuccess;
+    constraints_kernel<<<ntiles, dim3(CT_X, CT_Y, 1), 0, stream>>>(blocks, tiles, sel, ham, mom, partials);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sum_partials(const double* partials, int n, double* out, cudaStream_t stream) {
+    sum_partials_kernel<<<1, 256, 0, stream>>>(partials, n, out);
+    return cudaGetLastError();
+}
+
+}  // namespace granite_b200

@@ -1,0 +1,242 @@
+// ccz4_ghost.cu -- ghost-cell fills and inter-level transfers.
+//
+// All arithmetic here uses explicitly rounded intrinsics (no FMA contraction)
+// so the fills reproduce the reference host loops bit for bit:
+//   zero-gradient level fill   amr.cpp:447-480
+//   1/r outer falloff          main.cpp:351-463 (x faces, then y, then z)
+//   trilinear prolongation     amr.cpp:484-564
+//   2x2x2 restriction          amr.cpp:566-626
+// The work is described by host-built item lists (ghost-cell chunks,
+// prolongation / restriction / copy cells), so one launch serves every block
+// of a level whatever its size.
+#include "ccz4_common.cuh"
+#include "ccz4_kernels.h"
+
+namespace granite_b200 {
+
+namespace {
+
+__device__ __forceinline__ int clampi(int a, int lo, int hi) { return a < lo ? lo : (a > hi ? hi : a); }
+
+__device__ __forceinline__ double sq3(double a, double b, double c) {
+    // sqrt(a*a + b*b + c*c) + 1e-30, left-to-right, no contraction
+    return __dadd_rn(__dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), __dmul_rn(c, c))), 1e-30);
+}
+
+// finf + (f_int - finf) * r_int / r_gh
+__device__ __forceinline__ double falloff(double finf, double fint, double ri, double rg) {
+    return __dadd_rn(finf, __ddiv_rn(__dmul_rn(__dsub_rn(fint, finf), ri), rg));
+}
+
+__device__ __forceinline__ bool inside(int a, int n) { return a >= NG && a < NG + n; }
+
+// Value the reference's three passes leave in ghost cell (i,j,k): the last
+// pass that writes the cell wins, and each pass reads the value the earlier
+// passes left in the cell it copies from (main.cpp:395-463).
+__device__ double sommerfeld_value(const DevBlock& B, const double* __restrict__ f, double fi, int i, int j, int k) {
+    auto valX = [&](int a, int b, int c) -> double {  // after the x pass; b, c interior
+        if (inside(a, B.n[0])) return __ldg(f + cell_index(B, a, b, c));
+        const int ac = clampi(a, NG, NG + B.n[0] - 1);
+        const double y = coord(B, 1, b), z = coord(B, 2, c);
+        const double ri = sq3(coord(B, 0, ac), y, z), rg = sq3(coord(B, 0, a), y, z);
+        return falloff(fi, __ldg(f + cell_index(B, ac, b, c)), ri, rg);
+    };
+    auto valXY = [&](int a, int b, int c) -> double {  // after the y pass; c interior
+        if (inside(b, B.n[1])) return valX(a, b, c);
+        const int bc = clampi(b, NG, NG + B.n[1] - 1);
+        const double x = coord(B, 0, a), z = coord(B, 2, c);
+        const double ri = sq3(x, coord(B, 1, bc), z), rg = sq3(x, coord(B, 1, b), z);
+        return falloff(fi, valX(a, bc, c), ri, rg);
+    };
+    if (inside(k, B.n[2])) return valXY(i, j, k);
+    const int kc = clampi(k, NG, NG + B.n[2] - 1);
+    const double x = coord(B, 0, i), y = coord(B, 1, j);
+    const double ri = sq3(x, y, coord(B, 2, kc)), rg = sq3(x, y, coord(B, 2, k));
+    return falloff(fi, valXY(i, j, kc), ri, rg);
+}
+
+// k-th ghost cell of a block: z slabs first, then y slabs, then x slabs.
+__device__ __forceinline__ bool ghost_coords(const DevBlock& B, long long r, int& i, int& j, int& k) {
+    const int T0 = B.tx, T1 = B.ty;
+    const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
+    const long long A = (long long)T0 * T1 * (2 * NG);
+    if (r < A) {
+        const int kk = (int)(r / ((long long)T0 * T1));
+        const long long rem = r % ((long long)T0 * T1);
+        k = kk < NG ? kk : kk + n2;
+        j = (int)(rem / T0);
+        i = (int)(rem % T0);
+        return true;
+    }
+    r -= A;
+    const long long Bc = (long long)T0 * (2 * NG) * n2;
+    if (r < Bc) {
+        k = NG + (int)(r / ((long long)T0 * 2 * NG));
+        const long long rem = r % ((long long)T0 * 2 * NG);
+        const int jj = (int)(rem / T0);
+        j = jj < NG ? jj : jj + n1;
+        i = (int)(rem % T0);
+        return true;
+    }
+    r -= Bc;
+    const long long Cc = (long long)(2 * NG) * n1 * n2;
+    if (r < Cc) {
+        k = NG + (int)(r / ((long long)2 * NG * n1));
+        const long long rem = r % ((long long)2 * NG * n1);
+        j = NG + (int)(rem / (2 * NG));
+        const int ii = (int)(rem % (2 * NG));
+        i = ii < NG ? ii : ii + n0;
+        return true;
+    }
+    return false;
+}
+
+// items[x].cell holds the first ghost rank of a chunk of blockDim.x ranks.
+__global__ void ghost_fill_kernel(int mode, const DevBlock* __restrict__ blocks, const GhostItem* __restrict__ items,
+                                  int sel) {
+    const GhostItem it = items[blockIdx.x];
+    const DevBlock& B = blocks[it.block];
+    int i, j, k;
+    if (!ghost_coords(B, (long long)it.cell + threadIdx.x, i, j, k)) return;
+    double* base = B.buf[sel];
+    const long long c = cell_index(B, i, j, k);
+    if (mode == GHOST_SOMMERFELD) {
+        for (int v = 0; v < NV; ++v) {
+            const double* f = base + (long long)v * B.stride;
+            base[(long long)v * B.stride + c] = sommerfeld_value(B, f, f_inf(v), i, j, k);
+        }
+        return;
+    }
+    int si, sj, sk;
+    if (mode == GHOST_ZERO_GRADIENT) {
+        si = clampi(i, NG, NG + B.n[0] - 1);
+        sj = clampi(j, NG, NG + B.n[1] - 1);
+        sk = clampi(k, NG, NG + B.n[2] - 1);
+    } else {  // periodic
+        si = i < NG ? i + B.n[0] : (i >= NG + B.n[0] ? i - B.n[0] : i);
+        sj = j < NG ? j + B.n[1] : (j >= NG + B.n[1] ? j - B.n[1] : j);
+        sk = k < NG ? k + B.n[2] : (k >= NG + B.n[2] ? k - B.n[2] : k);
+    }
+    const long long s = cell_index(B, si, sj, sk);
+    for (int v = 0; v < NV; ++v) base[(long long)v * B.stride + c] = base[(long long)v * B.stride + s];
+}
+
+__global__ void prolong_kernel(const DevBlock* __restrict__ blocks, const ProlongItem* __restrict__ items, int n,
+                               int sel) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const ProlongItem it = items[t];
+    const DevBlock& F = blocks[it.fine_block];
+    const DevBlock& C = blocks[it.coarse_block];
+    const int i = it.cell % F.tx;
+    const int j = (it.cell / F.tx) % F.ty;
+    const int k = it.cell / (F.tx * F.ty);
+    const int fi[3] = {i, j, k};
+    const int ct[3] = {C.tx, C.ty, C.tz};
+    int c0[3], c1[3];
+    double ax[3];
+    for (int d = 0; d < 3; ++d) {
+        // (x - coarse.x(d, istart)) / coarse.dx + istart  (amr.cpp:502-507)
+        const double f = __dadd_rn(__ddiv_rn(__dsub_rn(coord(F, d, fi[d]), coord(C, d, NG)), C.dx[d]), (double)NG);
+        int a = (int)round(f);
+        a = a > ct[d] - 1 ? ct[d] - 1 : a;
+        a = a < 0 ? 0 : a;
+        const double fr = __dsub_rn(f, (double)a);
+        int b = a + (fr >= 0.0 ? 1 : -1);
+        b = b > ct[d] - 1 ? ct[d] - 1 : b;
+        b = b < 0 ? 0 : b;
+        c0[d] = a;
+        c1[d] = b;
+        ax[d] = fabs(fr);
+    }
+    const double bx = __dsub_rn(1.0, ax[0]), by = __dsub_rn(1.0, ax[1]), bz = __dsub_rn(1.0, ax[2]);
+    const double w000 = __dmul_rn(__dmul_rn(bx, by), bz);
+    const double w100 = __dmul_rn(__dmul_rn(ax[0], by), bz);
+    const double w010 = __dmul_rn(__dmul_rn(bx, ax[1]), bz);
+    const double w001 = __dmul_rn(__dmul_rn(bx, by), ax[2]);
+    const double w110 = __dmul_rn(__dmul_rn(ax[0], ax[1]), bz);
+    const double w101 = __dmul_rn(__dmul_rn(ax[0], by), ax[2]);
+    const double w011 = __dmul_rn(__dmul_rn(bx, ax[1]), ax[2]);
+    const double w111 = __dmul_rn(__dmul_rn(ax[0], ax[1]), ax[2]);
+    const long long o000 = cell_index(C, c0[0], c0[1], c0[2]), o100 = cell_index(C, c1[0], c0[1], c0[2]);
+    const long long o010 = cell_index(C, c0[0], c1[1], c0[2]), o001 = cell_index(C, c0[0], c0[1], c1[2]);
+    const long long o110 = cell_index(C, c1[0], c1[1], c0[2]), o101 = cell_index(C, c1[0], c0[1], c1[2]);
+    const long long o011 = cell_index(C, c0[0], c1[1], c1[2]), o111 = cell_index(C, c1[0], c1[1], c1[2]);
+    const double* cb = C.buf[sel];
+    double* fb = F.buf[sel];
+    for (int v = 0; v < NV; ++v) {
+        const double* q = cb + (long long)v * C.stride;
+        double val = __dmul_rn(w000, __ldg(q + o000));
+        val = __dadd_rn(val, __dmul_rn(w100, __ldg(q + o100)));
+        val = __dadd_rn(val, __dmul_rn(w010, __ldg(q + o010)));
+        val = __dadd_rn(val, __dmul_rn(w001, __ldg(q + o001)));
+        val = __dadd_rn(val, __dmul_rn(w110, __ldg(q + o110)));
+        val = __dadd_rn(val, __dmul_rn(w101, __ldg(q + o101)));
+        val = __dadd_rn(val, __dmul_rn(w011, __ldg(q + o011)));
+        val = __dadd_rn(val, __dmul_rn(w111, __ldg(q + o111)));
+        fb[(long long)v * F.stride + it.cell] = val;
+    }
+}
+
+__global__ void restrict_kernel(const DevBlock* __restrict__ blocks, const RestrictItem* __restrict__ items, int n,
+                                int sel) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const RestrictItem it = items[t];
+    const DevBlock& F = blocks[it.fine_block];
+    const DevBlock& C = blocks[it.coarse_block];
+    const long long sx = 1, sy_ = F.tx, sz = (long long)F.tx * F.ty;
+    const double* fb = F.buf[sel];
+    double* cb = C.buf[sel];
+    for (int v = 0; v < NV; ++v) {
+        const double* q = fb + (long long)v * F.stride + it.fine_base;
+        double s = 0.0;
+        for (int rk = 0; rk < 2; ++rk)
+            for (int rj = 0; rj < 2; ++rj)
+                for (int ri = 0; ri < 2; ++ri) s = __dadd_rn(s, __ldg(q + ri * sx + rj * sy_ + rk * sz));
+        cb[(long long)v * C.stride + it.cell] = __ddiv_rn(s, 8.0);
+    }
+}
+
+__global__ void copy_kernel(const DevBlock* __restrict__ blocks, const CopyItem* __restrict__ items, int n, int sel) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const CopyItem it = items[t];
+    const DevBlock& D = blocks[it.dst_block];
+    const DevBlock& S = blocks[it.src_block];
+    for (int v = 0; v < NV; ++v)
+        D.buf[sel][(long long)v * D.stride + it.dst_cell] = S.buf[sel][(long long)v * S.stride + it.src_cell];
+}
+
+}  // namespace
+
+constexpr int GHOST_CHUNK = 256;
+
+cudaError_t launch_ghost_fill(int mode, const DevBlock* blocks, const GhostItem* items, int nitems, int sel,
+                              cudaStream_t stream) {
+    if (nitems <= 0) return cudaSuccess;
+    ghost_fill_kernel<<<nitems, GHOST_CHUNK, 0, stream>>>(mode, blocks, items, sel);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prolong(const DevBlock* blocks, const ProlongItem* items, int nitems, int sel,
+                           cudaStream_t stream) {
+    if (nitems <= 0) return cudaSuccess;
+    prolong_kernel<<<(nitems + 255) / 256, 256, 0, stream>>>(blocks, items, nitems, sel);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_restrict(const DevBlock* blocks, const RestrictItem* items, int nitems, int sel,
+                            cudaStream_t stream) {
+    if (nitems <= 0) return cudaSuccess;
+    restrict_kernel<<<(nitems + 255) / 256, 256, 0, stream>>>(blocks, items, nitems, sel);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_copy(const DevBlock* blocks, const CopyItem* items, int nitems, int sel, cudaStream_t stream) {
+    if (nitems <= 0) return cudaSuccess;
+    copy_kernel<<<(nitems + 255) / 256, 256, 0, stream>>>(blocks, items, nitems, sel);
+    return cudaGetLastError();
+}
+
+}  // namespace granite_b200

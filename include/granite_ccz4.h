@@ -1,0 +1,211 @@
+/*
+ * granite_ccz4.h -- C ABI of the B200-native CCZ4 right-hand side and SSP-RK3
+ * stage update (libgranite_ccz4.so, CUDA sm_100a).
+ *
+ * Drop-in boundary for GRANITE's spacetime operator and RK3 driver. Every
+ * entry point below names the reference interface it replaces (paths inside
+ * the GRANITE tree). Field data always uses the reference GridBlock layout
+ * (include/granite/core/grid.hpp:109-116):
+ *
+ *   buf[v * stride + i + tx * (j + ty * k)],   tx = nx + 2 ng,  ty = ny + 2 ng,
+ *   stride = tx * ty * (nz + 2 ng),  v in SpacetimeVar order
+ *   (include/granite/core/types.hpp:104-130), 22 fields of double.
+ *
+ * so GridBlock::flatBuffer() can be passed unchanged.
+ *
+ * Conventions
+ *   - Every function returns an int status: GRANITE_OK (0) or a negative
+ *     GRANITE_ERR_* code; nothing aborts or traps. The message of the last
+ *     failure on a context is available from granite_ccz4_last_error().
+ *   - A context owns one CUDA device, one CUDA stream and all device memory it
+ *     allocates. A context is not re-entrant: call it from one host thread at
+ *     a time (the reference operator is const and re-entrant on the host; a
+ *     caller that needs concurrency creates one context per thread).
+ *   - "_host" entry points take host pointers and block until results are in
+ *     host memory. Resident-block entry points enqueue work on the context's
+ *     stream; granite_ccz4_sync() waits for it.
+ *   - There is no CPU fallback: without a usable sm_100 device,
+ *     granite_ccz4_create() fails with GRANITE_ERR_NO_DEVICE.
+ */
+#ifndef GRANITE_CCZ4_H
+#define GRANITE_CCZ4_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define GRANITE_API __attribute__((visibility("default")))
+#else
+#define GRANITE_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GRANITE_CCZ4_NUM_VARS 22
+#define GRANITE_CCZ4_ABI_VERSION 1
+
+/* status codes */
+#define GRANITE_OK 0
+#define GRANITE_ERR_INVALID (-1)     /* bad argument, size or state */
+#define GRANITE_ERR_CUDA (-2)        /* CUDA runtime error (message has the detail) */
+#define GRANITE_ERR_NO_DEVICE (-3)   /* no sm_100 device / driver */
+#define GRANITE_ERR_NOMEM (-4)       /* device or pinned allocation failed */
+#define GRANITE_ERR_NONFINITE (-5)   /* non-finite values detected in the evolved state */
+#define GRANITE_ERR_UNSUPPORTED (-6) /* option the library does not implement */
+#define GRANITE_ERR_TIMEOUT (-7)     /* a bounded host-side wait gave up */
+
+/* arithmetic of the RHS algebra */
+#define GRANITE_PRECISION_FP64 0  /* plain FP64 throughout */
+#define GRANITE_PRECISION_MIXED 1 /* FP32 algebra from FP64 stencil differences;
+                                     FP64 state, RK3 accumulation, chi, inverse metric */
+
+/* boundary treatment of a single-level (level-0) step */
+#define GRANITE_BC_REFERENCE 0 /* zero-gradient level fill (amr.cpp:400-482) before and after
+                                  the step, 1/r falloff on every stage buffer (main.cpp:351-521) */
+#define GRANITE_BC_PERIODIC 1  /* periodic wrap everywhere (gauge-wave test; the reference has
+                                  no periodic boundary) */
+
+/* Berger-Oliger inter-level semantics of granite_ccz4_hierarchy_step */
+#define GRANITE_AMR_REFERENCE 0  /* prolongate coarse data into ALL cells of a fine block before
+                                    and after each fine step, as amr.cpp:313-318,438 do */
+#define GRANITE_AMR_GHOSTS 1     /* prolongate into fine ghost cells only; same-level
+                                    neighbours copy ghosts from each other */
+
+/* CCZ4Params, include/granite/spacetime/ccz4.hpp:25-34 */
+typedef struct {
+    double kappa1;           /* 0.02 */
+    double kappa2;           /* 0.0 */
+    double eta;              /* 2.0 */
+    double ko_sigma;         /* 0.1; <= 0 disables KO exactly as applyDissipation does */
+    double chi_blend_center; /* 0.05 */
+    double chi_blend_width;  /* 0.02 */
+    int fd_order;            /* must be 4: the only order ccz4.cpp implements */
+    int device;              /* CUDA device ordinal */
+} granite_ccz4_params;
+
+/* Geometry of one GridBlock, mirroring its constructor (grid.hpp:55-61,
+ * grid.cpp:12-31): dx = (hi - lo) / ncells. nghost must be 4 (the upwind
+ * stencil reaches i +- 4, ccz4.cpp:109-152). */
+typedef struct {
+    int ncells[3];
+    int nghost;
+    double lo[3];
+    double hi[3];
+    int level; /* AMR level, 0 = coarsest */
+    int id;    /* caller's block id (informational) */
+} granite_block_desc;
+
+/* ---- context --------------------------------------------------------- */
+
+/* Fills p with the CCZ4Params defaults (ccz4.hpp:25-34), device 0. */
+GRANITE_API void granite_ccz4_default_params(granite_ccz4_params* p);
+
+/* Replaces: CCZ4Evolution::CCZ4Evolution(const CCZ4Params&), ccz4.hpp:60. */
+GRANITE_API int granite_ccz4_create(const granite_ccz4_params* p, void** ctx);
+GRANITE_API int granite_ccz4_destroy(void* ctx);
+/* Copies the message of the last failure (empty if none) into buf. */
+GRANITE_API int granite_ccz4_last_error(const void* ctx, char* buf, size_t len);
+/* Waits for all work enqueued on the context's stream. */
+GRANITE_API int granite_ccz4_sync(void* ctx);
+GRANITE_API int granite_ccz4_abi_version(void);
+
+/* ---- stateless operators on host buffers (drop-in for CCZ4Evolution) --- */
+
+/* Replaces: CCZ4Evolution::computeRHS / computeRHSVacuum, ccz4.hpp:69-81,
+ * ccz4.cpp:229-865 (RHS + Kreiss-Oliger). Writes interior cells of rhs;
+ * ghost cells of rhs keep their values. rho[N], Si[N][3], Sij[N][6], S[N]
+ * (N = cells of the block incl. ghosts) are the matter sources; pass all four
+ * NULL for vacuum. precision: GRANITE_PRECISION_*. */
+GRANITE_API int granite_ccz4_compute_rhs_host(void* ctx, const granite_block_desc* b, const double* u,
+                                  double* rhs, const double* rho, const double* Si,
+                                  const double* Sij, const double* S, int precision);
+
+/* Replaces: CCZ4Evolution::applyDissipation, ccz4.hpp:99, ccz4.cpp:871-935.
+ * rhs (interior) += KO(u). */
+GRANITE_API int granite_ccz4_apply_dissipation_host(void* ctx, const granite_block_desc* b,
+                                        const double* u, double* rhs);
+
+/* Replaces: CCZ4Evolution::computeConstraints, ccz4.hpp:90-92,
+ * ccz4.cpp:941-1159. ham[N], mom[N][3] over the whole block, ghosts zero. */
+GRANITE_API int granite_ccz4_compute_constraints_host(void* ctx, const granite_block_desc* b,
+                                          const double* u, double* ham, double* mom);
+
+/* Same RHS on caller-owned device memory, enqueued on `stream` (a
+ * cudaStream_t, NULL = the context stream). No host synchronisation. */
+GRANITE_API int granite_ccz4_compute_rhs_device(void* ctx, const granite_block_desc* b, const double* u_dev,
+                                    double* rhs_dev, const double* rho_dev, const double* Si_dev,
+                                    const double* Sij_dev, const double* S_dev, int precision,
+                                    void* stream);
+
+/* ---- resident blocks ----------------------------------------------------- */
+/* The hierarchy lives in one device arena per context: add every block, then
+ * commit (allocates state + 2 stage buffers per block and builds the per-level
+ * tile work-lists), then upload. Replaces the GridBlock storage owned by
+ * AMRHierarchy::Level (amr.hpp:104-109). */
+
+GRANITE_API int granite_ccz4_add_block(void* ctx, const granite_block_desc* b, int* block_index);
+GRANITE_API int granite_ccz4_commit(void* ctx);
+GRANITE_API int granite_ccz4_num_blocks(const void* ctx);
+/* bytes of device memory held by the arena after commit */
+GRANITE_API int granite_ccz4_arena_bytes(const void* ctx, size_t* bytes);
+GRANITE_API int granite_ccz4_upload_block(void* ctx, int block_index, const double* host_u);
+GRANITE_API int granite_ccz4_download_block(void* ctx, int block_index, double* host_u);
+
+/* ---- stepping -------------------------------------------------------------- */
+
+/* Replaces: one AMRHierarchy::subcycle(0) pass (amr.cpp:303-330) around
+ * TimeIntegrator::sspRK3Step (main.cpp:86-690, spacetime part) for every
+ * block of `level`, treated as independent single-level blocks: level ghost
+ * fill, 3 fused RHS+KO+RK-combine+floor launches (batched over all blocks of
+ * the level), outer boundary per stage, algebraic constraints on the last
+ * stage, level ghost fill. bc: GRANITE_BC_*. Enqueued as one CUDA graph. */
+GRANITE_API int granite_ccz4_rk3_step(void* ctx, int level, double dt, int precision, int bc);
+
+/* Replaces: AMRHierarchy::subcycle(0, evolve, ...) recursion over all levels
+ * (amr.cpp:303-350) with the RK3 step above as evolve_func
+ * (main.cpp:1142-1177): level l advances by dt_coarse / 2^l, twice per parent
+ * step, followed by restriction to the parent. amr_mode: GRANITE_AMR_*. */
+GRANITE_API int granite_ccz4_hierarchy_step(void* ctx, double dt_coarse, int precision, int amr_mode);
+
+/* ---- diagnostics ----------------------------------------------------------- */
+
+/* Replaces the constraint monitor of main.cpp:1216-1254:
+ * ||H||_2 = sqrt(sum H^2 / N) and ||M||_2 = sqrt(sum |M|^2 / N) over all
+ * interior points of the given level (-1 = all levels). Deterministic. */
+GRANITE_API int granite_ccz4_constraint_norms(void* ctx, int level, double* h_l2, double* m_l2);
+
+/* Number of non-finite chi/alpha values met by the floors since the last call
+ * (the floors repair them, main.cpp:586-608); a health signal, not an error. */
+GRANITE_API int granite_ccz4_nonfinite_count(void* ctx, long long* count);
+
+/* ---- tracing ---------------------------------------------------------------- */
+
+/* kernel classes reported by the profiler */
+#define GRANITE_KERNEL_STAGE 0       /* fused RHS + KO + RK-stage kernel */
+#define GRANITE_KERNEL_GHOST 1       /* ghost fills (level fill, outer boundary) */
+#define GRANITE_KERNEL_TRANSFER 2    /* prolongation, restriction, same-level copies */
+#define GRANITE_KERNEL_CONSTRAINTS 3 /* constraint monitor + reduction */
+#define GRANITE_KERNEL_CLASSES 4
+
+/* While profiling is on, stepping runs without CUDA graphs and brackets every
+ * launch with CUDA events on the context stream; granite_ccz4_profile_get
+ * returns the summed device time and launch count of a kernel class since the
+ * last reset (it synchronises the stream). No counterpart in the reference
+ * (which has no timers). */
+GRANITE_API int granite_ccz4_set_profiling(void* ctx, int enabled);
+GRANITE_API int granite_ccz4_profile_reset(void* ctx);
+GRANITE_API int granite_ccz4_profile_get(void* ctx, int kernel_class, double* total_ms,
+                                         long long* launches);
+/* The context's cudaStream_t, for callers that order their own work or events
+ * against the library's. */
+GRANITE_API int granite_ccz4_get_stream(void* ctx, void** stream);
+
+/* Kernel launches issued by this context so far (graph nodes count once per
+ * replay). */
+GRANITE_API int granite_ccz4_launch_count(const void* ctx, long long* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GRANITE_CCZ4_H */

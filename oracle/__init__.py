@@ -1,0 +1,405 @@
+"""CPU oracle for the CCZ4 RHS + SSP-RK3 hot path -- TEST INFRASTRUCTURE ONLY.
+
+The product library (granite_b200) never imports this package. Only tests/,
+the smoke check in __graft_entry__.py and the cpu_baseline leg of bench.py use
+it, always as the checker or as the timed CPU baseline.
+
+Two backends with one Python surface:
+
+* ``Oracle``  -- liboracle.so, this project's C restatement (ccz4_oracle.c).
+* ``Reference`` -- oracle/_ref/libgranite_ref_*.so, the reference GRANITE
+  sources compiled unmodified behind ref_shim.cpp (built only where the
+  reference tree is present; the built file travels with the repository).
+
+Arrays use the reference GridBlock layout (grid.hpp:109-116): a numpy float64
+array of shape (22, nz+2g, ny+2g, nx+2g), C order, i.e. u[v, k, j, i].
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+NV = 22
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+@dataclass
+class Geom:
+    """Block geometry with the reference's conventions (grid.cpp:12-31)."""
+
+    n: tuple  # interior cells (nx, ny, nz)
+    lo: tuple
+    hi: tuple
+    ng: int = 4
+
+    @property
+    def dx(self):
+        return tuple((self.hi[d] - self.lo[d]) / self.n[d] for d in range(3))
+
+    @property
+    def shape(self):
+        nx, ny, nz = self.n
+        g = 2 * self.ng
+        return (NV, nz + g, ny + g, nx + g)
+
+    @property
+    def cells(self):
+        s = self.shape
+        return s[1] * s[2] * s[3]
+
+    def zeros(self):
+        return np.zeros(self.shape, dtype=np.float64)
+
+    def interior(self):
+        g = self.ng
+        nx, ny, nz = self.n
+        return (slice(None), slice(g, g + nz), slice(g, g + ny), slice(g, g + nx))
+
+    def x(self, d, idx):
+        return self.lo[d] + (float(idx) - self.ng + 0.5) * self.dx[d]
+
+
+class _orc_geom(C.Structure):
+    _fields_ = [("n", C.c_int * 3), ("ng", C.c_int), ("lo", C.c_double * 3),
+                ("dx", C.c_double * 3)]
+
+
+class _orc_params(C.Structure):
+    _fields_ = [("kappa1", C.c_double), ("kappa2", C.c_double), ("eta", C.c_double),
+                ("ko_sigma", C.c_double), ("chi_blend_center", C.c_double),
+                ("chi_blend_width", C.c_double)]
+
+
+@dataclass
+class Params:
+    """CCZ4Params defaults, ccz4.hpp:25-34."""
+
+    kappa1: float = 0.02
+    kappa2: float = 0.0
+    eta: float = 2.0
+    ko_sigma: float = 0.1
+    chi_blend_center: float = 0.05
+    chi_blend_width: float = 0.02
+
+    def as6(self):
+        return np.array([self.kappa1, self.kappa2, self.eta, self.ko_sigma,
+                         self.chi_blend_center, self.chi_blend_width], dtype=np.float64)
+
+
+BC_SOMMERFELD = 0
+BC_PERIODIC = 1
+
+
+def build(force: bool = False) -> None:
+    """Compile liboracle.so (and oracle/_ref when the reference tree exists)."""
+    lib = os.path.join(HERE, "liboracle.so")
+    if force or not os.path.exists(lib) or not os.path.exists(os.path.join(HERE, "_ref")):
+        subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+
+
+def _cg(g: Geom) -> _orc_geom:
+    o = _orc_geom()
+    for d in range(3):
+        o.n[d] = g.n[d]
+        o.lo[d] = g.lo[d]
+        o.dx[d] = g.dx[d]
+    o.ng = g.ng
+    return o
+
+
+def _cp(p: Params) -> _orc_params:
+    return _orc_params(p.kappa1, p.kappa2, p.eta, p.ko_sigma, p.chi_blend_center,
+                       p.chi_blend_width)
+
+
+class Oracle:
+    """This project's C restatement (liboracle.so)."""
+
+    kind = "port"
+
+    def __init__(self, threads: int = 0):
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        self.lib = C.CDLL(path)
+        if threads:
+            self.lib.orc_set_threads(threads)
+
+    def rhs(self, p: Params, g: Geom, u, rho=None, Si=None, Sij=None, S=None):
+        out = g.zeros()
+        self.lib.orc_rhs(C.byref(_cp(p)), C.byref(_cg(g)), _p(u), _p(out), _p(rho), _p(Si),
+                         _p(Sij), _p(S))
+        return out
+
+    def dissipation(self, p: Params, g: Geom, u, rhs):
+        rhs = np.array(rhs, dtype=np.float64, copy=True)
+        self.lib.orc_dissipation(C.byref(_cp(p)), C.byref(_cg(g)), _p(u), _p(rhs))
+        return rhs
+
+    def constraints(self, g: Geom, u):
+        ham = np.zeros(g.shape[1:], dtype=np.float64)
+        mom = np.zeros(g.shape[1:] + (3,), dtype=np.float64)
+        self.lib.orc_constraints(C.byref(_cg(g)), _p(u), _p(ham), _p(mom))
+        return ham, mom
+
+    def constraint_sums(self, g: Geom, u):
+        h2, m2, n = C.c_double(), C.c_double(), C.c_long()
+        self.lib.orc_constraint_sums(C.byref(_cg(g)), _p(u), C.byref(h2), C.byref(m2),
+                                     C.byref(n))
+        return h2.value, m2.value, n.value
+
+    def fill(self, g: Geom, u, kind: str):
+        fn = {"zero_gradient": self.lib.orc_fill_zero_gradient,
+              "sommerfeld": self.lib.orc_fill_sommerfeld,
+              "periodic": self.lib.orc_fill_periodic,
+              "floors": self.lib.orc_floors,
+              "algebraic": self.lib.orc_algebraic}[kind]
+        fn(C.byref(_cg(g)), _p(u))
+        return u
+
+    def rk3_steps(self, p: Params, g: Geom, u, dt: float, nsteps: int, bc: int = BC_SOMMERFELD):
+        u = np.array(u, dtype=np.float64, copy=True)
+        stage = g.zeros()
+        rhs = g.zeros()
+        for _ in range(nsteps):
+            self.lib.orc_rk3_step(C.byref(_cp(p)), C.byref(_cg(g)), _p(u), _p(stage), _p(rhs),
+                                  C.c_double(dt), C.c_int(bc))
+        return u
+
+    def init_flat(self, g: Geom):
+        u = g.zeros()
+        self.lib.orc_init_flat(C.byref(_cg(g)), _p(u))
+        return u
+
+    def init_gauge_wave(self, g: Geom, amplitude: float, wavelength: float):
+        u = g.zeros()
+        self.lib.orc_init_gauge_wave(C.byref(_cg(g)), _p(u), C.c_double(amplitude),
+                                     C.c_double(wavelength))
+        return u
+
+    def init_brill_lindquist(self, g: Geom, masses, positions, r_floor: float = 0.0):
+        u = g.zeros()
+        m = np.ascontiguousarray(masses, dtype=np.float64)
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        self.lib.orc_init_brill_lindquist(C.byref(_cg(g)), _p(u), C.c_int(len(m)), _p(m),
+                                          _p(pos), C.c_double(r_floor))
+        return u
+
+    def bl_conformal_factor(self, masses, positions, x, y, z, r_floor=0.0):
+        m = np.ascontiguousarray(masses, dtype=np.float64)
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        self.lib.orc_bl_conformal_factor.restype = C.c_double
+        return self.lib.orc_bl_conformal_factor(C.c_int(len(m)), _p(m), _p(pos), C.c_double(x),
+                                                C.c_double(y), C.c_double(z),
+                                                C.c_double(r_floor))
+
+    def prolongate(self, gc: Geom, uc, gf: Geom, uf, ghosts_only: bool = False):
+        uf = np.array(uf, dtype=np.float64, copy=True)
+        self.lib.orc_prolongate(C.byref(_cg(gc)), _p(uc), C.byref(_cg(gf)), _p(uf),
+                                C.c_int(int(ghosts_only)))
+        return uf
+
+    def restrict(self, gf: Geom, uf, gc: Geom, uc):
+        uc = np.array(uc, dtype=np.float64, copy=True)
+        self.lib.orc_restrict(C.byref(_cg(gf)), _p(uf), C.byref(_cg(gc)), _p(uc))
+        return uc
+
+
+def _host_has_avx512() -> bool:
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = f.read()
+        return all(x in flags for x in ("avx512f", "avx512dq", "avx512bw", "avx512vl"))
+    except OSError:
+        return False
+
+
+def reference_path(variant: str = "strict") -> str:
+    """Path of a compiled reference library: 'strict' (IEEE, for pinning) or
+    'fast' (reference Release flags, for timing; ISA level picked for this host)."""
+    if variant == "fast":
+        variant = "fast_v4" if _host_has_avx512() else "fast_v3"
+    return os.path.join(HERE, "_ref", f"libgranite_ref_{variant}.so")
+
+
+def reference_available(variant: str = "strict") -> bool:
+    return os.path.exists(reference_path(variant))
+
+
+class Reference:
+    """The compiled reference sources behind ref_shim.cpp."""
+
+    kind = "reference"
+
+    def __init__(self, variant: str = "strict", threads: int = 0):
+        self.path = reference_path(variant)
+        self.lib = C.CDLL(self.path)
+        if threads:
+            self.lib.ref_set_threads(threads)
+        self.lib.ref_bl_conformal_factor.restype = C.c_double
+
+    @staticmethod
+    def _g(g: Geom):
+        n = (C.c_int * 3)(*g.n)
+        lo = (C.c_double * 3)(*g.lo)
+        hi = (C.c_double * 3)(*g.hi)
+        return n, C.c_int(g.ng), lo, hi
+
+    def max_threads(self) -> int:
+        return int(self.lib.ref_max_threads())
+
+    def rhs(self, p: Params, g: Geom, u, rho=None, Si=None, Sij=None, S=None):
+        out = g.zeros()
+        p6 = p.as6()
+        self.lib.ref_rhs(_p(p6), *self._g(g), _p(u), _p(out), _p(rho), _p(Si), _p(Sij), _p(S))
+        return out
+
+    def dissipation(self, p: Params, g: Geom, u, rhs):
+        rhs = np.array(rhs, dtype=np.float64, copy=True)
+        p6 = p.as6()
+        self.lib.ref_dissipation(_p(p6), *self._g(g), _p(u), _p(rhs))
+        return rhs
+
+    def constraints(self, g: Geom, u):
+        ham = np.zeros(g.shape[1:], dtype=np.float64)
+        mom = np.zeros(g.shape[1:] + (3,), dtype=np.float64)
+        self.lib.ref_constraints(*self._g(g), _p(u), _p(ham), _p(mom))
+        return ham, mom
+
+    def init_flat(self, g: Geom):
+        u = g.zeros()
+        self.lib.ref_init_flat(*self._g(g), _p(u))
+        return u
+
+    def init_gauge_wave(self, g: Geom, amplitude: float, wavelength: float):
+        u = g.zeros()
+        self.lib.ref_init_gauge_wave(*self._g(g), _p(u), C.c_double(amplitude),
+                                     C.c_double(wavelength))
+        return u
+
+    def init_brill_lindquist(self, g: Geom, masses, positions):
+        u = g.zeros()
+        m = np.ascontiguousarray(masses, dtype=np.float64)
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        self.lib.ref_init_brill_lindquist(*self._g(g), _p(u), C.c_int(len(m)), _p(m), _p(pos))
+        return u
+
+    def bl_conformal_factor(self, masses, positions, x, y, z):
+        m = np.ascontiguousarray(masses, dtype=np.float64)
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        return self.lib.ref_bl_conformal_factor(C.c_int(len(m)), _p(m), _p(pos), C.c_double(x),
+                                                C.c_double(y), C.c_double(z))
+
+    def fill_level0(self, g: Geom, u):
+        u = np.array(u, dtype=np.float64, copy=True)
+        self.lib.ref_fill_level0(*self._g(g), _p(u))
+        return u
+
+    def prolongate(self, gc: Geom, uc, clevel, gf: Geom, uf, flevel):
+        uf = np.array(uf, dtype=np.float64, copy=True)
+        cn, _, clo, chi = self._g(gc)
+        fn, ng, flo, fhi = self._g(gf)
+        self.lib.ref_prolongate(cn, clo, chi, C.c_int(clevel), _p(uc), fn, flo, fhi,
+                                C.c_int(flevel), _p(uf), ng)
+        return uf
+
+    def restrict(self, gf: Geom, uf, flevel, gc: Geom, uc, clevel):
+        uc = np.array(uc, dtype=np.float64, copy=True)
+        cn, _, clo, chi = self._g(gc)
+        fn, ng, flo, fhi = self._g(gf)
+        self.lib.ref_restrict(fn, flo, fhi, C.c_int(flevel), _p(uf), cn, clo, chi,
+                              C.c_int(clevel), _p(uc), ng)
+        return uc
+
+    def rk3_steps(self, p: Params, g: Geom, u, dt: float, nsteps: int, bc: int = BC_SOMMERFELD):
+        u = np.array(u, dtype=np.float64, copy=True)
+        p6 = p.as6()
+        self.lib.ref_rk3_steps(_p(p6), *self._g(g), _p(u), C.c_double(dt), C.c_int(nsteps),
+                               C.c_int(bc))
+        return u
+
+
+# ---------------------------------------------------------------------------
+# Seeded workloads shared by tests and bench (same draws on every backend)
+# ---------------------------------------------------------------------------
+
+def add_noise(u, amplitude: float, seed: int):
+    """Uniform(-a, a) noise on every field and cell, numpy PCG64 stream."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return u + rng.uniform(-amplitude, amplitude, size=u.shape)
+
+
+def random_state(g: Geom, seed: int, amp: float = 0.05):
+    """A smooth, strongly non-flat but well-conditioned state for RHS parity."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nz, ny, nx = g.shape[1:]
+    X = np.array([g.x(0, i) for i in range(nx)])[None, None, :]
+    Y = np.array([g.x(1, j) for j in range(ny)])[None, :, None]
+    Z = np.array([g.x(2, k) for k in range(nz)])[:, None, None]
+    L = [g.hi[d] - g.lo[d] for d in range(3)]
+    u = np.zeros(g.shape)
+    base = np.zeros(NV)
+    base[[0, 1, 4, 6, 18]] = 1.0  # chi, gxx, gyy, gzz, alpha
+    for v in range(NV):
+        a = rng.uniform(-1, 1, size=3)
+        ph = rng.uniform(0, 2 * np.pi, size=3)
+        u[v] = base[v] + amp * (a[0] * np.sin(2 * np.pi * X / L[0] * 1.3 + ph[0])
+                                * np.cos(2 * np.pi * Y / L[1] * 0.7 + ph[1])
+                                + a[1] * np.sin(2 * np.pi * Z / L[2] * 1.1 + ph[2])
+                                + a[2] * np.cos(2 * np.pi * (X / L[0] + Y / L[1] - Z / L[2])))
+    return u
+
+
+def hash_noise(shape, seed: int):
+    """Deterministic uniform(-0.5, 0.5) values from an integer hash (splitmix64),
+    exactly representable (k / 2^24 - 1/2), identical on every host."""
+    n = int(np.prod(shape))
+    with np.errstate(over="ignore"):
+        x = np.arange(n, dtype=np.uint64) + np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15)
+        x = x + np.uint64(0x9E3779B97F4A7C15)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        x = x ^ (x >> np.uint64(31))
+    k = (x >> np.uint64(40)).astype(np.float64)  # 24 bits
+    return (k / 16777216.0 - 0.5).reshape(shape)
+
+
+def seeded_state(g: Geom, seed: int, amp: float = 0.05, noise: float = 1e-3):
+    """Smooth polynomial background + hash noise, built from IEEE + and * only so
+    the same inputs are reproduced bit for bit on any machine."""
+    nz, ny, nx = g.shape[1:]
+    X = np.array([g.x(0, i) for i in range(nx)])[None, None, :]
+    Y = np.array([g.x(1, j) for j in range(ny)])[None, :, None]
+    Z = np.array([g.x(2, k) for k in range(nz)])[:, None, None]
+    L = max(g.hi[d] - g.lo[d] for d in range(3))
+    X, Y, Z = X / L, Y / L, Z / L
+    co = hash_noise((NV, 10), seed + 1000)
+    u = np.zeros(g.shape)
+    base = np.zeros(NV)
+    base[[0, 1, 4, 6, 18]] = 1.0
+    for v in range(NV):
+        c = co[v]
+        poly = (c[0] * X + c[1] * Y + c[2] * Z + c[3] * X * Y + c[4] * Y * Z + c[5] * X * Z
+                + c[6] * X * X + c[7] * Y * Y + c[8] * Z * Z + c[9] * X * Y * Z)
+        u[v] = base[v] + amp * poly
+    u += noise * hash_noise(g.shape, seed)
+    return u
+
+
+def seeded_matter(g: Geom, seed: int, amp: float = 1e-2):
+    N = g.cells
+    rho = amp * (hash_noise((N,), seed + 1) + 0.5)
+    Si = amp * hash_noise((N * 3,), seed + 2)
+    Sij = amp * hash_noise((N * 6,), seed + 3)
+    S = amp * (hash_noise((N,), seed + 4) + 0.5)
+    return rho, Si, Sij, S

@@ -1,0 +1,136 @@
+"""CPU-side checks of the product boundary (no GPU compute here).
+
+- libgranite_ccz4.so builds for sm_100a and loads, and exports every function
+  that include/granite_ccz4.h declares;
+- the header compiles as C and C++;
+- without a GPU the library reports GRANITE_ERR_NO_DEVICE instead of crashing
+  or falling back to a CPU path;
+- host-side logic (GridBlock layout and coordinates, initial data) matches the
+  oracle's conventions.
+"""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle import Geom
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "granite_ccz4.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(granite_ccz4_\w+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from granite_b200 import build
+    path = build.build()
+    return C.CDLL(path)
+
+
+def test_header_declares_the_boundary():
+    names = declared_functions()
+    for n in ["granite_ccz4_create", "granite_ccz4_destroy", "granite_ccz4_compute_rhs_host",
+              "granite_ccz4_apply_dissipation_host", "granite_ccz4_compute_constraints_host",
+              "granite_ccz4_rk3_step", "granite_ccz4_hierarchy_step",
+              "granite_ccz4_constraint_norms", "granite_ccz4_last_error"]:
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol(lib):
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_library_exports_nothing_else():
+    from granite_b200 import build
+    out = subprocess.run(["nm", "-D", "--defined-only", build.LIB], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    ours = {e for e in exported if e.startswith("granite_")}
+    assert ours == set(declared_functions())
+
+
+@pytest.mark.parametrize("compiler,flag", [("/usr/bin/gcc", "-std=c99"), ("/usr/bin/g++", "-std=c++17")])
+def test_header_compiles(tmp_path, compiler, flag):
+    if not os.path.exists(compiler):
+        pytest.skip("no system compiler")
+    src = tmp_path / ("t.c" if "gcc" in compiler else "t.cpp")
+    src.write_text('#include "granite_ccz4.h"\nint main(void){granite_ccz4_params p;'
+                   'granite_ccz4_default_params(&p);return p.fd_order == 4 ? 0 : 1;}\n')
+    subprocess.run([compiler, flag, "-Wall", "-Werror", "-c", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-o", str(tmp_path / "t.o")], check=True)
+
+
+def test_abi_version_and_defaults(lib):
+    assert lib.granite_ccz4_abi_version() == 1
+    import granite_b200 as gb
+    p = gb._Params()
+    lib.granite_ccz4_default_params(C.byref(p))
+    assert (p.kappa1, p.kappa2, p.eta, p.ko_sigma) == (0.02, 0.0, 2.0, 0.1)
+    assert (p.chi_blend_center, p.chi_blend_width, p.fd_order) == (0.05, 0.02, 4)
+
+
+def test_no_device_is_an_error_not_a_fallback(lib):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    import granite_b200 as gb
+    p = gb._Params()
+    lib.granite_ccz4_default_params(C.byref(p))
+    h = C.c_void_p()
+    rc = lib.granite_ccz4_create(C.byref(p), C.byref(h))
+    assert rc == -3 and not h.value
+    with pytest.raises(gb.GraniteError):
+        gb.CCZ4Evolution(gb.CCZ4Params())
+
+
+def test_invalid_arguments_rejected(lib):
+    import granite_b200 as gb
+    p = gb._Params()
+    lib.granite_ccz4_default_params(C.byref(p))
+    p.fd_order = 6
+    h = C.c_void_p()
+    assert lib.granite_ccz4_create(C.byref(p), C.byref(h)) == -6
+    assert lib.granite_ccz4_create(None, C.byref(h)) == -1
+    assert lib.granite_ccz4_destroy(None) == 0
+
+
+def test_gridblock_layout_matches_reference_conventions():
+    import granite_b200 as gb
+    b = gb.GridBlock(3, 1, (6, 5, 4), (-1.0, 0.0, 2.0), (2.0, 1.0, 3.0), 4, 22)
+    g = Geom((6, 5, 4), (-1.0, 0.0, 2.0), (2.0, 1.0, 3.0))
+    assert b.array.shape == g.shape
+    assert b.totalSize() == g.cells
+    for d, n in enumerate((6, 5, 4)):
+        for idx in range(n + 8):
+            assert b.x(d, idx) == g.x(d, idx)
+    # flat index = var*stride + i + nx*(j + ny*k) (grid.hpp:109-116)
+    b.set(5, 2, 3, 1, 7.0)
+    stride = 14 * 13 * 12
+    assert b.flatBuffer()[5 * stride + 2 + 14 * (3 + 13 * 1)] == 7.0
+
+
+def test_initial_data_matches_oracle(oracle_lib):
+    import granite_b200 as gb
+    g = Geom((12, 10, 8), (-3.0, -2.5, -2.0), (3.0, 2.5, 2.0))
+    b = gb.GridBlock(0, 0, g.n, g.lo, g.hi)
+    gb.brill_lindquist(b, [0.5, 0.4], [[0.3, 0.0, 0.0], [-0.4, 0.1, 0.0]], r_floor=0.2)
+    ref = oracle_lib.init_brill_lindquist(g, [0.5, 0.4], [[0.3, 0.0, 0.0], [-0.4, 0.1, 0.0]], 0.2)
+    np.testing.assert_allclose(b.array, ref, rtol=1e-14, atol=1e-15)
+    gw = Geom((16, 4, 4), (-0.5, -0.5, -0.5), (0.5, -0.25, -0.25))
+    b = gb.GridBlock(0, 0, gw.n, gw.lo, gw.hi)
+    gb.gauge_wave(b, -0.1, 1.0)
+    np.testing.assert_allclose(b.array, oracle_lib.init_gauge_wave(gw, -0.1, 1.0), rtol=1e-14,
+                               atol=1e-15)
