@@ -143,6 +143,8 @@ DevBlock make_devblock(const granite_block_desc& b, double sigma) {
         d.inv12h[a] = 1.0 / (12.0 * d.dx[a]);
         d.inv12h2[a] = 1.0 / (12.0 * d.dx[a] * d.dx[a]);
         d.kocf[a] = sigma / (64.0 * d.dx[a]);
+        const double wts[4] = {1.0, -6.0, 15.0, -20.0};
+        for (int s = 0; s < 4; ++s) d.kow[a][s] = d.kocf[a] * wts[s];
     }
     d.inv4hh[0] = 1.0 / (4.0 * d.dx[0] * d.dx[1]);
     d.inv4hh[1] = 1.0 / (4.0 * d.dx[0] * d.dx[2]);

@@ -33,6 +33,7 @@ struct DevBlock {
     double inv12h2[3];   // 1/(12 dx^2)    second derivative (ccz4.cpp:158)
     double inv4hh[3];    // 1/(4 dx_a dx_b) mixed (xy, xz, yz) (ccz4.cpp:188)
     double kocf[3];      // sigma/(64 dx)  KO (ccz4.cpp:886-887)
+    double kow[3][4];    // kocf[d] * {1, -6, 15, -20}: the KO weights of ccz4.cpp:921
     int level;
     int pad_;
 };

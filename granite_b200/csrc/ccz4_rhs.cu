@@ -87,7 +87,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     // ---- conformal metric: gradients, Hessian term of Ricci, advection ----
     P dg[6][3];     // d_k gt_ij
     P Rt[6];        // conformal Ricci (ccz4.cpp:465-516), accumulated term by term
-    P rgt[6];       // advection + KO of gt
+    P agt[6], kgt[6];  // advection and KO of gt
 #pragma unroll
     for (int a = 0; a < 6; ++a) {
         FieldDer<P> fd = field_der<P, true>(B, FP(GXX + a), beta, w, ko);
@@ -96,7 +96,8 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
         // term 1: -1/2 gtu^{lm} d_l d_m gt_ij
         Rt[a] = (P)-0.5 * (gtu[0] * fd.h[0] + gtu[3] * fd.h[3] + gtu[5] * fd.h[5] +
                            (P)2 * (gtu[1] * fd.h[1] + gtu[2] * fd.h[2] + gtu[4] * fd.h[4]));
-        rgt[a] = fd.adv + fd.ko;
+        agt[a] = fd.adv;
+        kgt[a] = fd.ko;
     }
     // first-kind Christoffels G1[k][ij] = 1/2 (d_i g_kj + d_j g_ki - d_k g_ij)
     P G1[3][6];
@@ -123,13 +124,14 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
 
     // ---- Gamma-hat: gradient (Ricci term 2), advection --------------------
     P dGh[3][3];
-    P rGh[3];
+    P aGh[3], kGh[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         FieldDer<P> fd = field_der<P, false>(B, FP(GHX + a), beta, w, ko);
 #pragma unroll
         for (int d = 0; d < 3; ++d) dGh[a][d] = fd.d[d];
-        rGh[a] = fd.adv + fd.ko;
+        aGh[a] = fd.adv;
+        kGh[a] = fd.ko;
     }
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -215,7 +217,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     // ---- shift: gradient, Hessian terms T5/T6 ---------------------------------
     P db[3][3];  // d_j beta^i as db[i][j]
     P T5[3], ddiv[3];
-    P rbe[3];
+    P abe[3], kbe[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) ddiv[d] = (P)0;
 #pragma unroll
@@ -228,7 +230,8 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
         // d_j (d_k beta^k): add d_j d_a beta^a
 #pragma unroll
         for (int d = 0; d < 3; ++d) ddiv[d] += fb.h[sy(a, d)];
-        rbe[a] = fb.adv + fb.ko;
+        abe[a] = fb.adv;
+        kbe[a] = fb.ko;
     }
     const P divb = db[0][0] + db[1][1] + db[2][2];  // :548
 
@@ -259,24 +262,25 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
 
     // ---- RHS assembly ----------------------------------------------------------
     // chi (ccz4.cpp:580)
-    out[CHI] = (double)((P)(2.0 / 3.0) * chiP * (alpha * K - divb) + fchi.adv + fchi.ko);
+    // each field: (RHS incl. advection) + KO, the order of ccz4.cpp:864,930
+    out[CHI] = (double)(((P)(2.0 / 3.0) * chiP * (alpha * K - divb) + fchi.adv) + fchi.ko);
     // gt (ccz4.cpp:586-607)
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = i; j < 3; ++j) {
             const int ij = sy(i, j);
-            P lie = (P)0;
+            P lie = agt[ij];
 #pragma unroll
             for (int d = 0; d < 3; ++d) lie += gt[sy(i, d)] * db[d][j] + gt[sy(j, d)] * db[d][i];
-            out[GXX + ij] = (double)((P)-2 * alpha * At[ij] + lie - (P)(2.0 / 3.0) * gt[ij] * divb + rgt[ij]);
+            out[GXX + ij] = (double)(((P)-2 * alpha * At[ij] + lie - (P)(2.0 / 3.0) * gt[ij] * divb) + kgt[ij]);
         }
     // K (ccz4.cpp:650-652)
     {
         FieldDer<P> fK = field_der<P, false>(B, FP(KTR), beta, w, ko);
         const P k1 = (P)A.kappa1, k2 = (P)A.kappa2;
-        out[KTR] = (double)(-phys_lap_alpha + alpha * (AtAt + K * K / (P)3) + (P)4 * PI * alpha * (rho + Str) +
-                            k1 * ((P)1 - k2) * alpha * Theta + fK.adv + fK.ko);
+        out[KTR] = (double)((-phys_lap_alpha + alpha * (AtAt + K * K / (P)3) + (P)4 * PI * alpha * (rho + Str) +
+                            k1 * ((P)1 - k2) * alpha * Theta + fK.adv) + fK.ko);
         // Gamma-hat (ccz4.cpp:747-815)
         const P c3a = (P)(3.0 * alpha_d / (chi + 1e-30));
 #pragma unroll
@@ -292,17 +296,17 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
             const P T6 = (P)(1.0 / 3.0) *
                 (gtu[sy(i, 0)] * ddiv[0] + gtu[sy(i, 1)] * ddiv[1] + gtu[sy(i, 2)] * ddiv[2]);
             P T7 = -(Gh[0] * db[i][0] + Gh[1] * db[i][1] + Gh[2] * db[i][2]);
-            T7 += rGh[i] + (P)(2.0 / 3.0) * Gh[i] * divb;
+            T7 += aGh[i] + (P)(2.0 / 3.0) * Gh[i] * divb;
             const P T8 = (P)-2 * (P)A.kappa1 * alpha * Gh[i];
-            out[GHX + i] = (double)(T1 + T2 + T3 + T4 + T5[i] + T6 + T7 + T8);
+            out[GHX + i] = (double)((T1 + T2 + T3 + T4 + T5[i] + T6 + T7 + T8) + kGh[i]);
         }
     }
     // Theta (ccz4.cpp:662-665)
     {
         FieldDer<P> fT = field_der<P, false>(B, FP(THETA), beta, w, ko);
         const P k1 = (P)A.kappa1, k2 = (P)A.kappa2;
-        out[THETA] = (double)((P)0.5 * alpha * (Rs - AtAt + (P)2 * K * K / (P)3 - (P)16 * PI * rho) -
-                              alpha * k1 * ((P)2 + k2) * Theta + fT.adv + fT.ko);
+        out[THETA] = (double)(((P)0.5 * alpha * (Rs - AtAt + (P)2 * K * K / (P)3 - (P)16 * PI * rho) -
+                              alpha * k1 * ((P)2 + k2) * Theta + fT.adv) + fT.ko);
     }
     // A-tilde (ccz4.cpp:671-726): the advection is part of Lie_At and is
     // trace-removed with the rest; KO is added after the trace removal.
@@ -330,11 +334,11 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
         for (int a = 0; a < 6; ++a) out[AXX + a] = (double)(raw[a] - (P)(1.0 / 3.0) * gt[a] * tr + koA[a]);
     }
     // lapse (ccz4.cpp:820) and shift (ccz4.cpp:825-831)
-    out[ALPHA] = (double)((P)-2 * alpha * K + fal.adv + fal.ko);
+    out[ALPHA] = (double)(((P)-2 * alpha * K + fal.adv) + fal.ko);
     {
         const P eta = (P)A.eta;
 #pragma unroll
-        for (int d = 0; d < 3; ++d) out[BETAX + d] = (double)((P)0.75 * Gh[d] - eta * (P)beta[d] + rbe[d]);
+        for (int d = 0; d < 3; ++d) out[BETAX + d] = (double)(((P)0.75 * Gh[d] - eta * (P)beta[d] + abe[d]) + kbe[d]);
     }
 #undef FP
 }

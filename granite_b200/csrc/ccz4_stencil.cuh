@@ -1,7 +1,19 @@
 // ccz4_stencil.cuh -- finite-difference stencils of the CCZ4 operator
-// (ccz4.cpp:71-223 and the KO operator of ccz4.cpp:871-935), evaluated from
-// FP64 pair differences so a reduced-precision algebra type P loses nothing
-// to cancellation.
+// (ccz4.cpp:71-223) and the Kreiss-Oliger operator (ccz4.cpp:871-935).
+//
+// Two evaluation modes, chosen by the algebra type P:
+//
+//  P = double (plain FP64): every stencil is evaluated in the reference's
+//    operation order with explicitly rounded products and sums, so the
+//    derivatives and the KO term are bit-identical to the host code. This
+//    matters where a field is O(1) and its RHS is ~1e-6 of that (noisy flat
+//    regions): there the rounding of the reference's own stencil sums is the
+//    size of the result, and only the same rounding reproduces it.
+//
+//  P = float (mixed): stencils are evaluated from FP64 pair differences
+//    (f[+k] - f[-k], f[+k] + f[-k] - 2 f[0], ...) that cancel exactly, and only
+//    the small differences are rounded to FP32; the algebra downstream runs in
+//    FP32 without losing the cancellation.
 #pragma once
 
 #include "ccz4_common.cuh"
@@ -9,69 +21,117 @@
 namespace granite_b200 {
 namespace {
 
-template <typename T>
-__device__ __forceinline__ T ld(const double* p) {
-    return (T)__ldg(p);
-}
+#define RN_MUL __dmul_rn
+#define RN_ADD __dadd_rn
+#define RN_SUB __dsub_rn
 
-// ---------------------------------------------------------------------------
-// Stencil evaluation. `f` points at the centre value; `s` is one cell along
-// the axis. Pair differences are taken in FP64 and rounded to P afterwards.
-// ---------------------------------------------------------------------------
 template <typename P>
 struct AxisDer {
-    P d1;   // 4th-order centred first derivative, ccz4.cpp:71-99
-    P up;   // 4th-order one-sided derivative on the upwind side, ccz4.cpp:109-152
-    P ko;   // sigma/(64 dx) x undivided 6th difference, ccz4.cpp:886-931
-    P d2;   // 4th-order second derivative, ccz4.cpp:156-184
+    P d1;  // 4th-order centred first derivative, ccz4.cpp:71-99
+    P up;  // 4th-order one-sided derivative on the upwind side, ccz4.cpp:109-152
+    P d2;  // 4th-order second derivative, ccz4.cpp:156-184
 };
 
-template <typename P, bool WANT_D2, bool WANT_KO>
-__device__ __forceinline__ AxisDer<P> axis_der(const double* __restrict__ f, long long s, double f0,
-                                              double beta, double inv12h, double inv12h2,
-                                              double kocf) {
+// Reference-order evaluation (P = double). `ko` accumulates the KO sum across
+// the three axes exactly as ccz4.cpp:912-926 does.
+template <bool WANT_D2, bool WANT_KO>
+__device__ __forceinline__ AxisDer<double> axis_exact(const double* __restrict__ f, long long s, double f0,
+                                                     double beta, double inv12h, double inv12h2,
+                                                     const double* kw, double& ko) {
     const double fm1 = __ldg(f - s), fp1 = __ldg(f + s);
     const double fm2 = __ldg(f - 2 * s), fp2 = __ldg(f + 2 * s);
-    const double fm3 = __ldg(f - 3 * s), fp3 = __ldg(f + 3 * s);
-    AxisDer<P> r;
-    // pair differences in FP64
-    const double a1 = fp1 - fm1, a2 = fp2 - fm2;
-    r.d1 = (P)inv12h * ((P)8.0 * (P)a1 - (P)a2);
-    double e;
+    AxisDer<double> r;
+    // inv12h * (-f[+2] + 8 f[+1] - 8 f[-1] + f[-2])
+    r.d1 = RN_MUL(inv12h, RN_ADD(RN_SUB(RN_ADD(-fp2, RN_MUL(8.0, fp1)), RN_MUL(8.0, fm1)), fm2));
+    double fm3 = 0.0, fp3 = 0.0;
+    if (WANT_KO || beta >= 0.0) fm3 = __ldg(f - 3 * s);
+    if (WANT_KO || !(beta >= 0.0)) fp3 = __ldg(f + 3 * s);
     if (beta >= 0.0) {
         const double fm4 = __ldg(f - 4 * s);
-        // 25 f0 - 48 f-1 + 36 f-2 - 16 f-3 + 3 f-4 (weights sum to zero): differences vs f0
+        // inv12h * (25 f0 - 48 f-1 + 36 f-2 - 16 f-3 + 3 f-4)
+        r.up = RN_MUL(inv12h, RN_ADD(RN_SUB(RN_ADD(RN_SUB(RN_MUL(25.0, f0), RN_MUL(48.0, fm1)), RN_MUL(36.0, fm2)),
+                                            RN_MUL(16.0, fm3)),
+                                     RN_MUL(3.0, fm4)));
+    } else {
+        const double fp4 = __ldg(f + 4 * s);
+        // inv12h * (-25 f0 + 48 f+1 - 36 f+2 + 16 f+3 - 3 f+4)
+        r.up = RN_MUL(inv12h, RN_SUB(RN_ADD(RN_SUB(RN_ADD(RN_MUL(-25.0, f0), RN_MUL(48.0, fp1)), RN_MUL(36.0, fp2)),
+                                            RN_MUL(16.0, fp3)),
+                                     RN_MUL(3.0, fp4)));
+    }
+    if (WANT_D2) {
+        // inv12h2 * (-f[+2] + 16 f[+1] - 30 f0 + 16 f[-1] - f[-2])
+        r.d2 = RN_MUL(inv12h2, RN_SUB(RN_ADD(RN_SUB(RN_ADD(-fp2, RN_MUL(16.0, fp1)), RN_MUL(30.0, f0)),
+                                             RN_MUL(16.0, fm1)),
+                                      fm2));
+    } else {
+        r.d2 = 0.0;
+    }
+    if (WANT_KO) {
+        // diss += (cf w_s) u(x + s e_d), s = -3..3, w = {1,-6,15,-20,15,-6,1}
+        ko = RN_ADD(ko, RN_MUL(kw[0], fm3));
+        ko = RN_ADD(ko, RN_MUL(kw[1], fm2));
+        ko = RN_ADD(ko, RN_MUL(kw[2], fm1));
+        ko = RN_ADD(ko, RN_MUL(kw[3], f0));
+        ko = RN_ADD(ko, RN_MUL(kw[2], fp1));
+        ko = RN_ADD(ko, RN_MUL(kw[1], fp2));
+        ko = RN_ADD(ko, RN_MUL(kw[0], fp3));
+    }
+    return r;
+}
+
+// Pair-difference evaluation (P = float).
+template <bool WANT_D2, bool WANT_KO>
+__device__ __forceinline__ AxisDer<float> axis_pairs(const double* __restrict__ f, long long s, double f0,
+                                                    double beta, double inv12h, double inv12h2, double kocf,
+                                                    float& ko) {
+    const double fm1 = __ldg(f - s), fp1 = __ldg(f + s);
+    const double fm2 = __ldg(f - 2 * s), fp2 = __ldg(f + 2 * s);
+    AxisDer<float> r;
+    const float a1 = (float)(fp1 - fm1), a2 = (float)(fp2 - fm2);
+    r.d1 = (float)inv12h * (8.0f * a1 - a2);
+    double e;
+    double fm3 = 0.0, fp3 = 0.0;
+    if (WANT_KO || beta >= 0.0) fm3 = __ldg(f - 3 * s);
+    if (WANT_KO || !(beta >= 0.0)) fp3 = __ldg(f + 3 * s);
+    if (beta >= 0.0) {
+        const double fm4 = __ldg(f - 4 * s);
+        // 25 f0 - 48 f-1 + 36 f-2 - 16 f-3 + 3 f-4 with weights summing to zero
         e = 48.0 * (f0 - fm1) - 36.0 * (f0 - fm2) + 16.0 * (f0 - fm3) - 3.0 * (f0 - fm4);
     } else {
         const double fp4 = __ldg(f + 4 * s);
         e = -48.0 * (f0 - fp1) + 36.0 * (f0 - fp2) - 16.0 * (f0 - fp3) + 3.0 * (f0 - fp4);
     }
-    r.up = (P)inv12h * (P)e;
-    if (WANT_D2) {
-        const double s1 = (fp1 - f0) + (fm1 - f0), s2 = (fp2 - f0) + (fm2 - f0);
-        r.d2 = (P)inv12h2 * ((P)16.0 * (P)s1 - (P)s2);
-    } else {
-        r.d2 = (P)0;
-    }
+    r.up = (float)inv12h * (float)e;
+    const float t1 = (float)((fp1 - f0) + (fm1 - f0));
+    const float t2 = (float)((fp2 - f0) + (fm2 - f0));
+    r.d2 = WANT_D2 ? (float)inv12h2 * (16.0f * t1 - t2) : 0.0f;
     if (WANT_KO) {
-        const double t1 = (fp1 - f0) + (fm1 - f0);
-        const double t2 = (fp2 - f0) + (fm2 - f0);
-        const double t3 = (fp3 - f0) + (fm3 - f0);
-        // (f-3 + f+3) - 6 (f-2 + f+2) + 15 (f-1 + f+1) - 20 f0 in differences vs f0
-        r.ko = (P)kocf * ((P)t3 - (P)6.0 * (P)t2 + (P)15.0 * (P)t1);
-    } else {
-        r.ko = (P)0;
+        const float t3 = (float)((fp3 - f0) + (fm3 - f0));
+        // (f-3 + f+3) - 6 (f-2 + f+2) + 15 (f-1 + f+1) - 20 f0
+        ko += (float)kocf * (t3 - 6.0f * t2 + 15.0f * t1);
     }
     return r;
 }
 
-// 2nd-order mixed derivative, ccz4.cpp:185-222
+// 2nd-order mixed derivative, ccz4.cpp:185-222: inv4hh * (f++ - f+- - f-+ + f--)
 template <typename P>
-__device__ __forceinline__ P dmix(const double* __restrict__ f, long long sa, long long sb,
-                                  double inv4hh) {
+__device__ __forceinline__ P dmix(const double* __restrict__ f, long long sa, long long sb, double inv4hh);
+
+template <>
+__device__ __forceinline__ double dmix<double>(const double* __restrict__ f, long long sa, long long sb,
+                                               double inv4hh) {
     const double pp = __ldg(f + sa + sb), pm = __ldg(f + sa - sb);
     const double mp = __ldg(f - sa + sb), mm = __ldg(f - sa - sb);
-    return (P)inv4hh * (P)((pp - pm) - (mp - mm));
+    return RN_MUL(inv4hh, RN_ADD(RN_SUB(RN_SUB(pp, pm), mp), mm));
+}
+
+template <>
+__device__ __forceinline__ float dmix<float>(const double* __restrict__ f, long long sa, long long sb,
+                                             double inv4hh) {
+    const double pp = __ldg(f + sa + sb), pm = __ldg(f + sa - sb);
+    const double mp = __ldg(f - sa + sb), mm = __ldg(f - sa - sb);
+    return (float)inv4hh * (float)((pp - pm) - (mp - mm));
 }
 
 // Everything one field contributes: gradient, blended advection, KO, and
@@ -79,31 +139,33 @@ __device__ __forceinline__ P dmix(const double* __restrict__ f, long long sa, lo
 template <typename P>
 struct FieldDer {
     P d[3];
-    P adv;   // w sum beta_d up_d + (1-w) sum beta_d d1_d, ccz4.cpp:567-574
-    P ko;
-    P h[6];  // xx xy xz yy yz zz
+    P adv;  // w sum beta_d up_d + (1-w) sum beta_d d1_d, ccz4.cpp:567-574
+    P ko;   // KO term of the field (added after the rest of its RHS)
+    P h[6]; // xx xy xz yy yz zz
 };
 
-template <typename P, bool HESS>
-__device__ __forceinline__ FieldDer<P> field_der(const DevBlock& B, const double* __restrict__ f,
-                                                 const double beta[3], P w, bool ko_on) {
+template <typename P, bool HESS, bool KO>
+__device__ __forceinline__ FieldDer<P> field_der_t(const DevBlock& B, const double* __restrict__ f,
+                                                   const double beta[3], P w) {
     const long long off[3] = {1, B.tx, (long long)B.tx * B.ty};
     const double f0 = __ldg(f);
     FieldDer<P> r;
-    P up_sum = (P)0, cen_sum = (P)0, ko = (P)0;
+    P up[3];
+    P ko = (P)0;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         AxisDer<P> a;
-        if (ko_on)
-            a = axis_der<P, HESS, true>(f, off[d], f0, beta[d], B.inv12h[d], B.inv12h2[d], B.kocf[d]);
+        if constexpr (sizeof(P) == 8)
+            a = axis_exact<HESS, KO>(f, off[d], f0, beta[d], B.inv12h[d], B.inv12h2[d], B.kow[d], ko);
         else
-            a = axis_der<P, HESS, false>(f, off[d], f0, beta[d], B.inv12h[d], B.inv12h2[d], B.kocf[d]);
+            a = axis_pairs<HESS, KO>(f, off[d], f0, beta[d], B.inv12h[d], B.inv12h2[d], B.kocf[d], ko);
         r.d[d] = a.d1;
-        up_sum += (P)beta[d] * a.up;
-        cen_sum += (P)beta[d] * a.d1;
-        ko += a.ko;
+        up[d] = a.up;
         if (HESS) r.h[d == 0 ? 0 : (d == 1 ? 3 : 5)] = a.d2;
     }
+    const P b0 = (P)beta[0], b1 = (P)beta[1], b2 = (P)beta[2];
+    const P up_sum = b0 * up[0] + b1 * up[1] + b2 * up[2];
+    const P cen_sum = b0 * r.d[0] + b1 * r.d[1] + b2 * r.d[2];
     r.adv = w * up_sum + ((P)1 - w) * cen_sum;
     r.ko = ko;
     if (HESS) {
@@ -115,6 +177,13 @@ __device__ __forceinline__ FieldDer<P> field_der(const DevBlock& B, const double
         for (int a = 0; a < 6; ++a) r.h[a] = (P)0;
     }
     return r;
+}
+
+template <typename P, bool HESS>
+__device__ __forceinline__ FieldDer<P> field_der(const DevBlock& B, const double* __restrict__ f,
+                                                 const double beta[3], P w, bool ko_on) {
+    if (ko_on) return field_der_t<P, HESS, true>(B, f, beta, w);
+    return field_der_t<P, HESS, false>(B, f, beta, w);
 }
 
 __device__ __forceinline__ int sy(int a, int b) {

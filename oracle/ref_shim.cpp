@@ -18,6 +18,7 @@
 #include "ccz4_oracle.h"
 
 #include <cstring>
+#include <iostream>
 #include <memory>
 #include <vector>
 #ifdef _OPENMP
@@ -236,7 +237,11 @@ void ref_fill_level0(const int* n, int ng, const double* lo, const double* hi, d
     }
     sp.ghost_cells = ng;
     amr::AMRHierarchy h(ap, sp);
+    // initialize() prints a level summary to std::cout (amr.cpp:55-57); keep
+    // the caller's stdout clean
+    std::cout.setstate(std::ios_base::failbit);
     h.initialize([](const GridBlock&, int, int, int) { return false; });
+    std::cout.clear();
     GridBlock* b = h.getLevel(0)[0];
     std::memcpy(b->flatBuffer(), u, nbytes(*b));
     h.fillGhostZones(0);
@@ -259,7 +264,11 @@ void ref_rk3_steps(const double* p6, const int* n, int ng, const double* lo, con
     }
     sp.ghost_cells = ng;
     amr::AMRHierarchy h(ap, sp);
+    // initialize() prints a level summary to std::cout (amr.cpp:55-57); keep
+    // the caller's stdout clean
+    std::cout.setstate(std::ios_base::failbit);
     h.initialize([](const GridBlock&, int, int, int) { return false; });
+    std::cout.clear();
     GridBlock& st = *h.getLevel(0)[0];
     std::memcpy(st.flatBuffer(), u, nbytes(st));
     Geo g = geo(n, ng, lo, hi);
