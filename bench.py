@@ -64,9 +64,9 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(workload: str):
+def ncu_traffic(workload: str, kernel: str):
     """dram bytes per stage launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", f"ccz4_stage_kernel_{workload}.md")
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -211,6 +211,8 @@ def main():
     ap.add_argument("--impl", default="granite", choices=["granite", "reference"])
     ap.add_argument("--workload", default="single_puncture_128", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--variant", default="smem", choices=["global", "smem"],
+                    help="stage-kernel variant: stencils from global memory or staged in shared memory")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -237,7 +239,8 @@ def main():
     import granite_b200 as gb
     prec = gb.PRECISION_FP64 if args.precision == "fp64" else gb.PRECISION_MIXED
     block = make_state(gb, w)
-    ev = gb.Evolver(gb.CCZ4Params(device=local))
+    variant = gb.VARIANT_SMEM if args.variant == "smem" else gb.VARIANT_GLOBAL
+    ev = gb.Evolver(gb.CCZ4Params(device=local), variant)
     ev.add_block(block)
     ev.commit()
     ev.upload()
@@ -289,11 +292,13 @@ def main():
     bytes_per_launch = BYTES_PER_POINT_UPDATE * pts / 3.0
     avg_launch_ms = st_ms / max(st_n, 1)
     achieved = bytes_per_launch / (avg_launch_ms / 1000.0) / 1e9
-    traffic = ncu_traffic(args.workload)
+    kname = "ccz4_stage_smem_kernel" if variant == gb.VARIANT_SMEM else "ccz4_stage_kernel"
+    traffic = ncu_traffic(args.workload, kname)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
                 "peak_source": peak_kind,
-                "kernel": "ccz4_stage_kernel", "avg_launch_ms": avg_launch_ms,
+                "kernel": "ccz4_stage_smem_kernel" if variant == gb.VARIANT_SMEM else "ccz4_stage_kernel",
+                "avg_launch_ms": avg_launch_ms,
                 "stage_share_of_step": st_ms / max(st_ms + gh_ms, 1e-12),
                 "algorithmic_bytes_per_launch": bytes_per_launch}
 
@@ -338,7 +343,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if prec == 0 else "f32+f64", "data": "synthetic",
                 "config": {"workload": args.workload, "grid": f"{w['n']}^3", "ghosts": 4,
-                           "fields": NV, "precision": args.precision,
+                           "fields": NV, "precision": args.precision, "kernel_variant": args.variant,
                            "points_per_step": pts, "dt": dt,
                            "l2": f"inputs larger than L2: {3 * state_bytes / 1e9:.2f} GB resident state",
                            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},

@@ -31,6 +31,7 @@ BC_PERIODIC = 1
 AMR_REFERENCE = 0
 AMR_GHOSTS = 1
 KERNEL_STAGE, KERNEL_GHOST, KERNEL_TRANSFER, KERNEL_CONSTRAINTS = 0, 1, 2, 3
+VARIANT_GLOBAL, VARIANT_SMEM = 0, 1
 
 _ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "no sm_100 device", -4: "out of memory",
            -5: "non-finite state", -6: "unsupported", -7: "timeout"}
@@ -99,6 +100,8 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_profile_reset.argtypes = [vp]
     lib.granite_ccz4_profile_get.argtypes = [vp, C.c_int, dp, C.POINTER(C.c_longlong)]
     lib.granite_ccz4_get_stream.argtypes = [vp, C.POINTER(vp)]
+    lib.granite_ccz4_set_kernel_variant.argtypes = [vp, C.c_int]
+    lib.granite_ccz4_get_kernel_variant.argtypes = [vp, C.POINTER(C.c_int)]
     _LIB = lib
     return lib
 
@@ -264,10 +267,13 @@ def _f64(a):
 class CCZ4Evolution:
     """GPU CCZ4 operator with the reference's method names and semantics."""
 
-    def __init__(self, params: CCZ4Params | None = None, precision: int = PRECISION_FP64):
+    def __init__(self, params: CCZ4Params | None = None, precision: int = PRECISION_FP64,
+                 variant: int | None = None):
         self.params_ = params or CCZ4Params()
         self.precision = precision
         self.ctx = _Context(self.params_)
+        if variant is not None:
+            self.ctx.check(self.ctx.lib.granite_ccz4_set_kernel_variant(self.ctx.h, variant))
 
     def params(self):
         return self.params_
@@ -315,11 +321,18 @@ class Evolver:
     add blocks, commit(), upload(), then rk3_step(level, dt) / hierarchy_step(dt).
     """
 
-    def __init__(self, params: CCZ4Params | None = None):
+    def __init__(self, params: CCZ4Params | None = None, variant: int | None = None):
         self.params = params or CCZ4Params()
         self.ctx = _Context(self.params)
         self.blocks: list[GridBlock] = []
         self.committed = False
+        if variant is not None:
+            self.ctx.check(self.ctx.lib.granite_ccz4_set_kernel_variant(self.ctx.h, variant))
+
+    def variant(self) -> int:
+        v = C.c_int()
+        self.ctx.check(self.ctx.lib.granite_ccz4_get_kernel_variant(self.ctx.h, C.byref(v)))
+        return v.value
 
     def add_block(self, b: GridBlock) -> int:
         idx = C.c_int()

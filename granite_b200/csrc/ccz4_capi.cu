@@ -31,8 +31,10 @@ struct Graph {
 
 struct LevelLists {
     std::vector<int> blocks;
-    Tile* d_tiles = nullptr;
+    Tile* d_tiles = nullptr;   // stage-kernel tiles (shape of the context's variant)
     int ntiles = 0;
+    Tile* d_mtiles = nullptr;  // constraint-monitor tiles (variant-0 shape)
+    int nmtiles = 0;
     GhostItem* d_ghost = nullptr;
     int nghost = 0;
     long long interior_points = 0;
@@ -59,6 +61,7 @@ long long cells_of(const granite_block_desc& b) {
 struct Ctx {
     granite_ccz4_params p{};
     int device = 0;
+    int variant = VARIANT_SMEM;  // stage-kernel variant (granite_ccz4_set_kernel_variant)
     cudaStream_t stream = nullptr;
     std::string err;
     long long launches = 0;
@@ -153,9 +156,9 @@ DevBlock make_devblock(const granite_block_desc& b, double sigma) {
     return d;
 }
 
-void tiles_of(int block, const granite_block_desc& b, std::vector<Tile>& out) {
+void tiles_of(int block, const granite_block_desc& b, std::vector<Tile>& out, int variant) {
     int TX, TY, TZ;
-    stage_tile_dims(&TX, &TY, &TZ);
+    stage_tile_dims(variant, &TX, &TY, &TZ);
     for (int k = 0; k < b.ncells[2]; k += TZ)
         for (int j = 0; j < b.ncells[1]; j += TY)
             for (int i = 0; i < b.ncells[0]; i += TX) out.push_back(Tile{block, i, j, k});
@@ -211,9 +214,9 @@ int ensure_scratch(Ctx* c, size_t cells, int ntiles) {
 }
 
 // Stage one block into the stateless scratch: descriptor + tile list.
-int stage_single(Ctx* c, const granite_block_desc* b, double* u_dev, int* ntiles, cudaStream_t s) {
+int stage_single(Ctx* c, const granite_block_desc* b, double* u_dev, int* ntiles, cudaStream_t s, int variant) {
     std::vector<Tile> t;
-    tiles_of(0, *b, t);
+    tiles_of(0, *b, t, variant);
     int r = ensure_scratch(c, (size_t)cells_of(*b), (int)t.size());
     if (r) return r;
     DevBlock d = make_devblock(*b, c->p.ko_sigma);
@@ -301,6 +304,22 @@ int granite_ccz4_profile_get(void* h, int cls, double* ms, long long* n) {
     return GRANITE_OK;
 }
 
+int granite_ccz4_set_kernel_variant(void* h, int variant) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (variant < 0 || variant >= NUM_VARIANTS) return fail(c, GRANITE_ERR_INVALID, "unknown kernel variant");
+    if (c->committed) return fail(c, GRANITE_ERR_INVALID, "set the kernel variant before commit");
+    c->variant = variant;
+    return GRANITE_OK;
+}
+
+int granite_ccz4_get_kernel_variant(const void* h, int* variant) {
+    const Ctx* c = static_cast<const Ctx*>(h);
+    if (!c || !variant) return GRANITE_ERR_INVALID;
+    *variant = c->variant;
+    return GRANITE_OK;
+}
+
 int granite_ccz4_get_stream(void* h, void** stream) {
     Ctx* c = static_cast<Ctx*>(h);
     if (!c || !stream) return GRANITE_ERR_INVALID;
@@ -340,6 +359,7 @@ int granite_ccz4_create(const granite_ccz4_params* p, void** out) {
     c->p = *p;
     c->device = p->device;
     cudaError_t e = cudaSetDevice(c->device);
+    if (e == cudaSuccess) e = configure_stage_kernels();
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_nonfinite, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(c->d_nonfinite, 0, sizeof(unsigned long long));
@@ -367,6 +387,7 @@ int granite_ccz4_destroy(void* h) {
     for (auto e : c->event_pool) cudaEventDestroy(e);
     for (auto& L : c->levels) {
         cudaFree(L.d_tiles);
+        cudaFree(L.d_mtiles);
         cudaFree(L.d_ghost);
     }
     cudaFree(c->d_blocks);
@@ -435,7 +456,7 @@ int granite_ccz4_compute_rhs_device(void* h, const granite_block_desc* b, const 
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     CK(cudaSetDevice(c->device), "cudaSetDevice");
     int nt = 0;
-    if ((r = stage_single(c, b, const_cast<double*>(u_dev), &nt, s))) return r;
+    if ((r = stage_single(c, b, const_cast<double*>(u_dev), &nt, s, c->variant))) return r;
     StageArgs a = base_args(c);
     a.in_sel = 0;
     a.rhs = rhs_dev;
@@ -443,7 +464,7 @@ int granite_ccz4_compute_rhs_device(void* h, const granite_block_desc* b, const 
     a.Si = Si;
     a.Sij = Sij;
     a.S = S;
-    CK(launch_stage(precision, EPI_STORE, c->s_desc, c->s_tiles, nt, a, s), "launch RHS");
+    CK(launch_stage(c->variant, precision, EPI_STORE, c->s_desc, c->s_tiles, nt, a, s), "launch RHS");
     c->launches += 1;
     return GRANITE_OK;
 }
@@ -461,7 +482,7 @@ int granite_ccz4_compute_rhs_host(void* h, const granite_block_desc* b, const do
     CK(cudaSetDevice(c->device), "cudaSetDevice");
     const size_t N = (size_t)cells_of(*b);
     std::vector<Tile> t;
-    tiles_of(0, *b, t);
+    tiles_of(0, *b, t, VARIANT_GLOBAL);
     if ((r = ensure_scratch(c, N, (int)t.size()))) return r;
     cudaStream_t s = c->stream;
     CK(cudaMemcpyAsync(c->s_u, u, N * NV * sizeof(double), cudaMemcpyHostToDevice, s), "H2D u");
@@ -496,7 +517,7 @@ int granite_ccz4_apply_dissipation_host(void* h, const granite_block_desc* b, co
     const size_t N = (size_t)cells_of(*b);
     cudaStream_t s = c->stream;
     int nt = 0;
-    if ((r = stage_single(c, b, nullptr, &nt, s))) return r;
+    if ((r = stage_single(c, b, nullptr, &nt, s, VARIANT_GLOBAL))) return r;
     CK(cudaMemcpyAsync(c->s_u, u, N * NV * sizeof(double), cudaMemcpyHostToDevice, s), "H2D u");
     CK(cudaMemcpyAsync(c->s_rhs, rhs, N * NV * sizeof(double), cudaMemcpyHostToDevice, s), "H2D rhs");
     CK(launch_dissipation(c->s_desc, 0, c->s_rhs, nt, c->s_tiles, s), "launch KO");
@@ -517,7 +538,7 @@ int granite_ccz4_compute_constraints_host(void* h, const granite_block_desc* b, 
     const size_t N = (size_t)cells_of(*b);
     cudaStream_t s = c->stream;
     int nt = 0;
-    if ((r = stage_single(c, b, nullptr, &nt, s))) return r;
+    if ((r = stage_single(c, b, nullptr, &nt, s, VARIANT_GLOBAL))) return r;
     CK(cudaMemcpyAsync(c->s_u, u, N * NV * sizeof(double), cudaMemcpyHostToDevice, s), "H2D u");
     // ham in s_rhs[0:N], mom in s_rhs[N:4N]; ghosts zero (ccz4.cpp:945-946)
     CK(cudaMemsetAsync(c->s_rhs, 0, 4 * N * sizeof(double), s), "memset");
@@ -587,23 +608,26 @@ int granite_ccz4_commit(void* h) {
     c->levels.assign(maxlev + 1, LevelLists());
     c->level_ghosts_valid.assign(maxlev + 1, false);
     for (int L = 0; L <= maxlev; ++L) {
-        std::vector<Tile> tiles;
+        std::vector<Tile> tiles, mtiles;
         std::vector<GhostItem> ghosts;
         LevelLists& ll = c->levels[L];
         for (size_t i = 0; i < c->descs.size(); ++i) {
             if (c->descs[i].level != L) continue;
             ll.blocks.push_back((int)i);
-            tiles_of((int)i, c->descs[i], tiles);
+            tiles_of((int)i, c->descs[i], tiles, c->variant);
+            tiles_of((int)i, c->descs[i], mtiles, VARIANT_GLOBAL);
             ghost_chunks_of((int)i, c->descs[i], ghosts);
             ll.interior_points += (long long)c->descs[i].ncells[0] * c->descs[i].ncells[1] * c->descs[i].ncells[2];
         }
         CK(upload_vec(tiles, &ll.d_tiles, c->stream), "upload tiles");
+        CK(upload_vec(mtiles, &ll.d_mtiles, c->stream), "upload monitor tiles");
+        ll.nmtiles = (int)mtiles.size();
         CK(upload_vec(ghosts, &ll.d_ghost, c->stream), "upload ghost chunks");
         ll.ntiles = (int)tiles.size();
         ll.nghost = (int)ghosts.size();
     }
     int maxt = 0;
-    for (auto& L : c->levels) maxt = std::max(maxt, L.ntiles);
+    for (auto& L : c->levels) maxt = std::max(maxt, std::max(L.ntiles, L.nmtiles));
     int r = ensure_scratch(c, 1, std::max(1, maxt));
     if (r) return r;
     c->committed = true;
@@ -665,17 +689,17 @@ static cudaError_t enqueue_level_step(Ctx* c, int level, double dt, int precisio
     // stage 1: u1 = u + dt L(u)                       main.cpp:673
     a.in_sel = 0; a.n_sel = 0; a.out_sel = 1; a.final_stage = 0;
     a.a1 = 1.0; a.a2 = 0.0; a.a3dt = 1.0 * dt;
-    if ((e = timed(c, GRANITE_KERNEL_STAGE, [&] { return launch_stage(precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, s); }))) return e;
+    if ((e = timed(c, GRANITE_KERNEL_STAGE, [&] { return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, s); }))) return e;
     if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(outer_mode, c->d_blocks, L.d_ghost, L.nghost, 1, s); }))) return e;
     // stage 2: u2 = 3/4 u + 1/4 u1 + 1/4 dt L(u1)      main.cpp:679
     a.in_sel = 1; a.n_sel = 0; a.out_sel = 2;
     a.a1 = 0.75; a.a2 = 0.25; a.a3dt = 0.25 * dt;
-    if ((e = timed(c, GRANITE_KERNEL_STAGE, [&] { return launch_stage(precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, s); }))) return e;
+    if ((e = timed(c, GRANITE_KERNEL_STAGE, [&] { return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, s); }))) return e;
     if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(outer_mode, c->d_blocks, L.d_ghost, L.nghost, 2, s); }))) return e;
     // stage 3: u = 1/3 u + 2/3 u2 + 2/3 dt L(u2), floors, det/trace   main.cpp:685-687
     a.in_sel = 2; a.n_sel = 0; a.out_sel = 0; a.final_stage = 1;
     a.a1 = 1.0 / 3.0; a.a2 = 2.0 / 3.0; a.a3dt = (2.0 / 3.0) * dt;
-    if ((e = timed(c, GRANITE_KERNEL_STAGE, [&] { return launch_stage(precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, s); }))) return e;
+    if ((e = timed(c, GRANITE_KERNEL_STAGE, [&] { return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, s); }))) return e;
     // main.cpp:689 outer BC on u is overwritten by the level fill of amr.cpp:329,
     // so only the level fill runs.
     if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(level_mode, c->d_blocks, L.d_ghost, L.nghost, 0, s); }))) return e;
@@ -751,9 +775,9 @@ int granite_ccz4_constraint_norms(void* h, int level, double* h_l2, double* m_l2
         if (level >= 0 && L != level) continue;
         LevelLists& ll = c->levels[L];
         if (ll.ntiles == 0) continue;
-        CK(launch_constraints(c->d_blocks, ll.d_tiles, ll.ntiles, 0, nullptr, nullptr, c->s_partials, c->stream),
+        CK(launch_constraints(c->d_blocks, ll.d_mtiles, ll.nmtiles, 0, nullptr, nullptr, c->s_partials, c->stream),
            "launch constraints");
-        CK(launch_sum_partials(c->s_partials, ll.ntiles, c->s_sum, c->stream), "launch sum");
+        CK(launch_sum_partials(c->s_partials, ll.nmtiles, c->s_sum, c->stream), "launch sum");
         c->launches += 2;
         double hs[2];
         CK(cudaMemcpyAsync(hs, c->s_sum, sizeof(hs), cudaMemcpyDeviceToHost, c->stream), "D2H sums");

@@ -9,12 +9,20 @@ namespace granite_b200 {
 
 enum { EPI_STORE = 0, EPI_RK = 1 };
 
-// Tile shape of the fused RHS kernel (points per CTA along x, y, z).
-int stage_tile_dims(int* tx, int* ty, int* tz);
+// Kernel variants of the fused stage: 0 = stencils from global memory
+// (32x4x1 tiles), 1 = fields staged through shared memory with cp.async
+// (16x4x2 tiles). The constraint and KO kernels always use variant-0 tiles.
+enum { VARIANT_GLOBAL = 0, VARIANT_SMEM = 1, NUM_VARIANTS = 2 };
+
+// Tile shape of a stage-kernel variant (points per CTA along x, y, z).
+int stage_tile_dims(int variant, int* tx, int* ty, int* tz);
+
+// Per-device kernel attributes (shared-memory opt-in); call with the device current.
+cudaError_t configure_stage_kernels();
 
 // Fused RHS (+KO) over a tile work-list. precision: 0 = FP64, 1 = mixed.
-cudaError_t launch_stage(int precision, int epi, const DevBlock* blocks, const Tile* tiles,
-                         int ntiles, const StageArgs& args, cudaStream_t stream);
+cudaError_t launch_stage(int variant, int precision, int epi, const DevBlock* blocks,
+                         const Tile* tiles, int ntiles, const StageArgs& args, cudaStream_t stream);
 
 // KO dissipation only: rhs += KO(u) at interior points of one block.
 cudaError_t launch_dissipation(const DevBlock* block, int in_sel, double* rhs, int ntiles,

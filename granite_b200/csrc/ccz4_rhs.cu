@@ -33,11 +33,129 @@ namespace {
 constexpr double PI_D = 3.14159265358979323846;
 
 // ---------------------------------------------------------------------------
+// Sources of per-field stencil results. ccz4_point asks for the fields in one
+// fixed order (FIELD_ORDER); a source may rely on that order.
+// ---------------------------------------------------------------------------
+__device__ constexpr int FIELD_ORDER[NV] = {GXX, GXY, GXZ, GYY, GYZ, GZZ, GHX, GHY, GHZ, CHI, ALPHA,
+                                            BETAX, BETAY, BETAZ, KTR, THETA, AXX, AXY, AXZ, AYY, AYZ, AZZ};
+
+// Stencils read straight from global memory (through L1).
+template <typename P>
+struct GlobalSource {
+    const DevBlock& B;
+    const double* __restrict__ u;
+    long long c;
+    bool ko;
+    template <bool HESS>
+    __device__ __forceinline__ FieldDer<P> der(int v, const double beta[3], P w) {
+        return field_der<P, HESS>(B, u + (long long)v * B.stride + c, beta, w, ko);
+    }
+};
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Tile staging geometry: a TX x TY x TZ tile of points plus the cells its
+// stencils touch (the tile grown by 1 in every direction for the mixed
+// derivatives, and arms of 3 more cells along each axis for the +-4 reach),
+// laid out in shared memory as a (TX+8) x (TY+8) x (TZ+8) box.
+template <int TX, int TY, int TZ>
+struct TileGeom {
+    static constexpr int BX = TX + 8, BY = TY + 8, BZ = TZ + 8;
+    static constexpr int BOX = BX * BY * BZ;
+    static constexpr int N_CORE = (TX + 2) * (TY + 2) * (TZ + 2);
+    static constexpr int N_XARM = 6 * TY * TZ, N_YARM = 6 * TX * TZ, N_ZARM = 6 * TX * TY;
+    static constexpr int NLOAD = N_CORE + N_XARM + N_YARM + N_ZARM;
+    // cell q of the load list -> offset (rx, ry, rz) from the tile origin
+    __device__ static void cell(int q, int& rx, int& ry, int& rz) {
+        constexpr int ARM[6] = {-4, -3, -2, 1, 2, 3};
+        if (q < N_CORE) {
+            rx = q % (TX + 2) - 1;
+            ry = (q / (TX + 2)) % (TY + 2) - 1;
+            rz = q / ((TX + 2) * (TY + 2)) - 1;
+            return;
+        }
+        q -= N_CORE;
+        if (q < N_XARM) {
+            const int a = q % 6;
+            rx = a < 3 ? ARM[a] : TX + ARM[a];
+            ry = (q / 6) % TY;
+            rz = q / (6 * TY);
+            return;
+        }
+        q -= N_XARM;
+        if (q < N_YARM) {
+            const int a = (q / TX) % 6;
+            rx = q % TX;
+            ry = a < 3 ? ARM[a] : TY + ARM[a];
+            rz = q / (6 * TX);
+            return;
+        }
+        q -= N_YARM;
+        const int a = q / (TX * TY);
+        rx = q % TX;
+        ry = (q / TX) % TY;
+        rz = a < 3 ? ARM[a] : TZ + ARM[a];
+    }
+};
+
+// Stencils read from a CTA-staged shared-memory tile. Fields are copied in
+// FIELD_ORDER with cp.async into NBUF rotating buffers, NBUF-1 fields ahead of
+// the one being differentiated, so the copies of the next fields overlap the
+// algebra of the current one. Every thread of the CTA must call der() for
+// every field in order (the calls carry the CTA barrier).
+template <typename P, int TX, int TY, int TZ, int NBUF>
+struct SmemSource {
+    using G = TileGeom<TX, TY, TZ>;
+    const DevBlock& B;
+    const double* __restrict__ u;  // stencil buffer (global)
+    double* sm;                    // NBUF x BOX doubles
+    const int2* table;             // NLOAD x {smem offset or -1, global offset from the tile origin}
+    long long origin;              // global cell index of the tile origin
+    int lin;                       // shared offset of this thread's point in a box
+    int next;                      // index in FIELD_ORDER of the next field to consume
+    bool ko;
+
+    __device__ __forceinline__ void issue(int k) {
+        if (k < NV) {
+            double* dst = sm + (k % NBUF) * G::BOX;
+            const double* src = u + (long long)FIELD_ORDER[k] * B.stride + origin;
+            for (int q = threadIdx.x; q < G::NLOAD; q += TX * TY * TZ) {
+                const int2 e = table[q];
+                if (e.x >= 0) cp_async8(dst + e.x, src + e.y);
+            }
+        }
+        cp_async_commit();
+    }
+    __device__ __forceinline__ void start() {
+        for (int k = 0; k < NBUF - 1; ++k) issue(k);
+    }
+    template <bool HESS>
+    __device__ __forceinline__ FieldDer<P> der(int /*v*/, const double beta[3], P w) {
+        cp_async_wait<NBUF - 2>();
+        __syncthreads();
+        issue(next + NBUF - 1);
+        const long long off[3] = {1, G::BX, G::BX * G::BY};
+        const SharedLoad L{sm + (next % NBUF) * G::BOX + lin};
+        ++next;
+        if (ko) return field_der_l<P, HESS, true>(B, L, off, beta, w);
+        return field_der_l<P, HESS, false>(B, L, off, beta, w);
+    }
+};
+
+// ---------------------------------------------------------------------------
 // RHS at one interior point. Returns L(u) for the 22 fields in `out` (FP64).
 // ---------------------------------------------------------------------------
-template <typename P>
+template <typename P, typename Src>
 __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __restrict__ u,
-                                           long long c, const StageArgs& A, double out[NV]) {
+                                           long long c, const StageArgs& A, Src& S, double out[NV]) {
     const long long st = B.stride;
     const double* __restrict__ uc = u + c;
 #define FP(v) (uc + (long long)(v) * st)
@@ -72,7 +190,6 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
         gtud[5] = (gtd[0] * gtd[3] - gtd[1] * gtd[1]) * inv;
     }
     const P w = (P)(0.5 * (1.0 + tanh((chi - A.chi_c) / A.chi_w)));  // :565
-    const bool ko = A.ko_on != 0;
     const P alpha = (P)alpha_d, K = (P)K_d, Theta = (P)Th_d;
     P gt[6], At[6], gtu[6], Gh[3];
 #pragma unroll
@@ -90,7 +207,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     P agt[6], kgt[6];  // advection and KO of gt
 #pragma unroll
     for (int a = 0; a < 6; ++a) {
-        FieldDer<P> fd = field_der<P, true>(B, FP(GXX + a), beta, w, ko);
+        FieldDer<P> fd = S.template der<true>(GXX + a, beta, w);
 #pragma unroll
         for (int d = 0; d < 3; ++d) dg[a][d] = fd.d[d];
         // term 1: -1/2 gtu^{lm} d_l d_m gt_ij
@@ -127,7 +244,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     P aGh[3], kGh[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        FieldDer<P> fd = field_der<P, false>(B, FP(GHX + a), beta, w, ko);
+        FieldDer<P> fd = S.template der<false>(GHX + a, beta, w);
 #pragma unroll
         for (int d = 0; d < 3; ++d) dGh[a][d] = fd.d[d];
         aGh[a] = fd.adv;
@@ -166,7 +283,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     }
 
     // ---- chi: Ricci chi-part (ccz4.cpp:518-541) -----------------------------
-    FieldDer<P> fchi = field_der<P, true>(B, FP(CHI), beta, w, ko);
+    FieldDer<P> fchi = S.template der<true>(CHI, beta, w);
     const P chiP = (P)chi;
     // 0.5/(chi+1e-30) and 0.25/(chi^2+1e-30) in FP64 (small chi near the puncture)
     const P c_half = (P)(0.5 / (chi + 1e-30));
@@ -200,7 +317,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     Rs *= chiP;
 
     // ---- lapse -------------------------------------------------------------
-    FieldDer<P> fal = field_der<P, true>(B, FP(ALPHA), beta, w, ko);
+    FieldDer<P> fal = S.template der<true>(ALPHA, beta, w);
     P DDa[6];
 #pragma unroll
     for (int ij = 0; ij < 6; ++ij)
@@ -222,7 +339,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     for (int d = 0; d < 3; ++d) ddiv[d] = (P)0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        FieldDer<P> fb = field_der<P, true>(B, FP(BETAX + a), beta, w, ko);
+        FieldDer<P> fb = S.template der<true>(BETAX + a, beta, w);
 #pragma unroll
         for (int d = 0; d < 3; ++d) db[a][d] = fb.d[d];
         T5[a] = gtu[0] * fb.h[0] + gtu[3] * fb.h[3] + gtu[5] * fb.h[5] +
@@ -277,7 +394,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
         }
     // K (ccz4.cpp:650-652)
     {
-        FieldDer<P> fK = field_der<P, false>(B, FP(KTR), beta, w, ko);
+        FieldDer<P> fK = S.template der<false>(KTR, beta, w);
         const P k1 = (P)A.kappa1, k2 = (P)A.kappa2;
         out[KTR] = (double)((-phys_lap_alpha + alpha * (AtAt + K * K / (P)3) + (P)4 * PI * alpha * (rho + Str) +
                             k1 * ((P)1 - k2) * alpha * Theta + fK.adv) + fK.ko);
@@ -303,7 +420,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     }
     // Theta (ccz4.cpp:662-665)
     {
-        FieldDer<P> fT = field_der<P, false>(B, FP(THETA), beta, w, ko);
+        FieldDer<P> fT = S.template der<false>(THETA, beta, w);
         const P k1 = (P)A.kappa1, k2 = (P)A.kappa2;
         out[THETA] = (double)(((P)0.5 * alpha * (Rs - AtAt + (P)2 * K * K / (P)3 - (P)16 * PI * rho) -
                               alpha * k1 * ((P)2 + k2) * Theta + fT.adv) + fT.ko);
@@ -317,7 +434,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
 #pragma unroll
             for (int j = i; j < 3; ++j) {
                 const int ij = sy(i, j);
-                FieldDer<P> fA = field_der<P, false>(B, FP(AXX + ij), beta, w, ko);
+                FieldDer<P> fA = S.template der<false>(AXX + ij, beta, w);
                 koA[ij] = fA.ko;
                 const P t1 = chiP * (-DDa[ij] + alpha * (Ric[ij] - (P)8 * PI * Sij[ij]));
                 const P Asq = At[sy(i, 0)] * Am[0][j] + At[sy(i, 1)] * Am[1][j] + At[sy(i, 2)] * Am[2][j];
@@ -386,23 +503,16 @@ __device__ __forceinline__ double rk_combine(double a1, double un, double a2, do
 
 }  // namespace
 
-template <typename P, int EPI, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TX* TY* TZ)
-    ccz4_stage_kernel(const DevBlock* __restrict__ blocks, const Tile* __restrict__ tiles, StageArgs A) {
-    const Tile t = tiles[blockIdx.x];
-    const DevBlock& B = blocks[t.block];
-    const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y, k = t.k0 + threadIdx.z;
-    if (i >= B.n[0] || j >= B.n[1] || k >= B.n[2]) return;
-    const long long c = cell_index(B, i + NG, j + NG, k + NG);
-    const double* __restrict__ uin = B.buf[A.in_sel];
-    double L[NV];
-    ccz4_point<P>(B, uin, c, A, L);
+// Shared epilogue: store L, or RK combine + floors (+ algebraic constraints).
+template <int EPI>
+__device__ __forceinline__ void stage_epilogue(const DevBlock& B, const StageArgs& A, long long c, const double L[NV]) {
     const long long st = B.stride;
     if (EPI == EPI_STORE) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) A.rhs[(long long)v * st + c] = L[v];
         return;
     }
+    const double* __restrict__ uin = B.buf[A.in_sel];
     const double* __restrict__ un = B.buf[A.n_sel];
     double* __restrict__ out = B.buf[A.out_sel];
     double r[NV];
@@ -426,41 +536,129 @@ __global__ void __launch_bounds__(TX* TY* TZ)
     for (int v = 0; v < NV; ++v) out[(long long)v * st + c] = r[v];
 }
 
+// Variant 0: stencils from global memory, one thread per point.
+template <typename P, int EPI, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(TX* TY* TZ)
+    ccz4_stage_kernel(const DevBlock* __restrict__ blocks, const Tile* __restrict__ tiles, StageArgs A) {
+    const Tile t = tiles[blockIdx.x];
+    const DevBlock& B = blocks[t.block];
+    const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y, k = t.k0 + threadIdx.z;
+    if (i >= B.n[0] || j >= B.n[1] || k >= B.n[2]) return;
+    const long long c = cell_index(B, i + NG, j + NG, k + NG);
+    const double* __restrict__ uin = B.buf[A.in_sel];
+    GlobalSource<P> S{B, uin, c, A.ko_on != 0};
+    double L[NV];
+    ccz4_point<P>(B, uin, c, A, S, L);
+    stage_epilogue<EPI>(B, A, c, L);
+}
+
+// Variant 1: every field of the tile (with its stencil halo) staged through
+// shared memory by cp.async, NBUF-1 fields ahead of the computation.
+template <typename P, int EPI, int TX, int TY, int TZ, int NBUF>
+__global__ void __launch_bounds__(TX* TY* TZ, 2)
+    ccz4_stage_smem_kernel(const DevBlock* __restrict__ blocks, const Tile* __restrict__ tiles, StageArgs A) {
+    using G = TileGeom<TX, TY, TZ>;
+    constexpr int NT = TX * TY * TZ;
+    extern __shared__ __align__(16) double smem[];
+    int2* table = reinterpret_cast<int2*>(smem + NBUF * G::BOX);
+    const Tile t = tiles[blockIdx.x];
+    const DevBlock& B = blocks[t.block];
+    const int tid = threadIdx.x;
+    const int lx = tid % TX, ly = (tid / TX) % TY, lz = tid / (TX * TY);
+    const int i = t.i0 + lx, j = t.j0 + ly, k = t.k0 + lz;
+    const bool valid = i < B.n[0] && j < B.n[1] && k < B.n[2];
+    // load list of this tile: shared offset (or -1 outside the block) and global offset
+    const int gi0 = t.i0 + NG, gj0 = t.j0 + NG, gk0 = t.k0 + NG;
+    const int row = B.tx, plane = B.tx * B.ty;
+    for (int q = tid; q < G::NLOAD; q += NT) {
+        int rx, ry, rz;
+        G::cell(q, rx, ry, rz);
+        const bool in = gi0 + rx < B.tx && gj0 + ry < B.ty && gk0 + rz < B.tz;
+        table[q] = make_int2(in ? (rx + 4) + G::BX * ((ry + 4) + G::BY * (rz + 4)) : -1, rx + row * ry + plane * rz);
+    }
+    __syncthreads();
+    const double* __restrict__ uin = B.buf[A.in_sel];
+    SmemSource<P, TX, TY, TZ, NBUF> S{B, uin, smem, table, cell_index(B, gi0, gj0, gk0),
+                                      (lx + 4) + G::BX * ((ly + 4) + G::BY * (lz + 4)), 0, A.ko_on != 0};
+    S.start();
+    // pointwise loads of threads outside the block use a valid cell; their results are dropped
+    const int ic = i < B.n[0] ? i : B.n[0] - 1, jc = j < B.n[1] ? j : B.n[1] - 1, kc = k < B.n[2] ? k : B.n[2] - 1;
+    const long long c = cell_index(B, ic + NG, jc + NG, kc + NG);
+    double L[NV];
+    ccz4_point<P>(B, uin, c, A, S, L);
+    if (!valid) return;  // no barrier follows the last field
+    stage_epilogue<EPI>(B, A, c, L);
+}
+
 // ---------------------------------------------------------------------------
 // Launchers
 // ---------------------------------------------------------------------------
-#define GRANITE_TILE_X 32
-#define GRANITE_TILE_Y 4
-#define GRANITE_TILE_Z 1
+constexpr int V0_TX = 32, V0_TY = 4, V0_TZ = 1;
+constexpr int V1_TX = 16, V1_TY = 4, V1_TZ = 2, V1_NBUF = 3;
 
-int stage_tile_dims(int* tx, int* ty, int* tz) {
-    *tx = GRANITE_TILE_X;
-    *ty = GRANITE_TILE_Y;
-    *tz = GRANITE_TILE_Z;
+int stage_tile_dims(int variant, int* tx, int* ty, int* tz) {
+    if (variant == 1) {
+        *tx = V1_TX;
+        *ty = V1_TY;
+        *tz = V1_TZ;
+    } else {
+        *tx = V0_TX;
+        *ty = V0_TY;
+        *tz = V0_TZ;
+    }
     return 0;
 }
 
-cudaError_t launch_stage(int precision, int epi, const DevBlock* blocks, const Tile* tiles, int ntiles,
+template <typename P, int EPI>
+static cudaError_t launch_smem(const DevBlock* blocks, const Tile* tiles, int ntiles, const StageArgs& args,
+                               cudaStream_t stream) {
+    using G = TileGeom<V1_TX, V1_TY, V1_TZ>;
+    constexpr size_t bytes = V1_NBUF * G::BOX * sizeof(double) + G::NLOAD * sizeof(int2);
+    auto k = ccz4_stage_smem_kernel<P, EPI, V1_TX, V1_TY, V1_TZ, V1_NBUF>;
+    k<<<ntiles, V1_TX * V1_TY * V1_TZ, bytes, stream>>>(blocks, tiles, args);
+    return cudaGetLastError();
+}
+
+template <typename P, int EPI>
+static cudaError_t configure_smem() {
+    using G = TileGeom<V1_TX, V1_TY, V1_TZ>;
+    constexpr size_t bytes = V1_NBUF * G::BOX * sizeof(double) + G::NLOAD * sizeof(int2);
+    return cudaFuncSetAttribute(ccz4_stage_smem_kernel<P, EPI, V1_TX, V1_TY, V1_TZ, V1_NBUF>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// Opt the shared-memory variants into more than 48 KB of dynamic shared memory
+// on the current device (called once per context at creation).
+cudaError_t configure_stage_kernels() {
+    cudaError_t e;
+    if ((e = configure_smem<double, EPI_STORE>())) return e;
+    if ((e = configure_smem<double, EPI_RK>())) return e;
+    if ((e = configure_smem<float, EPI_STORE>())) return e;
+    return configure_smem<float, EPI_RK>();
+}
+
+template <typename P, int EPI>
+static cudaError_t launch_global(const DevBlock* blocks, const Tile* tiles, int ntiles, const StageArgs& args,
+                                 cudaStream_t stream) {
+    ccz4_stage_kernel<P, EPI, V0_TX, V0_TY, V0_TZ><<<ntiles, dim3(V0_TX, V0_TY, V0_TZ), 0, stream>>>(blocks, tiles, args);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stage(int variant, int precision, int epi, const DevBlock* blocks, const Tile* tiles, int ntiles,
                          const StageArgs& args, cudaStream_t stream) {
     if (ntiles <= 0) return cudaSuccess;
-    dim3 blk(GRANITE_TILE_X, GRANITE_TILE_Y, GRANITE_TILE_Z);
-    dim3 grd(ntiles);
-    if (precision == 0) {
-        if (epi == EPI_STORE)
-            ccz4_stage_kernel<double, EPI_STORE, GRANITE_TILE_X, GRANITE_TILE_Y, GRANITE_TILE_Z>
-                <<<grd, blk, 0, stream>>>(blocks, tiles, args);
-        else
-            ccz4_stage_kernel<double, EPI_RK, GRANITE_TILE_X, GRANITE_TILE_Y, GRANITE_TILE_Z>
-                <<<grd, blk, 0, stream>>>(blocks, tiles, args);
-    } else {
-        if (epi == EPI_STORE)
-            ccz4_stage_kernel<float, EPI_STORE, GRANITE_TILE_X, GRANITE_TILE_Y, GRANITE_TILE_Z>
-                <<<grd, blk, 0, stream>>>(blocks, tiles, args);
-        else
-            ccz4_stage_kernel<float, EPI_RK, GRANITE_TILE_X, GRANITE_TILE_Y, GRANITE_TILE_Z>
-                <<<grd, blk, 0, stream>>>(blocks, tiles, args);
+    if (variant == 1) {
+        if (precision == 0)
+            return epi == EPI_STORE ? launch_smem<double, EPI_STORE>(blocks, tiles, ntiles, args, stream)
+                                    : launch_smem<double, EPI_RK>(blocks, tiles, ntiles, args, stream);
+        return epi == EPI_STORE ? launch_smem<float, EPI_STORE>(blocks, tiles, ntiles, args, stream)
+                                : launch_smem<float, EPI_RK>(blocks, tiles, ntiles, args, stream);
     }
-    return cudaGetLastError();
+    if (precision == 0)
+        return epi == EPI_STORE ? launch_global<double, EPI_STORE>(blocks, tiles, ntiles, args, stream)
+                                : launch_global<double, EPI_RK>(blocks, tiles, ntiles, args, stream);
+    return epi == EPI_STORE ? launch_global<float, EPI_STORE>(blocks, tiles, ntiles, args, stream)
+                            : launch_global<float, EPI_RK>(blocks, tiles, ntiles, args, stream);
 }
 
 
@@ -492,8 +690,7 @@ __global__ void __launch_bounds__(128)
 cudaError_t launch_dissipation(const DevBlock* block, int in_sel, double* rhs, int ntiles, const Tile* tiles,
                                cudaStream_t stream) {
     if (ntiles <= 0) return cudaSuccess;
-    dim3 blk(GRANITE_TILE_X, GRANITE_TILE_Y, GRANITE_TILE_Z);
-    ko_kernel<<<ntiles, blk, 0, stream>>>(block, tiles, in_sel, rhs);
+    ko_kernel<<<ntiles, dim3(V0_TX, V0_TY, V0_TZ), 0, stream>>>(block, tiles, in_sel, rhs);
     return cudaGetLastError();
 }
 

@@ -25,6 +25,16 @@ namespace {
 #define RN_ADD __dadd_rn
 #define RN_SUB __dsub_rn
 
+// Value loaders: offset (in cells) from a centre pointer.
+struct GlobalLoad {  // read-only global memory through the non-coherent path
+    const double* __restrict__ p;
+    __device__ __forceinline__ double operator()(long long o) const { return __ldg(p + o); }
+};
+struct SharedLoad {  // a CTA-staged tile in shared memory
+    const double* p;
+    __device__ __forceinline__ double operator()(long long o) const { return p[o]; }
+};
+
 template <typename P>
 struct AxisDer {
     P d1;  // 4th-order centred first derivative, ccz4.cpp:71-99
@@ -34,26 +44,26 @@ struct AxisDer {
 
 // Reference-order evaluation (P = double). `ko` accumulates the KO sum across
 // the three axes exactly as ccz4.cpp:912-926 does.
-template <bool WANT_D2, bool WANT_KO>
-__device__ __forceinline__ AxisDer<double> axis_exact(const double* __restrict__ f, long long s, double f0,
+template <bool WANT_D2, bool WANT_KO, typename L>
+__device__ __forceinline__ AxisDer<double> axis_exact(const L& f, long long s, double f0,
                                                      double beta, double inv12h, double inv12h2,
                                                      const double* kw, double& ko) {
-    const double fm1 = __ldg(f - s), fp1 = __ldg(f + s);
-    const double fm2 = __ldg(f - 2 * s), fp2 = __ldg(f + 2 * s);
+    const double fm1 = f(-s), fp1 = f(s);
+    const double fm2 = f(-2 * s), fp2 = f(2 * s);
     AxisDer<double> r;
     // inv12h * (-f[+2] + 8 f[+1] - 8 f[-1] + f[-2])
     r.d1 = RN_MUL(inv12h, RN_ADD(RN_SUB(RN_ADD(-fp2, RN_MUL(8.0, fp1)), RN_MUL(8.0, fm1)), fm2));
     double fm3 = 0.0, fp3 = 0.0;
-    if (WANT_KO || beta >= 0.0) fm3 = __ldg(f - 3 * s);
-    if (WANT_KO || !(beta >= 0.0)) fp3 = __ldg(f + 3 * s);
+    if (WANT_KO || beta >= 0.0) fm3 = f(-3 * s);
+    if (WANT_KO || !(beta >= 0.0)) fp3 = f(3 * s);
     if (beta >= 0.0) {
-        const double fm4 = __ldg(f - 4 * s);
+        const double fm4 = f(-4 * s);
         // inv12h * (25 f0 - 48 f-1 + 36 f-2 - 16 f-3 + 3 f-4)
         r.up = RN_MUL(inv12h, RN_ADD(RN_SUB(RN_ADD(RN_SUB(RN_MUL(25.0, f0), RN_MUL(48.0, fm1)), RN_MUL(36.0, fm2)),
                                             RN_MUL(16.0, fm3)),
                                      RN_MUL(3.0, fm4)));
     } else {
-        const double fp4 = __ldg(f + 4 * s);
+        const double fp4 = f(4 * s);
         // inv12h * (-25 f0 + 48 f+1 - 36 f+2 + 16 f+3 - 3 f+4)
         r.up = RN_MUL(inv12h, RN_SUB(RN_ADD(RN_SUB(RN_ADD(RN_MUL(-25.0, f0), RN_MUL(48.0, fp1)), RN_MUL(36.0, fp2)),
                                             RN_MUL(16.0, fp3)),
@@ -81,25 +91,25 @@ __device__ __forceinline__ AxisDer<double> axis_exact(const double* __restrict__
 }
 
 // Pair-difference evaluation (P = float).
-template <bool WANT_D2, bool WANT_KO>
-__device__ __forceinline__ AxisDer<float> axis_pairs(const double* __restrict__ f, long long s, double f0,
+template <bool WANT_D2, bool WANT_KO, typename L>
+__device__ __forceinline__ AxisDer<float> axis_pairs(const L& f, long long s, double f0,
                                                     double beta, double inv12h, double inv12h2, double kocf,
                                                     float& ko) {
-    const double fm1 = __ldg(f - s), fp1 = __ldg(f + s);
-    const double fm2 = __ldg(f - 2 * s), fp2 = __ldg(f + 2 * s);
+    const double fm1 = f(-s), fp1 = f(s);
+    const double fm2 = f(-2 * s), fp2 = f(2 * s);
     AxisDer<float> r;
     const float a1 = (float)(fp1 - fm1), a2 = (float)(fp2 - fm2);
     r.d1 = (float)inv12h * (8.0f * a1 - a2);
     double e;
     double fm3 = 0.0, fp3 = 0.0;
-    if (WANT_KO || beta >= 0.0) fm3 = __ldg(f - 3 * s);
-    if (WANT_KO || !(beta >= 0.0)) fp3 = __ldg(f + 3 * s);
+    if (WANT_KO || beta >= 0.0) fm3 = f(-3 * s);
+    if (WANT_KO || !(beta >= 0.0)) fp3 = f(3 * s);
     if (beta >= 0.0) {
-        const double fm4 = __ldg(f - 4 * s);
+        const double fm4 = f(-4 * s);
         // 25 f0 - 48 f-1 + 36 f-2 - 16 f-3 + 3 f-4 with weights summing to zero
         e = 48.0 * (f0 - fm1) - 36.0 * (f0 - fm2) + 16.0 * (f0 - fm3) - 3.0 * (f0 - fm4);
     } else {
-        const double fp4 = __ldg(f + 4 * s);
+        const double fp4 = f(4 * s);
         e = -48.0 * (f0 - fp1) + 36.0 * (f0 - fp2) - 16.0 * (f0 - fp3) + 3.0 * (f0 - fp4);
     }
     r.up = (float)inv12h * (float)e;
@@ -115,23 +125,14 @@ __device__ __forceinline__ AxisDer<float> axis_pairs(const double* __restrict__ 
 }
 
 // 2nd-order mixed derivative, ccz4.cpp:185-222: inv4hh * (f++ - f+- - f-+ + f--)
-template <typename P>
-__device__ __forceinline__ P dmix(const double* __restrict__ f, long long sa, long long sb, double inv4hh);
-
-template <>
-__device__ __forceinline__ double dmix<double>(const double* __restrict__ f, long long sa, long long sb,
-                                               double inv4hh) {
-    const double pp = __ldg(f + sa + sb), pm = __ldg(f + sa - sb);
-    const double mp = __ldg(f - sa + sb), mm = __ldg(f - sa - sb);
-    return RN_MUL(inv4hh, RN_ADD(RN_SUB(RN_SUB(pp, pm), mp), mm));
-}
-
-template <>
-__device__ __forceinline__ float dmix<float>(const double* __restrict__ f, long long sa, long long sb,
-                                             double inv4hh) {
-    const double pp = __ldg(f + sa + sb), pm = __ldg(f + sa - sb);
-    const double mp = __ldg(f - sa + sb), mm = __ldg(f - sa - sb);
-    return (float)inv4hh * (float)((pp - pm) - (mp - mm));
+template <typename P, typename L>
+__device__ __forceinline__ P dmix(const L& f, long long sa, long long sb, double inv4hh) {
+    const double pp = f(sa + sb), pm = f(sa - sb);
+    const double mp = f(-sa + sb), mm = f(-sa - sb);
+    if constexpr (sizeof(P) == 8)
+        return RN_MUL(inv4hh, RN_ADD(RN_SUB(RN_SUB(pp, pm), mp), mm));
+    else
+        return (float)inv4hh * (float)((pp - pm) - (mp - mm));
 }
 
 // Everything one field contributes: gradient, blended advection, KO, and
@@ -144,11 +145,10 @@ struct FieldDer {
     P h[6]; // xx xy xz yy yz zz
 };
 
-template <typename P, bool HESS, bool KO>
-__device__ __forceinline__ FieldDer<P> field_der_t(const DevBlock& B, const double* __restrict__ f,
+template <typename P, bool HESS, bool KO, typename L>
+__device__ __forceinline__ FieldDer<P> field_der_l(const DevBlock& B, const L& f, const long long off[3],
                                                    const double beta[3], P w) {
-    const long long off[3] = {1, B.tx, (long long)B.tx * B.ty};
-    const double f0 = __ldg(f);
+    const double f0 = f(0);
     FieldDer<P> r;
     P up[3];
     P ko = (P)0;
@@ -169,9 +169,9 @@ __device__ __forceinline__ FieldDer<P> field_der_t(const DevBlock& B, const doub
     r.adv = w * up_sum + ((P)1 - w) * cen_sum;
     r.ko = ko;
     if (HESS) {
-        r.h[1] = dmix<P>(f, off[0], off[1], B.inv4hh[0]);
-        r.h[2] = dmix<P>(f, off[0], off[2], B.inv4hh[1]);
-        r.h[4] = dmix<P>(f, off[1], off[2], B.inv4hh[2]);
+        r.h[1] = dmix<P, L>(f, off[0], off[1], B.inv4hh[0]);
+        r.h[2] = dmix<P, L>(f, off[0], off[2], B.inv4hh[1]);
+        r.h[4] = dmix<P, L>(f, off[1], off[2], B.inv4hh[2]);
     } else {
 #pragma unroll
         for (int a = 0; a < 6; ++a) r.h[a] = (P)0;
@@ -179,11 +179,14 @@ __device__ __forceinline__ FieldDer<P> field_der_t(const DevBlock& B, const doub
     return r;
 }
 
+// Field derivatives straight from global memory.
 template <typename P, bool HESS>
 __device__ __forceinline__ FieldDer<P> field_der(const DevBlock& B, const double* __restrict__ f,
                                                  const double beta[3], P w, bool ko_on) {
-    if (ko_on) return field_der_t<P, HESS, true>(B, f, beta, w);
-    return field_der_t<P, HESS, false>(B, f, beta, w);
+    const long long off[3] = {1, B.tx, (long long)B.tx * B.ty};
+    const GlobalLoad L{f};
+    if (ko_on) return field_der_l<P, HESS, true>(B, L, off, beta, w);
+    return field_der_l<P, HESS, false>(B, L, off, beta, w);
 }
 
 __device__ __forceinline__ int sy(int a, int b) {

@@ -197,6 +197,15 @@ GRANITE_API int granite_ccz4_set_profiling(void* ctx, int enabled);
 GRANITE_API int granite_ccz4_profile_reset(void* ctx);
 GRANITE_API int granite_ccz4_profile_get(void* ctx, int kernel_class, double* total_ms,
                                          long long* launches);
+/* Stage-kernel variant (set before granite_ccz4_commit; no counterpart in the
+ * reference): GRANITE_VARIANT_GLOBAL reads stencils from global memory through
+ * L1 (32x4x1 tiles); GRANITE_VARIANT_SMEM stages every field of a 16x4x2 tile
+ * and its halo through shared memory with cp.async (the default). */
+#define GRANITE_VARIANT_GLOBAL 0
+#define GRANITE_VARIANT_SMEM 1
+GRANITE_API int granite_ccz4_set_kernel_variant(void* ctx, int variant);
+GRANITE_API int granite_ccz4_get_kernel_variant(const void* ctx, int* variant);
+
 /* The context's cudaStream_t, for callers that order their own work or events
  * against the library's. */
 GRANITE_API int granite_ccz4_get_stream(void* ctx, void** stream);

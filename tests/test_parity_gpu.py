@@ -75,22 +75,26 @@ def gb():
     return granite_b200
 
 
-def evo(gb, p: Params, precision=0):
+VARIANTS = [0, 1]  # stencils from global memory / staged through shared memory
+
+
+def evo(gb, p: Params, precision=0, variant=None):
     return gb.CCZ4Evolution(gb.CCZ4Params(kappa1=p.kappa1, kappa2=p.kappa2, eta=p.eta,
                                           ko_sigma=p.ko_sigma, chi_blend_center=p.chi_blend_center,
-                                          chi_blend_width=p.chi_blend_width), precision)
+                                          chi_blend_width=p.chi_blend_width), precision, variant)
 
 
 # ---------------------------------------------------------------------------
 # single RHS evaluations
 # ---------------------------------------------------------------------------
 
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("name,ko", [("rhs_random", 0.1), ("rhs_random_noko", 0.0)])
-def test_rhs_golden(gb, name, ko):
+def test_rhs_golden(gb, name, ko, variant):
     g, z = load(name)
     u = oracle.seeded_state(g, int(z["seed"]))
     rhs = block_of(g)
-    evo(gb, Params(ko_sigma=ko)).computeRHSVacuum(block_of(g, u), rhs)
+    evo(gb, Params(ko_sigma=ko), variant=variant).computeRHSVacuum(block_of(g, u), rhs)
     parity(rhs.array[g.interior()], z["rhs"], what=name)
 
 
@@ -103,25 +107,27 @@ def test_rhs_matter_golden(gb):
     parity(rhs.array[g.interior()], z["rhs"], what="matter")
 
 
-def test_rhs_bl_golden(gb):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_rhs_bl_golden(gb, variant):
     g, z = load("rhs_bl")
     o = oracle.Oracle()
     u = o.init_brill_lindquist(g, [0.5, 0.5], [[0.7, 0.1, -0.05], [-0.8, -0.05, 0.1]])
     u = u + 1e-6 * oracle.hash_noise(g.shape, int(z["seed"]))
     rhs = block_of(g)
-    evo(gb, Params()).computeRHSVacuum(block_of(g, u), rhs)
+    evo(gb, Params(), variant=variant).computeRHSVacuum(block_of(g, u), rhs)
     parity(rhs.array[g.interior()], z["rhs"], what="bl")
 
 
-@pytest.mark.parametrize("seed,n", [(1, (33, 17, 9)), (2, (16, 16, 16)), (3, (40, 8, 12))])
-def test_rhs_random_vs_oracle(gb, oracle_lib, seed, n):
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("seed,n", [(1, (33, 17, 9)), (2, (16, 16, 16)), (3, (40, 8, 12)), (4, (5, 7, 6))])
+def test_rhs_random_vs_oracle(gb, oracle_lib, seed, n, variant):
     # uneven, non-cubic blocks (partial tiles), shifts of both signs, strong gradients
     g = Geom(n, (-1.3, -0.7, -2.0), (1.1, 0.9, -0.2))
     u = oracle.seeded_state(g, seed, amp=0.2, noise=1e-2)
     p = Params(kappa1=0.05, kappa2=0.1, eta=1.5, ko_sigma=0.3)
     ref = oracle_lib.rhs(p, g, u)
     rhs = block_of(g)
-    evo(gb, p).computeRHSVacuum(block_of(g, u), rhs)
+    evo(gb, p, variant=variant).computeRHSVacuum(block_of(g, u), rhs)
     parity(rhs.array[g.interior()], ref[g.interior()], what=f"seed {seed}")
     # ghosts of rhs are untouched (the reference writes interior cells only)
     mask = np.ones(g.shape[1:], bool)
@@ -129,7 +135,8 @@ def test_rhs_random_vs_oracle(gb, oracle_lib, seed, n):
     assert np.all(rhs.array[:, mask] == 0.0)
 
 
-def test_rhs_puncture_vs_oracle(gb, oracle_lib):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_rhs_puncture_vs_oracle(gb, oracle_lib, variant):
     # chi through the blend window and the 1e-4 clamp near the puncture
     g = Geom((24, 20, 16), (-1.5, -1.25, -1.0), (1.5, 1.25, 1.0))
     u = oracle_lib.init_brill_lindquist(g, [1.0], [[0.01, 0.02, -0.015]])
@@ -137,7 +144,7 @@ def test_rhs_puncture_vs_oracle(gb, oracle_lib):
     u[19] += 0.3 * oracle.hash_noise(g.shape[1:], 4)  # beta^x of both signs
     ref = oracle_lib.rhs(Params(), g, u)
     rhs = block_of(g)
-    evo(gb, Params()).computeRHSVacuum(block_of(g, u), rhs)
+    evo(gb, Params(), variant=variant).computeRHSVacuum(block_of(g, u), rhs)
     parity(rhs.array[g.interior()], ref[g.interior()], what="puncture")
 
 
@@ -235,8 +242,9 @@ def test_reference_suite_gauge_wave(gb):
 # fused RK3 steps against the oracle driver
 # ---------------------------------------------------------------------------
 
-def run_steps(gb, g: Geom, u, p: Params, dt, nsteps, bc, precision=0):
-    ev = gb.Evolver(gb.CCZ4Params(kappa1=p.kappa1, kappa2=p.kappa2, eta=p.eta, ko_sigma=p.ko_sigma))
+def run_steps(gb, g: Geom, u, p: Params, dt, nsteps, bc, precision=0, variant=None):
+    ev = gb.Evolver(gb.CCZ4Params(kappa1=p.kappa1, kappa2=p.kappa2, eta=p.eta, ko_sigma=p.ko_sigma),
+                    variant)
     b = block_of(g, u)
     ev.add_block(b)
     ev.commit()
@@ -247,12 +255,14 @@ def run_steps(gb, g: Geom, u, p: Params, dt, nsteps, bc, precision=0):
     return b.array, ev
 
 
-def test_rk3_golden_bl(gb):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_rk3_golden_bl(gb, variant):
     g, z = load("rk3_bl_3steps")
     o = oracle.Oracle()
     u = o.init_brill_lindquist(g, [0.5, 0.5], [[0.7, 0.1, -0.05], [-0.8, -0.05, 0.1]])
     u = u + 1e-6 * oracle.hash_noise(g.shape, int(z["seed"]))
-    out, _ = run_steps(gb, g, u, Params(), float(z["dt"]), int(z["nsteps"]), gb.BC_REFERENCE)
+    out, _ = run_steps(gb, g, u, Params(), float(z["dt"]), int(z["nsteps"]), gb.BC_REFERENCE,
+                       variant=variant)
     parity(out[g.interior()], z["u"], rtol=1e-11, what="rk3 bl")
 
 
@@ -264,7 +274,8 @@ def test_rk3_golden_gauge_wave_periodic(gb):
     parity(out[g.interior()], z["u"], rtol=1e-11, what="rk3 gauge wave")
 
 
-def test_rk3_single_puncture_vs_oracle(gb, oracle_lib):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_rk3_single_puncture_vs_oracle(gb, oracle_lib, variant):
     # the single-puncture workload at reduced size: 32^3 on [-16,16]^3, 20 steps
     g = Geom((32, 32, 32), (-16.0, -16.0, -16.0), (16.0, 16.0, 16.0))
     u = oracle_lib.init_brill_lindquist(g, [1.0], [[0.0, 0.0, 0.0]], r_floor=0.5 * g.dx[0])
@@ -272,7 +283,7 @@ def test_rk3_single_puncture_vs_oracle(gb, oracle_lib):
     dt = 0.25 * g.dx[0]
     n = 20
     ref = oracle_lib.rk3_steps(Params(), g, u, dt, n)
-    out, ev = run_steps(gb, g, u, Params(), dt, n, gb.BC_REFERENCE)
+    out, ev = run_steps(gb, g, u, Params(), dt, n, gb.BC_REFERENCE, variant=variant)
     parity(out[g.interior()], ref[g.interior()], rtol=1e-10, what="puncture 20 steps")
     # whole block including ghosts (level fill of the last step)
     parity(out, ref, rtol=1e-10, what="puncture ghosts")
