@@ -6,6 +6,9 @@
 // main.cpp:1216-1254 are sqrt(sum H^2 / N) over interior points; each CTA
 // writes its partial sums, and a single-CTA kernel adds the partials in a
 // fixed order, so the result does not depend on scheduling.
+#include <mutex>
+
+#include "../../include/granite_ccz4.h"
 #include "ccz4_common.cuh"
 #include "ccz4_kernels.h"
 #include "ccz4_stencil.cuh"
@@ -258,4 +261,137 @@ cudaError_t launch_sum_partials(const double* partials, int n, double* out, cuda
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Constraint norms without any allocation (granite_ccz4_constraint_norms_noalloc)
+//
+// For callers that cannot allocate device memory themselves (see the header):
+// the per-tile partial sums live in a fixed file-scope device array instead of
+// context-owned scratch, the block descriptor travels as a kernel argument,
+// and the tiles are derived from the grid instead of a device-side work-list.
+// ---------------------------------------------------------------------------
+
+// Capacity: one (sum H^2, sum |M|^2) pair per 32x4x1 tile of interior points.
+constexpr int NOALLOC_MAX_TILES = 65536;  // 1 MiB; up to 8,388,608 interior points per call
+static __device__ __align__(256) double g_noalloc_partials[2 * NOALLOC_MAX_TILES];
+
+namespace {
+
+__global__ void __launch_bounds__(CT_X* CT_Y)
+    constraints_noalloc_kernel(DevBlock B, const double* __restrict__ u, int ntx, int nty, double* partials) {
+    // tile index -> (i0, j0, k0) in the same order as the host work-lists (x fastest)
+    const int t = blockIdx.x;
+    const int i0 = (t % ntx) * CT_X, j0 = ((t / ntx) % nty) * CT_Y, k0 = t / (ntx * nty);
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y, k = k0;
+    double h2 = 0.0, m2 = 0.0;
+    if (i < B.n[0] && j < B.n[1] && k < B.n[2]) {
+        const long long c = cell_index(B, i + NG, j + NG, k + NG);
+        double H, M[3];
+        constraint_point(B, u, c, H, M);
+        h2 = H * H;
+        m2 = M[0] * M[0] + M[1] * M[1] + M[2] * M[2];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        h2 += __shfl_down_sync(0xffffffffu, h2, o);
+        m2 += __shfl_down_sync(0xffffffffu, m2, o);
+    }
+    __shared__ double sh[2][CT_X * CT_Y / 32];
+    const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+    const int warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
+    if (lane == 0) {
+        sh[0][warp] = h2;
+        sh[1][warp] = m2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < CT_X * CT_Y / 32; ++w) {
+            a += sh[0][w];
+            b += sh[1][w];
+        }
+        partials[2 * blockIdx.x] = a;
+        partials[2 * blockIdx.x + 1] = b;
+    }
+}
+
+// Fixed-order sum of the partials (same tree as sum_partials_kernel), then the
+// RMS norms of main.cpp:1216-1254: norms[0] = sqrt(sum H^2 / N), norms[1] = sqrt(sum |M|^2 / N).
+__global__ void noalloc_norms_kernel(const double* __restrict__ p, int n, double npts, double* norms) {
+    __shared__ double sa[256], sb[256];
+    double a = 0.0, b = 0.0;
+    for (int x = threadIdx.x; x < n; x += blockDim.x) {
+        a += p[2 * x];
+        b += p[2 * x + 1];
+    }
+    sa[threadIdx.x] = a;
+    sb[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            sa[threadIdx.x] += sa[threadIdx.x + s];
+            sb[threadIdx.x] += sb[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        norms[0] = sqrt(sa[0] / npts);
+        norms[1] = sqrt(sb[0] / npts);
+    }
+}
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+double* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};  // device address of g_noalloc_partials per device
+std::mutex g_noalloc_mutex;
+
+}  // namespace
+
 }  // namespace granite_b200
+
+extern "C" GRANITE_API int granite_ccz4_constraint_norms_noalloc(const granite_block_desc* b, const double* u_dev,
+                                                                  double* norms_dev, void* stream) {
+    using namespace granite_b200;
+    if (!b || !u_dev || !norms_dev) return GRANITE_ERR_INVALID;
+    if (b->nghost != NG) return GRANITE_ERR_INVALID;
+    for (int d = 0; d < 3; ++d)
+        if (b->ncells[d] < NG || !(b->hi[d] > b->lo[d])) return GRANITE_ERR_INVALID;
+    const int ntx = (b->ncells[0] + CT_X - 1) / CT_X, nty = (b->ncells[1] + CT_Y - 1) / CT_Y;
+    const long long ntiles = (long long)ntx * nty * b->ncells[2];
+    if (ntiles > NOALLOC_MAX_TILES) return GRANITE_ERR_TOO_LARGE;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return GRANITE_ERR_NO_DEVICE;
+    double* partials = nullptr;
+    {
+        // once per device, with that device current: host code must not use the
+        // array's name as a device address
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_addr[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) {
+                cudaGetLastError();
+                return GRANITE_ERR_CUDA;
+            }
+            g_noalloc_addr[dev] = static_cast<double*>(p);
+        }
+        partials = g_noalloc_addr[dev];
+    }
+    DevBlock B{};
+    for (int d = 0; d < 3; ++d) B.n[d] = b->ncells[d];
+    B.tx = b->ncells[0] + 2 * NG;
+    B.ty = b->ncells[1] + 2 * NG;
+    B.tz = b->ncells[2] + 2 * NG;
+    B.stride = (long long)B.tx * B.ty * B.tz;
+    for (int d = 0; d < 3; ++d) {
+        B.lo[d] = b->lo[d];
+        B.dx[d] = (b->hi[d] - b->lo[d]) / static_cast<double>(b->ncells[d]);  // grid.cpp:20-22
+        B.inv12h[d] = 1.0 / (12.0 * B.dx[d]);
+        B.inv12h2[d] = 1.0 / (12.0 * B.dx[d] * B.dx[d]);
+    }
+    B.inv4hh[0] = 1.0 / (4.0 * B.dx[0] * B.dx[1]);
+    B.inv4hh[1] = 1.0 / (4.0 * B.dx[0] * B.dx[2]);
+    B.inv4hh[2] = 1.0 / (4.0 * B.dx[1] * B.dx[2]);
+    B.level = b->level;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    constraints_noalloc_kernel<<<(unsigned)ntiles, dim3(CT_X, CT_Y, 1), 0, s>>>(B, u_dev, ntx, nty, partials);
+    const double npts = (double)b->ncells[0] * b->ncells[1] * b->ncells[2];
+    noalloc_norms_kernel<<<1, 256, 0, s>>>(partials, (int)ntiles, npts, norms_dev);
+    return cudaGetLastError() == cudaSuccess ? GRANITE_OK : GRANITE_ERR_CUDA;
+}

@@ -54,6 +54,7 @@ extern "C" {
 #define GRANITE_ERR_NONFINITE (-5)   /* non-finite values detected in the evolved state */
 #define GRANITE_ERR_UNSUPPORTED (-6) /* option the library does not implement */
 #define GRANITE_ERR_TIMEOUT (-7)     /* a bounded host-side wait gave up */
+#define GRANITE_ERR_TOO_LARGE (-8)   /* request exceeds a fixed capacity of the library */
 
 /* arithmetic of the RHS algebra */
 #define GRANITE_PRECISION_FP64 0  /* plain FP64 throughout */
@@ -213,6 +214,33 @@ GRANITE_API int granite_ccz4_get_stream(void* ctx, void** stream);
 /* Kernel launches issued by this context so far (graph nodes count once per
  * replay). */
 GRANITE_API int granite_ccz4_launch_count(const void* ctx, long long* count);
+
+/* ---- allocation-free constraint norms --------------------------------------- */
+
+/* No counterpart in the reference. ||H||_2 and ||M||_2 (the same norms as
+ * granite_ccz4_constraint_norms) of ONE block whose state u_dev (GridBlock
+ * layout, 22 fields) already sits in device memory, for callers that cannot
+ * allocate device memory themselves: code running inside another runtime's
+ * memory pool or a pre-sized arena, or code that must not call cudaMalloc /
+ * cudaFree because those calls synchronise the device and would stall work in
+ * flight on other streams. It needs no context and allocates nothing: its
+ * scratch (one pair of partial sums per 32x4x1 tile of interior points) is a
+ * fixed 1 MiB array in the library's device data, held by every GPU that loads
+ * the library until the process exits.
+ *   - Limit: at most 65,536 tiles, i.e. ceil(nx/32) * ceil(ny/4) * nz <= 65536
+ *     (8,388,608 interior points for tile-aligned blocks); larger blocks return
+ *     GRANITE_ERR_TOO_LARGE and launch nothing.
+ *   - norms_dev: caller-owned device memory for 2 doubles; written by the last
+ *     kernel of the call. Work is enqueued on `stream` (a cudaStream_t; NULL =
+ *     the legacy default stream) of the current device; nothing is synchronised.
+ *   - The first call on a device looks up the array's device address on that
+ *     device (it must be the current device); make that first call before any
+ *     stream capture.
+ *   - Every call shares the one array: calls whose kernels may overlap on the
+ *     GPU (other streams, other host threads) race on it. Each call rewrites
+ *     every partial it reads, so nothing needs clearing between calls. */
+GRANITE_API int granite_ccz4_constraint_norms_noalloc(const granite_block_desc* b, const double* u_dev,
+                                                      double* norms_dev, void* stream);
 
 #ifdef __cplusplus
 }
