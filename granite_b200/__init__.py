@@ -416,3 +416,5 @@ class Evolver:
 
 from .initial_data import (  # noqa: E402
     brill_lindquist, gauge_wave, set_flat_spacetime, set_gauge_wave_data)
+from .hierarchy import (  # noqa: E402,F401
+    Hierarchy, block_states, make_binary_hierarchy, make_hierarchy, make_triple_hierarchy)

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -38,6 +39,28 @@ struct LevelLists {
     GhostItem* d_ghost = nullptr;
     int nghost = 0;
     long long interior_points = 0;
+};
+
+// Device copy of a list of transfer boxes and the chunks that cover them.
+struct XferList {
+    XferBox* d_boxes = nullptr;
+    BoxChunk* d_chunks = nullptr;
+    int nchunks = 0;
+    int nboxes = 0;
+};
+
+void free_xfer(XferList& x) {
+    cudaFree(x.d_boxes);
+    cudaFree(x.d_chunks);
+    x = XferList();
+}
+
+// Inter-level / inter-block transfer lists of one level for one AMR mode.
+struct LevelXfer {
+    XferList prolong;               // into this level from level-1 (ghost slabs, or whole blocks)
+    XferList copy;                  // same-level ghost exchange (GRANITE_AMR_GHOSTS)
+    std::vector<XferList> restrict_;  // into this level from level+1; one list per launch
+    unsigned char* d_facemask = nullptr;  // faces left to the zero-gradient fill (REFERENCE)
 };
 
 // device copy of a host vector (nullptr for an empty one)
@@ -89,6 +112,11 @@ struct Ctx {
     std::vector<LevelLists> levels;
     std::vector<bool> level_ghosts_valid;
     std::map<std::tuple<int, int, int, unsigned long long, int>, Graph> graphs;
+    // hierarchy transfer lists per AMR mode (built on first use), and graphs
+    // of whole subcycled coarse steps keyed by (precision, mode, dt bits)
+    std::vector<LevelXfer> xfer[2];
+    bool xfer_built[2] = {false, false};
+    std::map<std::tuple<int, int, unsigned long long>, Graph> hgraphs;
 
     // profiler: pending (class, start, stop) event pairs and per-class totals
     bool profiling = false;
@@ -390,6 +418,15 @@ int granite_ccz4_destroy(void* h) {
         cudaFree(L.d_mtiles);
         cudaFree(L.d_ghost);
     }
+    for (auto& kv : c->hgraphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    for (auto& mode : c->xfer)
+        for (auto& X : mode) {
+            free_xfer(X.prolong);
+            free_xfer(X.copy);
+            for (auto& r : X.restrict_) free_xfer(r);
+            cudaFree(X.d_facemask);
+        }
     cudaFree(c->d_blocks);
     cudaFree(c->arena);
     cudaFree(c->s_u);
@@ -682,7 +719,7 @@ static cudaError_t enqueue_level_step(Ctx* c, int level, double dt, int precisio
     long long n = 0;
     // amr.cpp:319 level fill before the step (only when the state changed since the last one)
     if (prefill) {
-        if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(level_mode, c->d_blocks, L.d_ghost, L.nghost, 0, s); }))) return e;
+        if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(level_mode, c->d_blocks, L.d_ghost, L.nghost, 0, nullptr, s); }))) return e;
         ++n;
     }
     StageArgs a = base_args(c);
@@ -690,19 +727,19 @@ static cudaError_t enqueue_level_step(Ctx* c, int level, double dt, int precisio
     a.in_sel = 0; a.n_sel = 0; a.out_sel = 1; a.final_stage = 0;
     a.a1 = 1.0; a.a2 = 0.0; a.a3dt = 1.0 * dt;
     if ((e = timed(c, GRANITE_KERNEL_STAGE, [&] { return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, s); }))) return e;
-    if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(outer_mode, c->d_blocks, L.d_ghost, L.nghost, 1, s); }))) return e;
+    if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(outer_mode, c->d_blocks, L.d_ghost, L.nghost, 1, nullptr, s); }))) return e;
     // stage 2: u2 = 3/4 u + 1/4 u1 + 1/4 dt L(u1)      main.cpp:679
     a.in_sel = 1; a.n_sel = 0; a.out_sel = 2;
     a.a1 = 0.75; a.a2 = 0.25; a.a3dt = 0.25 * dt;
     if ((e = timed(c, GRANITE_KERNEL_STAGE, [&] { return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, s); }))) return e;
-    if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(outer_mode, c->d_blocks, L.d_ghost, L.nghost, 2, s); }))) return e;
+    if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(outer_mode, c->d_blocks, L.d_ghost, L.nghost, 2, nullptr, s); }))) return e;
     // stage 3: u = 1/3 u + 2/3 u2 + 2/3 dt L(u2), floors, det/trace   main.cpp:685-687
     a.in_sel = 2; a.n_sel = 0; a.out_sel = 0; a.final_stage = 1;
     a.a1 = 1.0 / 3.0; a.a2 = 2.0 / 3.0; a.a3dt = (2.0 / 3.0) * dt;
     if ((e = timed(c, GRANITE_KERNEL_STAGE, [&] { return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, s); }))) return e;
     // main.cpp:689 outer BC on u is overwritten by the level fill of amr.cpp:329,
     // so only the level fill runs.
-    if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(level_mode, c->d_blocks, L.d_ghost, L.nghost, 0, s); }))) return e;
+    if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(level_mode, c->d_blocks, L.d_ghost, L.nghost, 0, nullptr, s); }))) return e;
     n += 6;
     *nl = n;
     return cudaSuccess;
@@ -753,13 +790,415 @@ int granite_ccz4_rk3_step(void* h, int level, double dt, int precision, int bc) 
     return GRANITE_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Berger-Oliger hierarchy (amr.cpp:303-350)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct Interval {
+    int lo, hi;  // [lo, hi)
+    bool empty() const { return hi <= lo; }
+};
+Interval meet(Interval a, Interval b) { return {std::max(a.lo, b.lo), std::min(a.hi, b.hi)}; }
+
+// Reference cell centre, grid.hpp:92-94.
+double xref(const granite_block_desc& b, int d, int idx) {
+    const double dx = (b.hi[d] - b.lo[d]) / static_cast<double>(b.ncells[d]);
+    return b.lo[d] + (static_cast<double>(idx) - b.nghost + 0.5) * dx;
+}
+
+cudaError_t upload_xfer(const std::vector<XferBox>& boxes, XferList& out, cudaStream_t s) {
+    std::vector<BoxChunk> chunks;
+    for (int b = 0; b < (int)boxes.size(); ++b) {
+        const long long n = (long long)boxes[b].n[0] * boxes[b].n[1] * boxes[b].n[2];
+        for (long long r = 0; r < n; r += XFER_CHUNK) chunks.push_back(BoxChunk{b, (int)r});
+    }
+    cudaError_t e = upload_vec(boxes, &out.d_boxes, s);
+    if (e != cudaSuccess) return e;
+    e = upload_vec(chunks, &out.d_chunks, s);
+    out.nboxes = (int)boxes.size();
+    out.nchunks = (int)chunks.size();
+    return e;
+}
+
+// Global cell index of every block's first interior cell on its level's grid
+// (origin: the lower corner of level 0), for the aligned-grid transfers of
+// GRANITE_AMR_GHOSTS. Fails when a level's blocks do not share one spacing, a
+// level is not twice as fine as its parent, or a block is off the grid.
+int level_grid(Ctx* c, std::vector<std::array<int, 3>>& G) {
+    const int nb = (int)c->descs.size();
+    G.assign(nb, {0, 0, 0});
+    double X0[3] = {1e300, 1e300, 1e300};
+    for (int i : c->levels[0].blocks)
+        for (int d = 0; d < 3; ++d) X0[d] = std::min(X0[d], c->descs[i].lo[d]);
+    std::vector<std::array<double, 3>> dxl(c->levels.size());
+    for (size_t L = 0; L < c->levels.size(); ++L) {
+        const auto& first = c->hblocks[c->levels[L].blocks[0]];
+        for (int d = 0; d < 3; ++d) dxl[L][d] = first.dx[d];
+        for (int i : c->levels[L].blocks)
+            for (int d = 0; d < 3; ++d) {
+                if (std::fabs(c->hblocks[i].dx[d] - dxl[L][d]) > 1e-12 * dxl[L][d])
+                    return fail(c, GRANITE_ERR_UNSUPPORTED, "blocks of one level must share one cell spacing");
+                const double g = (c->descs[i].lo[d] - X0[d]) / dxl[L][d];
+                const double gr = std::round(g);
+                if (std::fabs(g - gr) > 1e-6)
+                    return fail(c, GRANITE_ERR_UNSUPPORTED, "block corner is not on its level's cell grid");
+                G[i][d] = (int)gr;
+            }
+        if (L > 0)
+            for (int d = 0; d < 3; ++d)
+                if (std::fabs(dxl[L - 1][d] - 2.0 * dxl[L][d]) > 1e-12 * dxl[L - 1][d])
+                    return fail(c, GRANITE_ERR_UNSUPPORTED, "refinement ratio must be 2");
+    }
+    return GRANITE_OK;
+}
+
+// Transfer lists for GRANITE_AMR_GHOSTS: ghost slabs of every fine block filled
+// from the coarse blocks covering them, then overwritten by same-level
+// neighbours where one covers the cell; coarse cells whose 2x2x2 children lie
+// in a fine interior are restricted.
+int build_ghosts_mode(Ctx* c) {
+    std::vector<std::array<int, 3>> G;
+    int r = level_grid(c, G);
+    if (r) return r;
+    auto& X = c->xfer[GRANITE_AMR_GHOSTS];
+    X.assign(c->levels.size(), LevelXfer());
+    for (size_t L = 0; L < c->levels.size(); ++L) {
+        const auto& blocks = c->levels[L].blocks;
+        // same-level copies
+        std::vector<XferBox> copies;
+        for (int a : blocks)
+            for (int b : blocks) {
+                if (a == b) continue;
+                XferBox x{};
+                bool ok = true;
+                for (int d = 0; d < 3; ++d) {
+                    const Interval full{G[a][d] - NG, G[a][d] + c->descs[a].ncells[d] + NG};
+                    const Interval inb{G[b][d], G[b][d] + c->descs[b].ncells[d]};
+                    const Interval m = meet(full, inb);
+                    if (m.empty()) {
+                        ok = false;
+                        break;
+                    }
+                    x.d0[d] = m.lo - (G[a][d] - NG);
+                    x.s0[d] = m.lo - (G[b][d] - NG);
+                    x.n[d] = m.hi - m.lo;
+                }
+                if (!ok) continue;
+                x.dst = a;
+                x.src = b;
+                copies.push_back(x);
+            }
+        CK(upload_xfer(copies, X[L].copy, c->stream), "upload copy boxes");
+        if (L == 0) continue;
+        // prolongation into the six ghost slabs of each fine block
+        std::vector<XferBox> pro;
+        for (int f : blocks) {
+            const auto& fd = c->descs[f];
+            Interval full[3], in[3];
+            for (int d = 0; d < 3; ++d) {
+                full[d] = {G[f][d] - NG, G[f][d] + fd.ncells[d] + NG};
+                in[d] = {G[f][d], G[f][d] + fd.ncells[d]};
+            }
+            const Interval lo_s[3] = {{full[0].lo, in[0].lo}, {full[1].lo, in[1].lo}, {full[2].lo, in[2].lo}};
+            const Interval hi_s[3] = {{in[0].hi, full[0].hi}, {in[1].hi, full[1].hi}, {in[2].hi, full[2].hi}};
+            // slabs: z-lo, z-hi (full x, y), y-lo, y-hi (interior z), x-lo, x-hi (interior y, z)
+            const Interval slabs[6][3] = {{full[0], full[1], lo_s[2]}, {full[0], full[1], hi_s[2]},
+                                          {full[0], lo_s[1], in[2]},   {full[0], hi_s[1], in[2]},
+                                          {lo_s[0], in[1], in[2]},     {hi_s[0], in[1], in[2]}};
+            for (int cb : c->levels[L - 1].blocks) {
+                Interval cov[3];
+                for (int d = 0; d < 3; ++d)
+                    cov[d] = {2 * G[cb][d], 2 * (G[cb][d] + c->descs[cb].ncells[d])};
+                for (auto& sl : slabs) {
+                    XferBox x{};
+                    bool ok = true;
+                    for (int d = 0; d < 3; ++d) {
+                        const Interval m = meet(sl[d], cov[d]);
+                        if (m.empty()) {
+                            ok = false;
+                            break;
+                        }
+                        x.d0[d] = m.lo - (G[f][d] - NG);
+                        x.n[d] = m.hi - m.lo;
+                    }
+                    if (!ok) continue;
+                    x.dst = f;
+                    x.src = cb;
+                    pro.push_back(x);
+                }
+            }
+        }
+        CK(upload_xfer(pro, X[L].prolong, c->stream), "upload prolongation boxes");
+        // restriction into level L-1 from level L
+        std::vector<XferBox> res;
+        for (int cb : c->levels[L - 1].blocks)
+            for (int f : blocks) {
+                XferBox x{};
+                bool ok = true;
+                for (int d = 0; d < 3; ++d) {
+                    const int F0 = G[f][d], nf = c->descs[f].ncells[d];
+                    // coarse I with children 2I, 2I+1 inside [F0, F0 + nf) (F0 >= 0)
+                    const Interval ci{(F0 + 1) / 2, (F0 + nf) / 2};
+                    const Interval m = meet(ci, {G[cb][d], G[cb][d] + c->descs[cb].ncells[d]});
+                    if (m.empty()) {
+                        ok = false;
+                        break;
+                    }
+                    x.d0[d] = m.lo - (G[cb][d] - NG);
+                    x.s0[d] = 2 * m.lo - (F0 - NG);
+                    x.n[d] = m.hi - m.lo;
+                }
+                if (!ok) continue;
+                x.dst = cb;
+                x.src = f;
+                res.push_back(x);
+            }
+        X[L - 1].restrict_.emplace_back();
+        CK(upload_xfer(res, X[L - 1].restrict_.back(), c->stream), "upload restriction boxes");
+    }
+    c->xfer_built[GRANITE_AMR_GHOSTS] = true;
+    return GRANITE_OK;
+}
+
+// Transfer lists for GRANITE_AMR_REFERENCE, literally amr.cpp: every fine block
+// is overwritten in all its cells by prolongation from each coarse block in
+// turn (the last one wins, amr.cpp:313-318,438), faces no coarse block covers
+// get the zero-gradient fill (amr.cpp:420-480), and restriction runs fine block
+// by fine block (amr.cpp:339-341,566-626).
+int build_reference_mode(Ctx* c) {
+    auto& X = c->xfer[GRANITE_AMR_REFERENCE];
+    X.assign(c->levels.size(), LevelXfer());
+    for (size_t L = 0; L < c->levels.size(); ++L) {
+        const auto& blocks = c->levels[L].blocks;
+        std::vector<unsigned char> mask(c->descs.size(), 0x3F);
+        if (L > 0) {
+            const int last = c->levels[L - 1].blocks.back();
+            std::vector<XferBox> pro;
+            for (int f : blocks) {
+                const auto& fd = c->descs[f];
+                XferBox x{};
+                x.dst = f;
+                x.src = last;
+                for (int d = 0; d < 3; ++d) x.n[d] = fd.ncells[d] + 2 * NG;
+                pro.push_back(x);
+                unsigned char m = 0;
+                for (int d = 0; d < 3; ++d) {
+                    const double dxf = (fd.hi[d] - fd.lo[d]) / static_cast<double>(fd.ncells[d]);
+                    const double fine_lo = xref(fd, d, fd.nghost), fine_hi = xref(fd, d, fd.nghost + fd.ncells[d] - 1);
+                    bool flo = false, fhi = false;
+                    for (int cb : c->levels[L - 1].blocks) {
+                        const auto& cd = c->descs[cb];
+                        if (xref(cd, d, cd.nghost) <= fine_lo + 0.5 * dxf) flo = true;
+                        if (xref(cd, d, cd.nghost + cd.ncells[d] - 1) >= fine_hi - 0.5 * dxf) fhi = true;
+                    }
+                    if (!flo) m |= (unsigned char)(1u << (2 * d));
+                    if (!fhi) m |= (unsigned char)(1u << (2 * d + 1));
+                }
+                mask[f] = m;
+            }
+            CK(upload_xfer(pro, X[L].prolong, c->stream), "upload prolongation boxes");
+            // restriction into level L-1, one launch per fine block in order
+            for (int f : blocks) {
+                const auto& fd = c->descs[f];
+                std::vector<XferBox> res;
+                for (int cb : c->levels[L - 1].blocks) {
+                    const auto& cd = c->descs[cb];
+                    XferBox x{};
+                    bool ok = true;
+                    for (int d = 0; d < 3; ++d) {
+                        const double dxf = (fd.hi[d] - fd.lo[d]) / static_cast<double>(fd.ncells[d]);
+                        const double fx0 = xref(fd, d, 0);
+                        int first = -1, last = -1, base0 = 0;
+                        for (int ci = cd.nghost; ci < cd.nghost + cd.ncells[d]; ++ci) {
+                            const int fb = (int)std::round((xref(cd, d, ci) - fx0) / dxf) - 1;
+                            const bool in = fb >= fd.nghost && fb + 2 <= fd.nghost + fd.ncells[d] + fd.nghost;
+                            if (!in) continue;
+                            if (first < 0) {
+                                first = ci;
+                                base0 = fb;
+                            } else if (ci != last + 1 || fb != base0 + 2 * (ci - first)) {
+                                return fail(c, GRANITE_ERR_UNSUPPORTED,
+                                            "restriction needs ratio-2 aligned blocks");
+                            }
+                            last = ci;
+                        }
+                        if (first < 0) {
+                            ok = false;
+                            break;
+                        }
+                        x.d0[d] = first;
+                        x.s0[d] = base0;
+                        x.n[d] = last - first + 1;
+                    }
+                    if (!ok) continue;
+                    x.dst = cb;
+                    x.src = f;
+                    res.push_back(x);
+                }
+                X[L - 1].restrict_.emplace_back();
+                CK(upload_xfer(res, X[L - 1].restrict_.back(), c->stream), "upload restriction boxes");
+            }
+        }
+        CK(upload_vec(mask, &X[L].d_facemask, c->stream), "upload face masks");
+    }
+    c->xfer_built[GRANITE_AMR_REFERENCE] = true;
+    return GRANITE_OK;
+}
+
+cudaError_t xfer(Ctx* c, int kind, const XferList& x, int dst_sel, int src_sel) {
+    if (x.nchunks == 0) return cudaSuccess;
+    return timed(c, GRANITE_KERNEL_TRANSFER, [&] {
+        return launch_xfer(kind, c->d_blocks, x.d_boxes, x.d_chunks, x.nchunks, dst_sel, src_sel, c->stream);
+    });
+}
+
+// Ghost fill of one level's buffer slot. level_fill: the fill around a step
+// (zero-gradient base); otherwise a stage fill (1/r falloff base).
+cudaError_t fill_level(Ctx* c, int L, int slot, bool level_fill, int mode, long long* n) {
+    LevelLists& ll = c->levels[L];
+    const LevelXfer& X = c->xfer[mode][L];
+    cudaError_t e;
+    if (mode == GRANITE_AMR_REFERENCE) {
+        if (level_fill) {
+            if (L > 0) {  // fillGhostZones: prolongate into all cells, then the uncovered faces
+                if ((e = xfer(c, XFER_PROLONG, X.prolong, slot, 0))) return e;
+                ++*n;
+            }
+            const int gm = L > 0 ? GHOST_ZERO_GRADIENT_MASKED : GHOST_ZERO_GRADIENT;
+            if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] {
+                     return launch_ghost_fill(gm, c->d_blocks, ll.d_ghost, ll.nghost, slot, X.d_facemask, c->stream);
+                 })))
+                return e;
+        } else {  // applyOuterBC on every block (main.cpp:351-521)
+            if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] {
+                     return launch_ghost_fill(GHOST_SOMMERFELD, c->d_blocks, ll.d_ghost, ll.nghost, slot, nullptr,
+                                              c->stream);
+                 })))
+                return e;
+        }
+        ++*n;
+        return cudaSuccess;
+    }
+    // GRANITE_AMR_GHOSTS: block-local fill, then coarse data, then same-level neighbours
+    const int base = level_fill ? GHOST_ZERO_GRADIENT : GHOST_SOMMERFELD;
+    if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] {
+             return launch_ghost_fill(base, c->d_blocks, ll.d_ghost, ll.nghost, slot, nullptr, c->stream);
+         })))
+        return e;
+    ++*n;
+    if (L > 0 && X.prolong.nchunks) {
+        if ((e = xfer(c, XFER_PROLONG, X.prolong, slot, 0))) return e;
+        ++*n;
+    }
+    if (X.copy.nchunks) {
+        if ((e = xfer(c, XFER_COPY, X.copy, slot, slot))) return e;
+        ++*n;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t stage(Ctx* c, int L, int precision, int in, int out, double a1, double a2, double a3dt, int final_stage,
+                  long long* n) {
+    LevelLists& ll = c->levels[L];
+    StageArgs a = base_args(c);
+    a.in_sel = in;
+    a.n_sel = 0;
+    a.out_sel = out;
+    a.final_stage = final_stage;
+    a.a1 = a1;
+    a.a2 = a2;
+    a.a3dt = a3dt;
+    ++*n;
+    return timed(c, GRANITE_KERNEL_STAGE, [&] {
+        return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, ll.d_tiles, ll.ntiles, a, c->stream);
+    });
+}
+
+// AMRHierarchy::subcycle(L) with the RK3 step as evolve_func, amr.cpp:303-350.
+cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long long* n) {
+    cudaError_t e;
+    const LevelXfer& X = c->xfer[mode][L];
+    if (mode == GRANITE_AMR_REFERENCE && L > 0) {  // amr.cpp:313-318 (the fill below repeats it exactly)
+        if ((e = xfer(c, XFER_PROLONG, X.prolong, 0, 0))) return e;
+        ++*n;
+        LevelLists& ll = c->levels[L];
+        if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] {
+                 return launch_ghost_fill(GHOST_ZERO_GRADIENT_MASKED, c->d_blocks, ll.d_ghost, ll.nghost, 0,
+                                          X.d_facemask, c->stream);
+             })))
+            return e;
+        ++*n;
+    } else {
+        if ((e = fill_level(c, L, 0, true, mode, n))) return e;  // amr.cpp:319
+    }
+    // TimeIntegrator::sspRK3Step, main.cpp:673-689
+    if ((e = stage(c, L, precision, 0, 1, 1.0, 0.0, 1.0 * dt, 0, n))) return e;
+    if ((e = fill_level(c, L, 1, false, mode, n))) return e;
+    if ((e = stage(c, L, precision, 1, 2, 0.75, 0.25, 0.25 * dt, 0, n))) return e;
+    if ((e = fill_level(c, L, 2, false, mode, n))) return e;
+    if ((e = stage(c, L, precision, 2, 0, 1.0 / 3.0, 2.0 / 3.0, (2.0 / 3.0) * dt, 1, n))) return e;
+    if ((e = fill_level(c, L, 0, true, mode, n))) return e;  // amr.cpp:329
+    if (L + 1 < (int)c->levels.size()) {
+        for (int r = 0; r < 2; ++r)
+            if ((e = subcycle(c, L + 1, dt / 2.0, precision, mode, n))) return e;  // amr.cpp:334-336, :393-397
+        for (const XferList& rl : X.restrict_) {                                   // amr.cpp:339-341
+            if ((e = xfer(c, XFER_RESTRICT, rl, 0, 0))) return e;
+            ++*n;
+        }
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
 int granite_ccz4_hierarchy_step(void* h, double dt_coarse, int precision, int amr_mode) {
     Ctx* c = static_cast<Ctx*>(h);
     if (!c) return GRANITE_ERR_INVALID;
-    (void)dt_coarse;
-    (void)precision;
-    (void)amr_mode;
-    return fail(c, GRANITE_ERR_UNSUPPORTED, "hierarchy_step: not built yet");
+    if (!c->committed) return fail(c, GRANITE_ERR_INVALID, "commit before stepping");
+    int r = check_precision(c, precision);
+    if (r) return r;
+    if (amr_mode != GRANITE_AMR_REFERENCE && amr_mode != GRANITE_AMR_GHOSTS)
+        return fail(c, GRANITE_ERR_INVALID, "amr_mode must be GRANITE_AMR_REFERENCE or GRANITE_AMR_GHOSTS");
+    if (!std::isfinite(dt_coarse)) return fail(c, GRANITE_ERR_INVALID, "dt must be finite");
+    for (auto& L : c->levels)
+        if (L.blocks.empty()) return fail(c, GRANITE_ERR_INVALID, "hierarchy levels must be contiguous from 0");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    if (!c->xfer_built[amr_mode]) {
+        r = amr_mode == GRANITE_AMR_GHOSTS ? build_ghosts_mode(c) : build_reference_mode(c);
+        if (r) return r;
+    }
+    if (c->profiling) {
+        long long n = 0;
+        cudaError_t e = subcycle(c, 0, dt_coarse, precision, amr_mode, &n);
+        if (e != cudaSuccess) return cuda_fail(c, e, "hierarchy step");
+        c->launches += n;
+        return GRANITE_OK;
+    }
+    unsigned long long dtbits;
+    std::memcpy(&dtbits, &dt_coarse, sizeof(dt_coarse));
+    auto key = std::make_tuple(precision, amr_mode, dtbits);
+    auto it = c->hgraphs.find(key);
+    if (it == c->hgraphs.end()) {
+        Graph g;
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        long long n = 0;
+        cudaError_t e = subcycle(c, 0, dt_coarse, precision, amr_mode, &n);
+        cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
+        if (e != cudaSuccess) return cuda_fail(c, e, "enqueue hierarchy step");
+        if (e2 != cudaSuccess) return cuda_fail(c, e2, "end capture");
+        e = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return cuda_fail(c, e, "graph instantiate");
+        g.launches = n;
+        it = c->hgraphs.emplace(key, g).first;
+    }
+    CK(cudaGraphLaunch(it->second.exec, c->stream), "graph launch");
+    c->launches += it->second.launches;
+    for (size_t L = 0; L < c->level_ghosts_valid.size(); ++L) c->level_ghosts_valid[L] = false;
+    return GRANITE_OK;
 }
 
 int granite_ccz4_constraint_norms(void* h, int level, double* h_l2, double* m_l2) {

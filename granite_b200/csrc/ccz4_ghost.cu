@@ -1,14 +1,15 @@
-// ccz4_ghost.cu -- ghost-cell fills and inter-level transfers.
+// ccz4_ghost.cu -- ghost-cell fills and inter-block transfers.
 //
 // All arithmetic here uses explicitly rounded intrinsics (no FMA contraction)
 // so the fills reproduce the reference host loops bit for bit:
-//   zero-gradient level fill   amr.cpp:447-480
+//   zero-gradient level fill   amr.cpp:447-480 (all faces, or the faces the
+//                              reference leaves uncovered by a parent block)
 //   1/r outer falloff          main.cpp:351-463 (x faces, then y, then z)
 //   trilinear prolongation     amr.cpp:484-564
 //   2x2x2 restriction          amr.cpp:566-626
-// The work is described by host-built item lists (ghost-cell chunks,
-// prolongation / restriction / copy cells), so one launch serves every block
-// of a level whatever its size.
+// The work is described by host-built lists (ghost-cell chunks, transfer
+// boxes cut into chunks), so one launch serves every block of a level
+// whatever its size.
 #include "ccz4_common.cuh"
 #include "ccz4_kernels.h"
 
@@ -55,7 +56,7 @@ __device__ double sommerfeld_value(const DevBlock& B, const double* __restrict__
     return falloff(fi, valXY(i, j, kc), ri, rg);
 }
 
-// k-th ghost cell of a block: z slabs first, then y slabs, then x slabs.
+// r-th ghost cell of a block: z slabs first, then y slabs, then x slabs.
 __device__ __forceinline__ bool ghost_coords(const DevBlock& B, long long r, int& i, int& j, int& k) {
     const int T0 = B.tx, T1 = B.ty;
     const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
@@ -91,9 +92,18 @@ __device__ __forceinline__ bool ghost_coords(const DevBlock& B, long long r, int
     return false;
 }
 
+// Zero-gradient with a face mask: the reference's x, y, z passes over the
+// flagged faces only. Copies are exact, so the result is the cell reached by
+// clamping each coordinate that lies beyond a flagged face (amr.cpp:447-480).
+__device__ __forceinline__ int masked_clamp(int a, int n, unsigned mask, int axis) {
+    if (a < NG) return (mask >> (2 * axis)) & 1u ? NG : a;
+    if (a >= NG + n) return (mask >> (2 * axis + 1)) & 1u ? NG + n - 1 : a;
+    return a;
+}
+
 // items[x].cell holds the first ghost rank of a chunk of blockDim.x ranks.
 __global__ void ghost_fill_kernel(int mode, const DevBlock* __restrict__ blocks, const GhostItem* __restrict__ items,
-                                  int sel) {
+                                  int sel, const unsigned char* __restrict__ facemask) {
     const GhostItem it = items[blockIdx.x];
     const DevBlock& B = blocks[it.block];
     int i, j, k;
@@ -112,6 +122,12 @@ __global__ void ghost_fill_kernel(int mode, const DevBlock* __restrict__ blocks,
         si = clampi(i, NG, NG + B.n[0] - 1);
         sj = clampi(j, NG, NG + B.n[1] - 1);
         sk = clampi(k, NG, NG + B.n[2] - 1);
+    } else if (mode == GHOST_ZERO_GRADIENT_MASKED) {
+        const unsigned m = facemask[it.block];
+        si = masked_clamp(i, B.n[0], m, 0);
+        sj = masked_clamp(j, B.n[1], m, 1);
+        sk = masked_clamp(k, B.n[2], m, 2);
+        if (si == i && sj == j && sk == k) return;
     } else {  // periodic
         si = i < NG ? i + B.n[0] : (i >= NG + B.n[0] ? i - B.n[0] : i);
         sj = j < NG ? j + B.n[1] : (j >= NG + B.n[1] ? j - B.n[1] : j);
@@ -121,22 +137,16 @@ __global__ void ghost_fill_kernel(int mode, const DevBlock* __restrict__ blocks,
     for (int v = 0; v < NV; ++v) base[(long long)v * B.stride + c] = base[(long long)v * B.stride + s];
 }
 
-__global__ void prolong_kernel(const DevBlock* __restrict__ blocks, const ProlongItem* __restrict__ items, int n,
-                               int sel) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const ProlongItem it = items[t];
-    const DevBlock& F = blocks[it.fine_block];
-    const DevBlock& C = blocks[it.coarse_block];
-    const int i = it.cell % F.tx;
-    const int j = (it.cell / F.tx) % F.ty;
-    const int k = it.cell / (F.tx * F.ty);
+// Trilinear prolongation of coarse block C into fine cell (i,j,k) of F,
+// amr.cpp:496-561: nearest coarse centre by rounding, one-sided neighbour by
+// the sign of the fractional offset, indices clamped to the coarse block.
+__device__ void prolong_cell(const DevBlock& F, const DevBlock& C, int i, int j, int k, double* __restrict__ fb,
+                             const double* __restrict__ cb) {
     const int fi[3] = {i, j, k};
     const int ct[3] = {C.tx, C.ty, C.tz};
     int c0[3], c1[3];
     double ax[3];
     for (int d = 0; d < 3; ++d) {
-        // (x - coarse.x(d, istart)) / coarse.dx + istart  (amr.cpp:502-507)
         const double f = __dadd_rn(__ddiv_rn(__dsub_rn(coord(F, d, fi[d]), coord(C, d, NG)), C.dx[d]), (double)NG);
         int a = (int)round(f);
         a = a > ct[d] - 1 ? ct[d] - 1 : a;
@@ -162,8 +172,7 @@ __global__ void prolong_kernel(const DevBlock* __restrict__ blocks, const Prolon
     const long long o010 = cell_index(C, c0[0], c1[1], c0[2]), o001 = cell_index(C, c0[0], c0[1], c1[2]);
     const long long o110 = cell_index(C, c1[0], c1[1], c0[2]), o101 = cell_index(C, c1[0], c0[1], c1[2]);
     const long long o011 = cell_index(C, c0[0], c1[1], c1[2]), o111 = cell_index(C, c1[0], c1[1], c1[2]);
-    const double* cb = C.buf[sel];
-    double* fb = F.buf[sel];
+    const long long fc = cell_index(F, i, j, k);
     for (int v = 0; v < NV; ++v) {
         const double* q = cb + (long long)v * C.stride;
         double val = __dmul_rn(w000, __ldg(q + o000));
@@ -174,38 +183,43 @@ __global__ void prolong_kernel(const DevBlock* __restrict__ blocks, const Prolon
         val = __dadd_rn(val, __dmul_rn(w101, __ldg(q + o101)));
         val = __dadd_rn(val, __dmul_rn(w011, __ldg(q + o011)));
         val = __dadd_rn(val, __dmul_rn(w111, __ldg(q + o111)));
-        fb[(long long)v * F.stride + it.cell] = val;
+        fb[(long long)v * F.stride + fc] = val;
     }
 }
 
-__global__ void restrict_kernel(const DevBlock* __restrict__ blocks, const RestrictItem* __restrict__ items, int n,
-                                int sel) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const RestrictItem it = items[t];
-    const DevBlock& F = blocks[it.fine_block];
-    const DevBlock& C = blocks[it.coarse_block];
-    const long long sx = 1, sy_ = F.tx, sz = (long long)F.tx * F.ty;
-    const double* fb = F.buf[sel];
-    double* cb = C.buf[sel];
+__global__ void xfer_kernel(int kind, const DevBlock* __restrict__ blocks, const XferBox* __restrict__ boxes,
+                            const BoxChunk* __restrict__ chunks, int dst_sel, int src_sel) {
+    const BoxChunk ch = chunks[blockIdx.x];
+    const XferBox bx = boxes[ch.box];
+    const int r = ch.start + threadIdx.x;
+    if (r >= bx.n[0] * bx.n[1] * bx.n[2]) return;
+    const int a = r % bx.n[0], b = (r / bx.n[0]) % bx.n[1], c = r / (bx.n[0] * bx.n[1]);
+    const DevBlock& D = blocks[bx.dst];
+    const DevBlock& S = blocks[bx.src];
+    const int i = bx.d0[0] + a, j = bx.d0[1] + b, k = bx.d0[2] + c;
+    double* db = D.buf[dst_sel];
+    const double* sb = S.buf[src_sel];
+    if (kind == XFER_PROLONG) {
+        prolong_cell(D, S, i, j, k, db, sb);
+        return;
+    }
+    const long long dc = cell_index(D, i, j, k);
+    if (kind == XFER_COPY) {
+        const long long sc = cell_index(S, bx.s0[0] + a, bx.s0[1] + b, bx.s0[2] + c);
+        for (int v = 0; v < NV; ++v) db[(long long)v * D.stride + dc] = __ldg(sb + (long long)v * S.stride + sc);
+        return;
+    }
+    // restriction: mean of the 2x2x2 fine cells, summed rk, rj, ri (amr.cpp:601-609)
+    const long long f0 = cell_index(S, bx.s0[0] + 2 * a, bx.s0[1] + 2 * b, bx.s0[2] + 2 * c);
+    const long long sx = 1, sy = S.tx, sz = (long long)S.tx * S.ty;
     for (int v = 0; v < NV; ++v) {
-        const double* q = fb + (long long)v * F.stride + it.fine_base;
+        const double* q = sb + (long long)v * S.stride + f0;
         double s = 0.0;
         for (int rk = 0; rk < 2; ++rk)
             for (int rj = 0; rj < 2; ++rj)
-                for (int ri = 0; ri < 2; ++ri) s = __dadd_rn(s, __ldg(q + ri * sx + rj * sy_ + rk * sz));
-        cb[(long long)v * C.stride + it.cell] = __ddiv_rn(s, 8.0);
+                for (int ri = 0; ri < 2; ++ri) s = __dadd_rn(s, __ldg(q + ri * sx + rj * sy + rk * sz));
+        db[(long long)v * D.stride + dc] = __ddiv_rn(s, 8.0);
     }
-}
-
-__global__ void copy_kernel(const DevBlock* __restrict__ blocks, const CopyItem* __restrict__ items, int n, int sel) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const CopyItem it = items[t];
-    const DevBlock& D = blocks[it.dst_block];
-    const DevBlock& S = blocks[it.src_block];
-    for (int v = 0; v < NV; ++v)
-        D.buf[sel][(long long)v * D.stride + it.dst_cell] = S.buf[sel][(long long)v * S.stride + it.src_cell];
 }
 
 }  // namespace
@@ -213,29 +227,16 @@ __global__ void copy_kernel(const DevBlock* __restrict__ blocks, const CopyItem*
 constexpr int GHOST_CHUNK = 256;
 
 cudaError_t launch_ghost_fill(int mode, const DevBlock* blocks, const GhostItem* items, int nitems, int sel,
-                              cudaStream_t stream) {
+                              const unsigned char* facemask, cudaStream_t stream) {
     if (nitems <= 0) return cudaSuccess;
-    ghost_fill_kernel<<<nitems, GHOST_CHUNK, 0, stream>>>(mode, blocks, items, sel);
+    ghost_fill_kernel<<<nitems, GHOST_CHUNK, 0, stream>>>(mode, blocks, items, sel, facemask);
     return cudaGetLastError();
 }
 
-cudaError_t launch_prolong(const DevBlock* blocks, const ProlongItem* items, int nitems, int sel,
-                           cudaStream_t stream) {
-    if (nitems <= 0) return cudaSuccess;
-    prolong_kernel<<<(nitems + 255) / 256, 256, 0, stream>>>(blocks, items, nitems, sel);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_restrict(const DevBlock* blocks, const RestrictItem* items, int nitems, int sel,
-                            cudaStream_t stream) {
-    if (nitems <= 0) return cudaSuccess;
-    restrict_kernel<<<(nitems + 255) / 256, 256, 0, stream>>>(blocks, items, nitems, sel);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_copy(const DevBlock* blocks, const CopyItem* items, int nitems, int sel, cudaStream_t stream) {
-    if (nitems <= 0) return cudaSuccess;
-    copy_kernel<<<(nitems + 255) / 256, 256, 0, stream>>>(blocks, items, nitems, sel);
+cudaError_t launch_xfer(int kind, const DevBlock* blocks, const XferBox* boxes, const BoxChunk* chunks, int nchunks,
+                        int dst_sel, int src_sel, cudaStream_t stream) {
+    if (nchunks <= 0) return cudaSuccess;
+    xfer_kernel<<<nchunks, XFER_CHUNK, 0, stream>>>(kind, blocks, boxes, chunks, dst_sel, src_sel);
     return cudaGetLastError();
 }
 

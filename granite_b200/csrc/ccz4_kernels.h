@@ -34,38 +34,42 @@ struct GhostItem {
     int cell;  // linear cell index within the block (incl. ghosts)
 };
 
-enum GhostMode { GHOST_ZERO_GRADIENT = 0, GHOST_SOMMERFELD = 1, GHOST_PERIODIC = 2 };
+enum GhostMode {
+    GHOST_ZERO_GRADIENT = 0,    // all faces (amr.cpp:447-480)
+    GHOST_SOMMERFELD = 1,       // 1/r falloff (main.cpp:351-463)
+    GHOST_PERIODIC = 2,         // periodic wrap (gauge-wave workload)
+    GHOST_ZERO_GRADIENT_MASKED = 3  // only the faces flagged in a per-block 6-bit mask
+};
 
 // Fill every listed ghost cell of buffer slot `sel` for all 22 fields.
+// facemask (per block; bit 2d = low face of axis d, bit 2d+1 = high face) is
+// read only by GHOST_ZERO_GRADIENT_MASKED.
 cudaError_t launch_ghost_fill(int mode, const DevBlock* blocks, const GhostItem* items, int nitems,
-                              int sel, cudaStream_t stream);
+                              int sel, const unsigned char* facemask, cudaStream_t stream);
 
-// Trilinear prolongation (amr.cpp:484-564) of coarse block `cb` into the
-// listed fine cells of fine block `fb` (slot sel of both).
-struct ProlongItem {
-    int fine_block;
-    int coarse_block;
-    int cell;  // fine cell index
+// A box of cells moved between two blocks. Coordinates are block-local cell
+// indices including ghosts.
+//   copy:     dst <- src, same level, cell for cell (s0 = source origin)
+//   prolong:  dst (fine) <- trilinear interpolation of src (coarse), amr.cpp:484-564
+//   restrict: dst (coarse) <- mean of the 2x2x2 fine cells of src at s0 + 2 (a, b, c),
+//             amr.cpp:566-626
+struct XferBox {
+    int dst, src;
+    int d0[3];
+    int s0[3];
+    int n[3];
 };
-cudaError_t launch_prolong(const DevBlock* blocks, const ProlongItem* items, int nitems, int sel,
-                           cudaStream_t stream);
+// One CTA of a transfer launch: XFER_CHUNK consecutive cells of a box.
+struct BoxChunk {
+    int box;
+    int start;
+};
+constexpr int XFER_CHUNK = 256;
+enum XferKind { XFER_COPY = 0, XFER_PROLONG = 1, XFER_RESTRICT = 2 };
 
-// 2x2x2 restriction (amr.cpp:566-626) into listed coarse cells.
-struct RestrictItem {
-    int coarse_block;
-    int fine_block;
-    int cell;      // coarse cell index
-    int fine_base; // fine cell index of the (0,0,0) corner of the 2x2x2 stencil
-};
-cudaError_t launch_restrict(const DevBlock* blocks, const RestrictItem* items, int nitems, int sel,
-                            cudaStream_t stream);
-
-// Same-level ghost copy: dst cell of block a takes src cell of block b.
-struct CopyItem {
-    int dst_block, dst_cell, src_block, src_cell;
-};
-cudaError_t launch_copy(const DevBlock* blocks, const CopyItem* items, int nitems, int sel,
-                        cudaStream_t stream);
+// Transfers of slot src_sel of the source blocks into slot dst_sel of the destinations.
+cudaError_t launch_xfer(int kind, const DevBlock* blocks, const XferBox* boxes, const BoxChunk* chunks,
+                        int nchunks, int dst_sel, int src_sel, cudaStream_t stream);
 
 // Constraint monitor (ccz4.cpp:941-1159) over a tile work-list. Writes ham /
 // mom (single-block drop-in; may be null) and per-CTA partial sums of H^2 and

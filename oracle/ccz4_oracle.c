@@ -1003,3 +1003,105 @@ void orc_restrict(const orc_geom* fg, const double* uf, const orc_geom* cg, doub
                 }
     }
 }
+
+/* ---------------------------------------------------------------------------
+ * Pieces for hierarchy drivers (oracle/hierarchy.py)
+ * ------------------------------------------------------------------------- */
+
+/* One RK stage of one block: rhs = L(u_in); u_out = a1 u_n + a2 u_in + a3 dt rhs
+ * on interior cells; floors on all cells; det/trace constraints when final
+ * (main.cpp:673-687). u_out may alias u_n. */
+void orc_stage(const orc_params* p, const orc_geom* g, const double* u_n, const double* u_in,
+               double* u_out, double* rhs, double a1, double a2, double a3, double dt, int final) {
+    orc_rhs(p, g, u_in, rhs, NULL, NULL, NULL, NULL);
+    combine(g, u_out, u_n, a1, u_in, a2, rhs, a3, dt);
+    orc_floors(g, u_out);
+    if (final) orc_algebraic(g, u_out);
+}
+
+/* Zero-gradient copy on the faces flagged in mask (bit 2d: low face of axis
+ * d, bit 2d+1: high face), x then y then z passes, amr.cpp:447-480. */
+void orc_fill_zero_gradient_masked(const orc_geom* g, double* u, int mask) {
+    const int ng = g->ng, tx = tx_(g), ty = ty_(g), tz = tz_(g);
+    const long stride = orc_stride(g);
+    const int ie[3] = {ng + g->n[0], ng + g->n[1], ng + g->n[2]};
+    for (int v = 0; v < ORC_NV; ++v) {
+        double* f = u + (long)v * stride;
+#define A(i, j, k) f[(i) + (long)tx * ((j) + (long)ty * (k))]
+        if (mask & 1)
+            for (int k = 0; k < tz; ++k)
+                for (int j = 0; j < ty; ++j)
+                    for (int q = 0; q < ng; ++q) A(q, j, k) = A(ng, j, k);
+        if (mask & 2)
+            for (int k = 0; k < tz; ++k)
+                for (int j = 0; j < ty; ++j)
+                    for (int q = 0; q < ng; ++q) A(ie[0] + q, j, k) = A(ie[0] - 1, j, k);
+        if (mask & 4)
+            for (int k = 0; k < tz; ++k)
+                for (int i = 0; i < tx; ++i)
+                    for (int q = 0; q < ng; ++q) A(i, q, k) = A(i, ng, k);
+        if (mask & 8)
+            for (int k = 0; k < tz; ++k)
+                for (int i = 0; i < tx; ++i)
+                    for (int q = 0; q < ng; ++q) A(i, ie[1] + q, k) = A(i, ie[1] - 1, k);
+        if (mask & 16)
+            for (int j = 0; j < ty; ++j)
+                for (int i = 0; i < tx; ++i)
+                    for (int q = 0; q < ng; ++q) A(i, j, q) = A(i, j, ng);
+        if (mask & 32)
+            for (int j = 0; j < ty; ++j)
+                for (int i = 0; i < tx; ++i)
+                    for (int q = 0; q < ng; ++q) A(i, j, ie[2] + q) = A(i, j, ie[2] - 1);
+#undef A
+    }
+}
+
+/* Trilinear prolongation (amr.cpp:484-564) into the fine cells whose mask
+ * byte is non-zero. */
+void orc_prolongate_masked(const orc_geom* cg, const double* uc, const orc_geom* fg, double* uf,
+                           const unsigned char* mask) {
+    const int ftx = tx_(fg), fty = ty_(fg), ftz = tz_(fg);
+    const int ctx = tx_(cg), cty = ty_(cg), ctz = tz_(cg);
+    const long fs = orc_stride(fg), cs = orc_stride(cg);
+    const int cis = cg->ng;
+    const int ct[3] = {ctx, cty, ctz};
+    for (int k = 0; k < ftz; ++k)
+        for (int j = 0; j < fty; ++j)
+            for (int i = 0; i < ftx; ++i) {
+                const long fc = i + (long)ftx * (j + (long)fty * k);
+                if (!mask[fc]) continue;
+                const double X[3] = {xc(fg, 0, i), xc(fg, 1, j), xc(fg, 2, k)};
+                double fr[3];
+                int ci[3], cn[3];
+                for (int d = 0; d < 3; ++d) {
+                    double f = (X[d] - xc(cg, d, cis)) / cg->dx[d] + cis;
+                    int c0 = (int)round(f);
+                    if (c0 > ct[d] - 1) c0 = ct[d] - 1;
+                    if (c0 < 0) c0 = 0;
+                    fr[d] = f - (double)c0;
+                    int c1 = c0 + (fr[d] >= 0.0 ? 1 : -1);
+                    if (c1 > ct[d] - 1) c1 = ct[d] - 1;
+                    if (c1 < 0) c1 = 0;
+                    ci[d] = c0;
+                    cn[d] = c1;
+                }
+                const double ax = fabs(fr[0]), ay = fabs(fr[1]), az = fabs(fr[2]);
+                const double w000 = (1 - ax) * (1 - ay) * (1 - az);
+                const double w100 = ax * (1 - ay) * (1 - az);
+                const double w010 = (1 - ax) * ay * (1 - az);
+                const double w001 = (1 - ax) * (1 - ay) * az;
+                const double w110 = ax * ay * (1 - az);
+                const double w101 = ax * (1 - ay) * az;
+                const double w011 = (1 - ax) * ay * az;
+                const double w111 = ax * ay * az;
+                for (int v = 0; v < ORC_NV; ++v) {
+                    const double* C = uc + (long)v * cs;
+#define CV(a, b, c) C[(a) + (long)ctx * ((b) + (long)cty * (c))]
+                    uf[(long)v * fs + fc] = w000 * CV(ci[0], ci[1], ci[2]) + w100 * CV(cn[0], ci[1], ci[2]) +
+                        w010 * CV(ci[0], cn[1], ci[2]) + w001 * CV(ci[0], ci[1], cn[2]) +
+                        w110 * CV(cn[0], cn[1], ci[2]) + w101 * CV(cn[0], ci[1], cn[2]) +
+                        w011 * CV(ci[0], cn[1], cn[2]) + w111 * CV(cn[0], cn[1], cn[2]);
+#undef CV
+                }
+            }
+}

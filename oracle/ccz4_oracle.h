@@ -78,6 +78,13 @@ void orc_prolongate(const orc_geom* coarse, const double* uc, const orc_geom* fi
                     int ghosts_only);
 void orc_restrict(const orc_geom* fine, const double* uf, const orc_geom* coarse, double* uc);
 
+/* hierarchy-driver pieces (oracle/hierarchy.py) */
+void orc_stage(const orc_params* p, const orc_geom* g, const double* u_n, const double* u_in,
+               double* u_out, double* rhs, double a1, double a2, double a3, double dt, int final);
+void orc_fill_zero_gradient_masked(const orc_geom* g, double* u, int mask);
+void orc_prolongate_masked(const orc_geom* cg, const double* uc, const orc_geom* fg, double* uf,
+                           const unsigned char* mask);
+
 /* sum over interior points of H^2 and |M|^2 of one block (for RMS norms) */
 void orc_constraint_sums(const orc_geom* g, const double* u, double* h2, double* m2,
                          long* npts);

@@ -316,4 +316,107 @@ void ref_rk3_steps(const double* p6, const int* n, int ng, const double* lo, con
     std::memcpy(u, st.flatBuffer(), nbytes(st));
 }
 
+// ---------------------------------------------------------------------------
+// The reference Berger-Oliger hierarchy: AMRHierarchy built from tracking
+// spheres (amr.cpp:34-301), stepped by AMRHierarchy::subcycle (amr.cpp:303-350)
+// with the spacetime part of TimeIntegrator::sspRK3Step as evolve_func
+// (main.cpp:86-690, the restated lambdas of ccz4_oracle.c around the reference
+// computeRHSVacuum). Regridding is off (regrid_interval = 0).
+// ---------------------------------------------------------------------------
+struct RefHier {
+    std::unique_ptr<amr::AMRHierarchy> h;
+    std::vector<GridBlock*> blocks;  // level order, then creation order
+};
+
+void* ref_hier_create(const int* n, const double* lo, const double* hi, int max_levels, int nspheres,
+                      const double* centers, const double* radii, const int* min_levels) {
+    amr::AMRParams ap;
+    ap.max_levels = max_levels;
+    ap.regrid_interval = 0;
+    SimulationParams sp;
+    for (int d = 0; d < 3; ++d) {
+        sp.ncells[d] = n[d];
+        sp.domain_lo[d] = lo[d];
+        sp.domain_hi[d] = hi[d];
+    }
+    sp.ghost_cells = 4;
+    auto* r = new RefHier();
+    r->h = std::make_unique<amr::AMRHierarchy>(ap, sp);
+    for (int s = 0; s < nspheres; ++s)
+        r->h->addTrackingSphere({centers[3 * s], centers[3 * s + 1], centers[3 * s + 2]}, radii[s], min_levels[s]);
+    std::cout.setstate(std::ios_base::failbit);
+    r->h->initialize([](const GridBlock&, int, int, int) { return false; });
+    std::cout.clear();
+    for (int L = 0; L < r->h->numLevels(); ++L)
+        for (GridBlock* b : r->h->getLevel(L)) r->blocks.push_back(b);
+    return r;
+}
+
+int ref_hier_num_blocks(void* hp) { return (int)static_cast<RefHier*>(hp)->blocks.size(); }
+
+void ref_hier_block_info(void* hp, int i, int* level, int* n, double* lo, double* hi) {
+    GridBlock* b = static_cast<RefHier*>(hp)->blocks[i];
+    *level = b->getLevel();
+    for (int d = 0; d < 3; ++d) {
+        n[d] = b->numCells()[d];
+        lo[d] = b->lowerCorner()[d];
+        hi[d] = b->upperCorner()[d];
+    }
+}
+
+void ref_hier_get(void* hp, int i, double* u) {
+    GridBlock* b = static_cast<RefHier*>(hp)->blocks[i];
+    std::memcpy(u, b->flatBuffer(), nbytes(*b));
+}
+
+void ref_hier_set(void* hp, int i, const double* u) {
+    GridBlock* b = static_cast<RefHier*>(hp)->blocks[i];
+    std::memcpy(b->flatBuffer(), u, nbytes(*b));
+}
+
+void ref_hier_step(void* hp, const double* p6, double dt_coarse, int nsteps) {
+    RefHier* r = static_cast<RefHier*>(hp);
+    spacetime::CCZ4Evolution ev(params(p6));
+    auto evolve = [&](std::vector<GridBlock*>& blocks, Real dt) {
+        // stage by stage over all blocks of the level, as sspRK3Step does
+        std::vector<std::unique_ptr<GridBlock>> stage, rhs;
+        for (GridBlock* b : blocks) {
+            stage.push_back(std::make_unique<GridBlock>(b->getId(), b->getLevel(), b->numCells(),
+                                                        b->lowerCorner(), b->upperCorner(),
+                                                        b->getNumGhost(), NUM_SPACETIME_VARS));
+            rhs.push_back(std::make_unique<GridBlock>(b->getId(), b->getLevel(), b->numCells(),
+                                                      b->lowerCorner(), b->upperCorner(),
+                                                      b->getNumGhost(), NUM_SPACETIME_VARS));
+        }
+        const double a1[3] = {1.0, 0.75, 1.0 / 3.0}, a2[3] = {0.0, 0.25, 2.0 / 3.0},
+                     a3[3] = {1.0, 0.25, 2.0 / 3.0};
+        for (int s = 0; s < 3; ++s) {
+            for (size_t q = 0; q < blocks.size(); ++q) {
+                GridBlock& st = *blocks[q];
+                GridBlock& in = s == 0 ? st : *stage[q];
+                GridBlock& out = s == 2 ? st : *stage[q];
+                const orc_geom og = ogeom(st);
+                ev.computeRHSVacuum(in, *rhs[q]);
+                const int is = st.istart();
+                for (int v = 0; v < NUM_SPACETIME_VARS; ++v)
+                    for (int k = is; k < st.iend(2); ++k)
+                        for (int j = is; j < st.iend(1); ++j)
+                            for (int i = is; i < st.iend(0); ++i)
+                                out.data(v, i, j, k) = a1[s] * st.data(v, i, j, k) + a2[s] * in.data(v, i, j, k) +
+                                    a3[s] * dt * rhs[q]->data(v, i, j, k);
+                orc_floors(&og, out.flatBuffer());
+                if (s == 2) orc_algebraic(&og, out.flatBuffer());
+                orc_fill_sommerfeld(&og, out.flatBuffer());
+            }
+        }
+    };
+    r->h->setLevelDt(0, dt_coarse);
+    std::cout.setstate(std::ios_base::failbit);
+    for (int s = 0; s < nsteps; ++s)
+        r->h->subcycle(0, evolve, [](const GridBlock&, int, int, int) { return false; });
+    std::cout.clear();
+}
+
+void ref_hier_destroy(void* hp) { delete static_cast<RefHier*>(hp); }
+
 } // extern "C"

@@ -1,0 +1,140 @@
+"""GPU Berger-Oliger hierarchy step against the hierarchy oracle.
+
+GRANITE_AMR_REFERENCE is checked on the reference's own tracking-sphere
+hierarchy (built by the compiled AMRHierarchy where available, else rebuilt
+from its recorded geometry) and GRANITE_AMR_GHOSTS on seeded multi-block
+hierarchies, both with the scaled per-point bound of test_parity_gpu.py.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from oracle import Geom, Params
+from oracle.hierarchy import HierarchyOracle
+
+from test_parity_gpu import VARIANTS, parity
+
+pytestmark = pytest.mark.gpu
+
+BL_M = [0.5, 0.5]
+BL_X = [[1.5, 0.0, 0.0], [-1.5, 0.0, 0.0]]
+
+# geometry of the reference hierarchy of test_hierarchy_cpu (base 16^3 on [-8, 8]^3,
+# tracking spheres at x = +-1.5, radius 2, min_level 2), as AMRHierarchy builds it
+REF_LAYOUT = None
+
+
+def reference_layout():
+    global REF_LAYOUT
+    if REF_LAYOUT is None:
+        if oracle.reference_available("strict"):
+            from oracle.hierarchy import RefHierarchy
+            rh = RefHierarchy(oracle.Reference("strict"), (16, 16, 16), (-8.0, -8.0, -8.0), (8.0, 8.0, 8.0),
+                              [((1.5, 0.0, 0.0), 2.0, 2), ((-1.5, 0.0, 0.0), 2.0, 2)])
+            REF_LAYOUT = (rh.geoms, rh.levels)
+        else:  # the layout AMRHierarchy::regrid produces for these spheres (amr.cpp:147-300)
+            REF_LAYOUT = ([Geom((16, 16, 16), (-8.0, -8.0, -8.0), (8.0, 8.0, 8.0)),
+                           Geom((22, 16, 16), (-6.0, -4.0, -4.0), (5.0, 4.0, 4.0)),
+                           Geom((28, 16, 16), (-3.5, -2.0, -2.0), (3.5, 2.0, 2.0))], [0, 1, 2])
+    return REF_LAYOUT
+
+
+def gpu_hierarchy(gb, geoms, levels, states, variant=None):
+    ev = gb.Evolver(gb.CCZ4Params(), variant)
+    blocks = []
+    for i, (g, L) in enumerate(zip(geoms, levels)):
+        b = gb.GridBlock(i, L, g.n, g.lo, g.hi)
+        b.array[...] = states[i]
+        ev.add_block(b)
+        blocks.append(b)
+    ev.commit()
+    ev.upload()
+    return ev, blocks
+
+
+@pytest.fixture(scope="module")
+def gb():
+    import granite_b200
+    return granite_b200
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_reference_mode_matches_oracle(gb, oracle_lib, variant):
+    geoms, levels = reference_layout()
+    states = []
+    for i, g in enumerate(geoms):
+        u = oracle_lib.init_brill_lindquist(g, BL_M, BL_X)
+        states.append(u + 1e-8 * oracle.hash_noise(g.shape, 100 + i))
+    ho = HierarchyOracle(geoms, levels, oracle_lib)
+    for i, u in enumerate(states):
+        ho.u[i][...] = u
+    dt = 0.25 * geoms[0].dx[0]
+    ho.step(Params(), dt, "reference", 2)
+    ev, blocks = gpu_hierarchy(gb, geoms, levels, states, variant)
+    for _ in range(2):
+        ev.hierarchy_step(dt, gb.PRECISION_FP64, gb.AMR_REFERENCE)
+    ev.download()
+    for i, b in enumerate(blocks):
+        parity(b.array, ho.u[i], rtol=1e-10, what=f"reference-mode block {i} level {levels[i]}")
+
+
+def small_hierarchy(seed=5, levels=3):
+    from granite_b200.hierarchy import make_binary_hierarchy
+    h = make_binary_hierarchy(seed=seed, levels=levels, coarse_n=32, extent=16.0, sizes=(8, 16, 24),
+                              blocks_per_level=(8, 40))
+    geoms = [Geom(b.ncells, b.lo, b.hi) for b in h.blocks]
+    return h, geoms, [b.level for b in h.blocks]
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_ghosts_mode_matches_oracle(gb, oracle_lib, variant):
+    h, geoms, levels = small_hierarchy()
+    states = []
+    for i, g in enumerate(geoms):
+        u = oracle_lib.init_brill_lindquist(g, h.masses, h.positions, r_floor=0.5 * g.dx[0])
+        states.append(oracle.add_noise(u, 1e-10, 12345 + i))
+    ho = HierarchyOracle(geoms, levels, oracle_lib)
+    for i, u in enumerate(states):
+        ho.u[i][...] = u
+    dt = 0.25 * geoms[0].dx[0]
+    ho.step(Params(), dt, "ghosts", 2)
+    ev, blocks = gpu_hierarchy(gb, geoms, levels, states, variant)
+    for _ in range(2):
+        ev.hierarchy_step(dt, gb.PRECISION_FP64, gb.AMR_GHOSTS)
+    ev.download()
+    for i, b in enumerate(blocks):
+        parity(b.array, ho.u[i], rtol=1e-10, what=f"ghosts-mode block {i} level {levels[i]}")
+
+
+def test_hierarchy_graph_replay_deterministic(gb, oracle_lib):
+    h, geoms, levels = small_hierarchy(seed=9, levels=2)
+    states = [oracle_lib.init_brill_lindquist(g, h.masses, h.positions, r_floor=0.5 * g.dx[0]) for g in geoms]
+    dt = 0.25 * geoms[0].dx[0]
+    outs = []
+    for _ in range(2):
+        ev, blocks = gpu_hierarchy(gb, geoms, levels, states)
+        for _ in range(3):
+            ev.hierarchy_step(dt, gb.PRECISION_FP64, gb.AMR_GHOSTS)
+        ev.download()
+        outs.append([b.array.copy() for b in blocks])
+        ev.close()
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+
+
+def test_hierarchy_mixed_close_to_fp64(gb, oracle_lib):
+    h, geoms, levels = small_hierarchy(seed=11, levels=2)
+    states = [oracle.add_noise(oracle_lib.init_brill_lindquist(g, h.masses, h.positions, r_floor=0.5 * g.dx[0]),
+                               1e-10, 7 + i) for i, g in enumerate(geoms)]
+    dt = 0.25 * geoms[0].dx[0]
+    res = {}
+    for prec in (gb.PRECISION_FP64, gb.PRECISION_MIXED):
+        ev, blocks = gpu_hierarchy(gb, geoms, levels, states)
+        for _ in range(4):
+            ev.hierarchy_step(dt, prec, gb.AMR_GHOSTS)
+        ev.download()
+        res[prec] = [b.array.copy() for b in blocks]
+        ev.close()
+    # mixed-precision deviation from the FP64 run, relative to each tensor's scale
+    for a, b in zip(res[gb.PRECISION_FP64], res[gb.PRECISION_MIXED]):
+        parity(b, a, rtol=1e-5, what="mixed vs fp64")
