@@ -2,23 +2,31 @@
 """CCZ4 SSP-RK3 point-updates/s on B200 (one process per GPU).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl granite|reference]
-                    [--workload single_puncture_128|gauge_wave_48] [--precision fp64|mixed]
+                    [--workload binary_bl_4level|triple_bl_6level|single_puncture_128|gauge_wave_48]
+                    [--precision mixed|fp64] [--variant global|smem]
 
-A step is one full SSP-RK3 coarse step of the workload (3 fused RHS+KO+RK
-stage launches, ghost fills), inputs resident in HBM. The metric counts
-interior points x RK3 steps per wall second, timed with CUDA events on the
-library's stream between barriers, max over ranks. Multi-GPU runs are
-independent replicas (the single-block workloads do not shard), weak scaling.
+Default workload: binary Brill-Lindquist punctures (m = 0.5 at x = +-3) on the
+4-level Berger-Oliger hierarchy (coarse dx = 1 on [-64,64]^3, 80-400 uneven
+blocks per level with edges from {16,24,32,48,64}, seeded), one coarse step =
+the subcycled RK3 step of all levels (level L takes 2^L steps), ghost exchange
+between blocks and levels, captured as one CUDA graph. value = point-updates/s
+of the mixed-precision form; the FP64 plain form runs on the same hierarchy
+and its throughput, the ratio and the mixed-vs-FP64 accuracy are on the line.
+A point-update is one interior point advanced by one RK3 step of its level.
+
+Timing: W warm-up steps, then K steps between barriers, timed with CUDA events
+on the library's stream, max over ranks; the resident state (GBs) is far larger
+than L2. Multi-GPU runs are independent replicas (weak scaling).
 
 Extra objects on the JSON line:
   roofline      HBM roofline of the fused stage kernel: algorithmic bytes
                 (1408 B per point-update) / its device time, measured in a
                 profiling pass with CUDA events around every stage launch.
   e2e           the same metric through the C ABI with host buffers: every
-                step uploads the state from pinned host memory, steps, and
-                downloads the state.
+                step uploads every block from pinned memory, steps, and
+                downloads every block.
   cpu_baseline  the compiled reference (oracle/_ref, Release flags, OpenMP on
-                all host cores) on a bounded sample of the same workload.
+                all host cores) on a bounded sample of the workload's blocks.
 """
 from __future__ import annotations
 
@@ -40,14 +48,15 @@ METRIC = "CCZ4 RK3 point-updates/s on 1 B200: mixed/batched vs FP64 plain, equal
 UNIT = "point-updates/s"
 BYTES_PER_POINT_UPDATE = 1408  # 3 stages: (2 + 3 + 3) x 22 fields x 8 B
 NV = 22
+GROUPS = [[0], [1, 2, 3, 4, 5, 6], [7, 8, 9, 10, 11, 12], [13], [14, 15, 16], [17], [18], [19, 20, 21]]
 
 WORKLOADS = {
-    # Single Brill-Lindquist puncture, M = 1 at the origin, 128^3 on [-16,16]^3,
-    # r floored at dx/2, U(-1e-10, 1e-10) noise (seed 12345), CFL 0.25,
-    # reference boundaries (zero-gradient level fill + 1/r falloff).
-    "single_puncture_128": dict(n=128, lo=-16.0, hi=16.0, kind="bl", bc=0),
-    # Gauge wave g_xx = 1 - 0.1 sin(2 pi x), 48^3 on [-0.5,0.5]^3, periodic.
-    "gauge_wave_48": dict(n=48, lo=-0.5, hi=0.5, kind="gw", bc=1),
+    "binary_bl_4level": dict(kind="hier", builder="binary"),
+    "triple_bl_6level": dict(kind="hier", builder="triple"),
+    # single BL puncture M = 1, 128^3 on [-16,16]^3, r >= dx/2, 1e-10 noise, reference boundaries
+    "single_puncture_128": dict(kind="block", n=128, lo=-16.0, hi=16.0, data="bl", bc=0),
+    # gauge wave g_xx = 1 - 0.1 sin(2 pi x), 48^3 on [-0.5,0.5]^3, periodic
+    "gauge_wave_48": dict(kind="block", n=48, lo=-0.5, hi=0.5, data="gw", bc=1),
 }
 
 
@@ -59,8 +68,7 @@ def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         with open(p) as f:
-            d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
+            return float(json.load(f)["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
 
 
@@ -78,15 +86,50 @@ def ncu_traffic(workload: str, kernel: str):
     return None
 
 
-def make_state(gb, w):
-    n, lo, hi = w["n"], w["lo"], w["hi"]
-    b = gb.GridBlock(0, 0, (n, n, n), (lo, lo, lo), (hi, hi, hi))
-    if w["kind"] == "bl":
-        gb.brill_lindquist(b, [1.0], [[0.0, 0.0, 0.0]], r_floor=0.5 * b.dx(0))
-        gb.initial_data.add_noise(b, 1e-10, 12345)
-    else:
-        gb.gauge_wave(b, -0.1, 1.0)
-    return b
+class Runner:
+    """One workload on one device through the library's resident-block API."""
+
+    def __init__(self, gb, name, w, precision, variant, device):
+        self.gb, self.w, self.prec = gb, w, precision
+        self.ev = gb.Evolver(gb.CCZ4Params(device=device), variant)
+        if w["kind"] == "hier":
+            build = gb.make_binary_hierarchy if w["builder"] == "binary" else gb.make_triple_hierarchy
+            self.h = build()
+            self.blocks = gb.block_states(self.h, noise=1e-10, seed=12345)
+            self.points_per_step = self.h.point_updates_per_coarse_step()
+            self.dt = 0.25 * self.h.level_dx[0]
+        else:
+            n, lo, hi = w["n"], w["lo"], w["hi"]
+            b = gb.GridBlock(0, 0, (n, n, n), (lo, lo, lo), (hi, hi, hi))
+            if w["data"] == "bl":
+                gb.brill_lindquist(b, [1.0], [[0.0, 0.0, 0.0]], r_floor=0.5 * b.dx(0))
+                gb.initial_data.add_noise(b, 1e-10, 12345)
+            else:
+                gb.gauge_wave(b, -0.1, 1.0)
+            self.h = None
+            self.blocks = [b]
+            self.points_per_step = n ** 3
+            self.dt = 0.25 * b.dx(0)
+        for b in self.blocks:
+            self.ev.add_block(b)
+        self.ev.commit()
+        self.ev.upload()
+        self.state_bytes = sum(b.array.nbytes for b in self.blocks)
+
+    def step(self):
+        if self.h is not None:
+            self.ev.hierarchy_step(self.dt, self.prec, self.gb.AMR_GHOSTS)
+        else:
+            self.ev.rk3_step(0, self.dt, self.prec, self.w["bc"])
+
+    def config(self):
+        if self.h is None:
+            n = self.w["n"]
+            return {"grid": f"{n}^3", "blocks": 1}
+        lv = [sum(1 for b in self.h.blocks if b.level == L) for L in range(self.h.num_levels)]
+        return {"levels": self.h.num_levels, "blocks": len(self.h.blocks), "blocks_per_level": lv,
+                "interior_points": self.h.interior_points(), "amr_mode": "ghosts",
+                "coarse_dx": self.h.level_dx[0], "refinement_ratio": 2, "subcycling": True}
 
 
 class ClockSampler:
@@ -100,7 +143,6 @@ class ClockSampler:
         self.device = device
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.p = None
-        self.t0 = self.t1 = None
 
     def start(self):
         try:
@@ -109,9 +151,6 @@ class ClockSampler:
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
-
-    def mark(self, which):
-        setattr(self, which, time.time())
 
     def stop(self):
         if self.p:
@@ -126,8 +165,9 @@ class ClockSampler:
         os.unlink(self.f.name)
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if len(r) > 8 and r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if len(r) > 8 and r[2].strip().replace(".", "").isdigit()]
+        num = lambda s: s.strip().replace(".", "", 1).isdigit()  # noqa: E731
+        sm = [float(r[1]) for r in rows if len(r) > 8 and num(r[1])]
+        mx = [float(r[2]) for r in rows if len(r) > 8 and num(r[2])]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
         for r in rows:
@@ -135,49 +175,65 @@ class ClockSampler:
                 for k, nm in enumerate(names):
                     if r[5 + k].strip() == "Active":
                         reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None,
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(w, seconds_target=15.0):
-    """Compiled reference (Release flags, OpenMP on all cores) on a bounded sample:
-    whole RK3 steps of the same workload until ~seconds_target of CPU work."""
+# ---------------------------------------------------------------------------
+# CPU reference (bounded samples)
+# ---------------------------------------------------------------------------
+
+def reference_sample(w, seconds_target: float):
+    """The compiled reference (Release flags, OpenMP on all cores) advancing blocks of
+    the workload by whole RK3 steps (reference boundaries per block) until
+    ~seconds_target of CPU work; returns a cpu_baseline object."""
     import oracle
     from oracle import Geom, Params
-    n, lo, hi = w["n"], w["lo"], w["hi"]
-    g = Geom((n, n, n), (lo, lo, lo), (hi, hi, hi))
     if oracle.reference_available("fast"):
-        impl = oracle.Reference("fast")
-        kind = "reference"
+        impl, kind = oracle.Reference("fast"), "reference"
         cores = impl.max_threads()
     else:
-        impl = oracle.Oracle()
-        kind = "port"
+        impl, kind = oracle.Oracle(), "port"
         cores = os.cpu_count()
     o = oracle.Oracle()
-    if w["kind"] == "bl":
-        u = o.init_brill_lindquist(g, [1.0], [[0.0, 0.0, 0.0]], r_floor=0.5 * g.dx[0])
-        u = oracle.add_noise(u, 1e-10, 12345)
+    if w["kind"] == "hier":
+        import granite_b200 as gb
+        h = (gb.make_binary_hierarchy if w["builder"] == "binary" else gb.make_triple_hierarchy)()
+        # blocks taken round-robin over the levels, so every level's sizes appear
+        per = [[b for b in h.blocks if b.level == L] for L in range(h.num_levels)]
+        order = [per[L][i] for i in range(max(len(p) for p in per)) for L in range(h.num_levels) if i < len(per[L])]
+
+        def block_jobs():
+            for b in order:
+                g = Geom(b.ncells, b.lo, b.hi)
+                u = o.init_brill_lindquist(g, h.masses, h.positions, r_floor=0.5 * g.dx[0])
+                yield g, oracle.add_noise(u, 1e-10, 12345), 0.25 * h.level_dx[b.level], 0
+
+        jobs = block_jobs()
+        desc = "one RK3 step of each of {} blocks of the hierarchy ({} interior points), each as a single block"
     else:
-        u = o.init_gauge_wave(g, -0.1, 1.0)
-    dt = 0.25 * g.dx[0]
-    bc = w["bc"]
-    t = time.perf_counter()
-    u = impl.rk3_steps(Params(), g, u, dt, 1, bc)
-    first = time.perf_counter() - t
-    steps = 1
-    total = first
-    extra = int(max(0, min(20, seconds_target / max(first, 1e-3) - 1)))
-    if extra:
+        n, lo, hi = w["n"], w["lo"], w["hi"]
+        g = Geom((n, n, n), (lo, lo, lo), (hi, hi, hi))
+        if w["data"] == "bl":
+            u = oracle.add_noise(o.init_brill_lindquist(g, [1.0], [[0.0, 0.0, 0.0]], r_floor=0.5 * g.dx[0]),
+                                 1e-10, 12345)
+        else:
+            u = o.init_gauge_wave(g, -0.1, 1.0)
+        jobs = [(g, u, 0.25 * g.dx[0], w["bc"])] * 1000
+        desc = "{} RK3 step(s) of the full workload block ({} interior points per step)"
+    total, pts, used, npts_block = 0.0, 0, 0, 0
+    for g, u, dt, bc in jobs:
+        npts_block = int(np.prod(g.n))
         t = time.perf_counter()
-        u = impl.rk3_steps(Params(), g, u, dt, extra, bc)
+        impl.rk3_steps(Params(), g, u, dt, 1, bc)
         total += time.perf_counter() - t
-        steps += extra
-    pts = n ** 3 * steps
+        pts += int(np.prod(g.n))
+        used += 1
+        if total >= seconds_target:
+            break
+    sample = desc.format(used, pts if w["kind"] == "hier" else npts_block)
     return {"value": pts / total, "unit": UNIT, "cores": int(cores), "kind": kind,
-            "sample": f"{steps} RK3 step(s) of the full {n}^3 workload, {total:.1f} s, "
-                      f"OMP threads = {cores}"}
+            "sample": f"{sample}; {total:.1f} s; OMP threads = {cores}"}
 
 
 def run_reference(args, w, rank, world):
@@ -187,33 +243,108 @@ def run_reference(args, w, rank, world):
     if not (oracle.reference_available("fast") or os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so"))):
         print(json.dumps({"impl": "reference", "unavailable": "compiled reference library not built"}))
         return 0
-    # each reference step is one RK3 step of the same workload; bound the run to ~2 minutes
-    cb = cpu_baseline(w, seconds_target=min(120.0, 6.0 * max(1, args.steps)))
-    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world,
-            "steps": int(cb["sample"].split()[0]), "warmup": 0,
-            "ms_per_step": 1000.0 * w["n"] ** 3 / cb["value"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": args.workload, "grid": f"{w['n']}^3", "precision": "fp64",
-                       "parallelism": "host OpenMP"},
+    cb = reference_sample(w, seconds_target=min(120.0, 4.0 * max(1, args.steps)))
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world, "steps": 1,
+            "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.workload, "precision": "fp64", "parallelism": "host OpenMP"},
             "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def timed_steps(torch, dist, world, local, run: Runner, steps: int):
+    stream = torch.cuda.ExternalStream(run.ev.stream_handle(), device=local)
+    n0 = run.ev.launch_count()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        run.step()
+    e1.record(stream)
+    run.ev.sync()
+    torch.cuda.synchronize(local)
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item()), run.ev.launch_count() - n0
+
+
+def roofline(gb, run: Runner, workload, prof_steps, kernel):
+    run.ev.set_profiling(True)
+    run.ev.profile_reset()
+    for _ in range(prof_steps):
+        run.step()
+    st_ms, st_n = run.ev.profile(gb.KERNEL_STAGE)
+    gh_ms, _ = run.ev.profile(gb.KERNEL_GHOST)
+    xf_ms, _ = run.ev.profile(gb.KERNEL_TRANSFER)
+    run.ev.set_profiling(False)
+    peak, peak_kind = measured_peaks()
+    total_bytes = BYTES_PER_POINT_UPDATE * run.points_per_step * prof_steps
+    achieved = total_bytes / (st_ms / 1000.0) / 1e9
+    per_launch = total_bytes / max(st_n, 1)
+    traffic = ncu_traffic(workload, kernel)
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "peak_source": peak_kind, "kernel": kernel,
+            "avg_launch_ms": st_ms / max(st_n, 1), "launches_per_step": st_n / prof_steps,
+            "algorithmic_bytes_per_launch": per_launch,
+            "stage_share_of_step": st_ms / max(st_ms + gh_ms + xf_ms, 1e-12)}
+
+
+def accuracy(gb, a: Runner, b: Runner, steps: int):
+    """Mixed (b) against FP64 (a) after the same steps: per-field max deviation
+    relative to the field's tensor scale over all blocks, and ||H||_2 ratio."""
+    a.ev.sync()
+    b.ev.sync()
+    dev = np.zeros(NV)
+    scale = np.zeros(NV)
+    for i in range(len(a.blocks)):
+        ua = np.empty_like(a.blocks[i].array)
+        ub = np.empty_like(ua)
+        a.ev.download(i, ua)
+        b.ev.download(i, ub)
+        it = a.blocks[i].interior()
+        d = np.abs(ua[it] - ub[it]).reshape(NV, -1).max(axis=1)
+        s = np.abs(ua[it]).reshape(NV, -1).max(axis=1)
+        dev = np.maximum(dev, d)
+        scale = np.maximum(scale, s)
+    gscale = np.zeros(NV)
+    for grp in GROUPS:
+        gscale[grp] = scale[grp].max()
+    rel = dev / np.maximum(gscale, 1e-300)
+    ha, ma = a.ev.constraint_norms(-1)
+    hb, mb = b.ev.constraint_norms(-1)
+    return {"coarse_steps": steps, "max_rel_dev": float(rel.max()),
+            "max_rel_dev_field": int(rel.argmax()), "h_l2_fp64": ha, "h_l2_mixed": hb,
+            "h_l2_ratio": hb / ha if ha else None, "m_l2_ratio": mb / ma if ma else None}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="granite", choices=["granite", "reference"])
-    ap.add_argument("--workload", default="single_puncture_128", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--variant", default="smem", choices=["global", "smem"],
-                    help="stage-kernel variant: stencils from global memory or staged in shared memory")
+    ap.add_argument("--workload", default="binary_bl_4level", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
+                    help="headline precision (default: mixed for hierarchies, fp64 for single blocks)")
+    ap.add_argument("--variant", default="global",
+                    choices=["global", "smem", "global_r168", "global_r128"],
+                    help="stage-kernel variant: stencils from global memory (optionally register-capped) "
+                         "or staged in shared memory")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison run")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -221,13 +352,15 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     w = WORKLOADS[args.workload]
+    hier = w["kind"] == "hier"
+    precision = args.precision or ("mixed" if hier else "fp64")
 
     import torch
     import torch.distributed as dist
     if world > 1:
         import datetime
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     if args.impl == "reference":
         rc = run_reference(args, w, rank, world)
@@ -237,124 +370,105 @@ def main():
         return rc
 
     import granite_b200 as gb
-    prec = gb.PRECISION_FP64 if args.precision == "fp64" else gb.PRECISION_MIXED
-    block = make_state(gb, w)
-    variant = gb.VARIANT_SMEM if args.variant == "smem" else gb.VARIANT_GLOBAL
-    ev = gb.Evolver(gb.CCZ4Params(device=local), variant)
-    ev.add_block(block)
-    ev.commit()
-    ev.upload()
-    dt = 0.25 * block.dx(0)
-    bc = w["bc"]
-    pts = w["n"] ** 3
-    stream = torch.cuda.ExternalStream(ev.stream_handle(), device=local)
+    variant = gb.VARIANT_NAMES[args.variant]
+    kname = "ccz4_stage_smem_kernel" if variant == gb.VARIANT_SMEM else "ccz4_stage_kernel"
+    prec = gb.PRECISION_MIXED if precision == "mixed" else gb.PRECISION_FP64
+    run = Runner(gb, args.workload, w, prec, variant, local)
+    compare = None
+    if hier and prec == gb.PRECISION_MIXED and not args.no_compare:
+        compare = Runner(gb, args.workload, w, gb.PRECISION_FP64, variant, local)
 
-    for _ in range(args.warmup):
-        ev.rk3_step(0, dt, prec, bc)
-    ev.sync()
+    for r in (run, compare):
+        if r is None:
+            continue
+        for _ in range(args.warmup):
+            r.step()
+        r.ev.sync()
+    # mixed vs FP64 after the warm-up steps: the reference formulation itself
+    # collapses the lapse and diverges on these punctures at t ~ 1.9 M once they
+    # are resolved at dx <= 0.125, so accuracy is compared before that
+    acc = accuracy(gb, compare, run, args.warmup) if compare is not None else None
 
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
-    n0 = ev.launch_count()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize(local)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        ev.rk3_step(0, dt, prec, bc)
-    e1.record(stream)
-    ev.sync()
-    torch.cuda.synchronize(local)
-    if world > 1:
-        dist.barrier()
-    ms = e0.elapsed_time(e1)
-    launches = ev.launch_count() - n0
+    ms, launches = timed_steps(torch, dist, world, local, run, args.steps)
     clocks = sampler.stop()
-    ms_t = torch.tensor([ms], device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = pts * args.steps * world / (ms_max / 1000.0)
+    value = run.points_per_step * args.steps * world / (ms / 1000.0)
+    cmp_line = None
+    if compare is not None:
+        cms, _ = timed_steps(torch, dist, world, local, compare, args.steps)
+        cvalue = compare.points_per_step * args.steps * world / (cms / 1000.0)
+        # the same FP64 kernel launched block by block without graphs (a per-block
+        # drop-in of the reference's per-GridBlock calls)
+        ksteps = max(1, min(args.steps, 5))
+        compare.ev.set_batching(False)
+        ums, _ = timed_steps(torch, dist, world, local, compare, ksteps)
+        compare.ev.set_batching(True)
+        uvalue = compare.points_per_step * ksteps * world / (ums / 1000.0)
+        cmp_line = {"fp64_value": cvalue, "fp64_ms_per_step": cms / args.steps,
+                    "mixed_over_fp64": value / cvalue,
+                    "fp64_unbatched_value": uvalue, "fp64_unbatched_ms_per_step": ums / ksteps,
+                    "fp64_unbatched_steps": ksteps, "mixed_over_fp64_unbatched": value / uvalue}
+        compare.ev.close()
+        compare = None
 
-    # roofline pass: every stage launch bracketed by events on the library stream
-    prof_steps = min(args.steps, 20)
-    ev.set_profiling(True)
-    ev.profile_reset()
-    for _ in range(prof_steps):
-        ev.rk3_step(0, dt, prec, bc)
-    st_ms, st_n = ev.profile(gb.KERNEL_STAGE)
-    gh_ms, gh_n = ev.profile(gb.KERNEL_GHOST)
-    ev.set_profiling(False)
-    peak, peak_kind = measured_peaks()
-    bytes_per_launch = BYTES_PER_POINT_UPDATE * pts / 3.0
-    avg_launch_ms = st_ms / max(st_n, 1)
-    achieved = bytes_per_launch / (avg_launch_ms / 1000.0) / 1e9
-    kname = "ccz4_stage_smem_kernel" if variant == gb.VARIANT_SMEM else "ccz4_stage_kernel"
-    traffic = ncu_traffic(args.workload, kname)
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic,
-                "peak_source": peak_kind,
-                "kernel": "ccz4_stage_smem_kernel" if variant == gb.VARIANT_SMEM else "ccz4_stage_kernel",
-                "avg_launch_ms": avg_launch_ms,
-                "stage_share_of_step": st_ms / max(st_ms + gh_ms, 1e-12),
-                "algorithmic_bytes_per_launch": bytes_per_launch}
+    prof_steps = max(1, min(args.steps, 5 if hier else 20))
+    rl = roofline(gb, run, args.workload, prof_steps, kname)
 
     # e2e through the C ABI with host buffers (pinned), copies inside the timed region
-    host = torch.empty(block.array.size, dtype=torch.float64, pin_memory=True)
-    hview = host.numpy().reshape(block.array.shape)
-    hview[...] = block.array
-    e2e_steps = max(1, min(args.steps, 20))
-    ev.sync()
+    hosts = []
+    for i, b in enumerate(run.blocks):
+        t = torch.empty(b.array.size, dtype=torch.float64, pin_memory=True)
+        v = t.numpy().reshape(b.array.shape)
+        run.ev.download(i, v)
+        hosts.append((t, v))
+    e2e_steps = max(1, min(args.steps, 3 if hier else 20))
+    run.ev.sync()
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
-    x0 = torch.cuda.Event(enable_timing=True)
-    x1 = torch.cuda.Event(enable_timing=True)
-    x0.record(stream)
     for _ in range(e2e_steps):
-        ev.upload(0, hview)
-        ev.rk3_step(0, dt, prec, bc)
-        ev.download(0, hview)
-    x1.record(stream)
-    ev.sync()
-    e2e_ms = x0.elapsed_time(x1)
-    wall_ms = (time.perf_counter() - t0) * 1000.0
-    e2e_ms = max(e2e_ms, wall_ms)
+        for i, (_, v) in enumerate(hosts):
+            run.ev.upload(i, v)
+        run.step()
+        for i, (_, v) in enumerate(hosts):
+            run.ev.download(i, v)
+    run.ev.sync()
+    e2e_ms = (time.perf_counter() - t0) * 1000.0
     e_t = torch.tensor([e2e_ms], device=f"cuda:{local}")
     if world > 1:
         dist.all_reduce(e_t, op=dist.ReduceOp.MAX)
-    e2e_val = pts * e2e_steps * world / (float(e_t.item()) / 1000.0)
-    state_bytes = block.array.nbytes
+    e2e_val = run.points_per_step * e2e_steps * world / (float(e_t.item()) / 1000.0)
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cb = cpu_baseline(w)
+            cb = reference_sample(w, seconds_target=15.0)
         except Exception as ex:  # the baseline is a reported number, not the product
             cb = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                   "sample": f"failed: {ex}"}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if prec == 0 else "f32+f64", "data": "synthetic",
-                "config": {"workload": args.workload, "grid": f"{w['n']}^3", "ghosts": 4,
-                           "fields": NV, "precision": args.precision, "kernel_variant": args.variant,
-                           "points_per_step": pts, "dt": dt,
-                           "l2": f"inputs larger than L2: {3 * state_bytes / 1e9:.2f} GB resident state",
-                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-                "roofline": roofline,
-                "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
-                        "d2h_bytes_per_step": state_bytes, "steps": e2e_steps},
-                "cpu_baseline": cb,
-                "clocks": clocks,
-                "gpu_launches": launches}
+        cfg = {"workload": args.workload, "precision": precision, "kernel_variant": args.variant,
+               "ghosts": 4, "fields": NV, "point_updates_per_step": run.points_per_step, "dt": run.dt,
+               "l2": f"inputs larger than L2: {3 * run.state_bytes / 1e9:.2f} GB resident state",
+               "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+        cfg.update(run.config())
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+f64" if prec == gb.PRECISION_MIXED else "f64", "data": "synthetic",
+                "config": cfg, "roofline": rl,
+                "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": run.state_bytes,
+                        "d2h_bytes_per_step": run.state_bytes, "steps": e2e_steps},
+                "cpu_baseline": cb, "clocks": clocks, "gpu_launches": launches}
+        if cmp_line:
+            line["fp64_plain"] = cmp_line
+        if acc:
+            line["accuracy_mixed_vs_fp64"] = acc
         print(json.dumps(line))
-    ev.close()
+    run.ev.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

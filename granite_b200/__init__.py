@@ -31,7 +31,8 @@ BC_PERIODIC = 1
 AMR_REFERENCE = 0
 AMR_GHOSTS = 1
 KERNEL_STAGE, KERNEL_GHOST, KERNEL_TRANSFER, KERNEL_CONSTRAINTS = 0, 1, 2, 3
-VARIANT_GLOBAL, VARIANT_SMEM = 0, 1
+VARIANT_GLOBAL, VARIANT_SMEM, VARIANT_GLOBAL_R168, VARIANT_GLOBAL_R128 = 0, 1, 2, 3
+VARIANT_NAMES = {"global": 0, "smem": 1, "global_r168": 2, "global_r128": 3}
 
 _ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "no sm_100 device", -4: "out of memory",
            -5: "non-finite state", -6: "unsupported", -7: "timeout"}
@@ -101,6 +102,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_profile_get.argtypes = [vp, C.c_int, dp, C.POINTER(C.c_longlong)]
     lib.granite_ccz4_get_stream.argtypes = [vp, C.POINTER(vp)]
     lib.granite_ccz4_set_kernel_variant.argtypes = [vp, C.c_int]
+    lib.granite_ccz4_set_batching.argtypes = [vp, C.c_int]
     lib.granite_ccz4_get_kernel_variant.argtypes = [vp, C.POINTER(C.c_int)]
     _LIB = lib
     return lib
@@ -328,6 +330,9 @@ class Evolver:
         self.committed = False
         if variant is not None:
             self.ctx.check(self.ctx.lib.granite_ccz4_set_kernel_variant(self.ctx.h, variant))
+
+    def set_batching(self, batched: bool):
+        self.ctx.check(self.ctx.lib.granite_ccz4_set_batching(self.ctx.h, int(bool(batched))))
 
     def variant(self) -> int:
         v = C.c_int()

@@ -39,6 +39,8 @@ struct LevelLists {
     GhostItem* d_ghost = nullptr;
     int nghost = 0;
     long long interior_points = 0;
+    // per block of the level: [first, first + count) of its tiles / ghost chunks
+    std::vector<std::pair<int, int>> tile_range, ghost_range;
 };
 
 // Device copy of a list of transfer boxes and the chunks that cover them.
@@ -61,6 +63,9 @@ struct LevelXfer {
     XferList copy;                  // same-level ghost exchange (GRANITE_AMR_GHOSTS)
     std::vector<XferList> restrict_;  // into this level from level+1; one list per launch
     unsigned char* d_facemask = nullptr;  // faces left to the zero-gradient fill (REFERENCE)
+    GhostSrc* d_src = nullptr;            // one source per ghost cell of the level (GHOSTS)
+    long long nsrc = 0;
+    std::vector<std::pair<long long, long long>> src_range;  // per block: first item, count
 };
 
 // device copy of a host vector (nullptr for an empty one)
@@ -84,7 +89,8 @@ long long cells_of(const granite_block_desc& b) {
 struct Ctx {
     granite_ccz4_params p{};
     int device = 0;
-    int variant = VARIANT_SMEM;  // stage-kernel variant (granite_ccz4_set_kernel_variant)
+    int variant = VARIANT_GLOBAL;  // stage-kernel variant (granite_ccz4_set_kernel_variant)
+    bool batched = true;           // one launch per level and stage + CUDA graphs (else per block, eager)
     cudaStream_t stream = nullptr;
     std::string err;
     long long launches = 0;
@@ -184,12 +190,31 @@ DevBlock make_devblock(const granite_block_desc& b, double sigma) {
     return d;
 }
 
-void tiles_of(int block, const granite_block_desc& b, std::vector<Tile>& out, int variant) {
+// Tiles of one block. adaptive (global-load stage kernels only): pick the tile
+// width w in {32, 16, 8} (128 / w rows) that leaves the fewest idle threads on
+// this block's x-y face, preferring the wider tile on ties (longer coalesced rows).
+void tiles_of(int block, const granite_block_desc& b, std::vector<Tile>& out, int variant, bool adaptive = false) {
     int TX, TY, TZ;
     stage_tile_dims(variant, &TX, &TY, &TZ);
+    int w = 0;
+    if (adaptive) {
+        long long best = -1;
+        for (int cand : {32, 16, 8}) {
+            const int h = 128 / cand;
+            const long long cells = (long long)((b.ncells[0] + cand - 1) / cand) * cand *
+                ((b.ncells[1] + h - 1) / h) * h;
+            if (best < 0 || cells < best) {
+                best = cells;
+                w = cand;
+            }
+        }
+        TX = w;
+        TY = 128 / w;
+        TZ = 1;
+    }
     for (int k = 0; k < b.ncells[2]; k += TZ)
         for (int j = 0; j < b.ncells[1]; j += TY)
-            for (int i = 0; i < b.ncells[0]; i += TX) out.push_back(Tile{block, i, j, k});
+            for (int i = 0; i < b.ncells[0]; i += TX) out.push_back(Tile{block, i, j, k, w});
 }
 
 long long ghost_count(const granite_block_desc& b) {
@@ -332,6 +357,14 @@ int granite_ccz4_profile_get(void* h, int cls, double* ms, long long* n) {
     return GRANITE_OK;
 }
 
+int granite_ccz4_set_batching(void* h, int batched) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    CK(drain_profile(c), "profile drain");
+    c->batched = batched != 0;
+    return GRANITE_OK;
+}
+
 int granite_ccz4_set_kernel_variant(void* h, int variant) {
     Ctx* c = static_cast<Ctx*>(h);
     if (!c) return GRANITE_ERR_INVALID;
@@ -426,6 +459,7 @@ int granite_ccz4_destroy(void* h) {
             free_xfer(X.copy);
             for (auto& r : X.restrict_) free_xfer(r);
             cudaFree(X.d_facemask);
+            cudaFree(X.d_src);
         }
     cudaFree(c->d_blocks);
     cudaFree(c->arena);
@@ -651,9 +685,12 @@ int granite_ccz4_commit(void* h) {
         for (size_t i = 0; i < c->descs.size(); ++i) {
             if (c->descs[i].level != L) continue;
             ll.blocks.push_back((int)i);
-            tiles_of((int)i, c->descs[i], tiles, c->variant);
+            const int t0 = (int)tiles.size(), g0 = (int)ghosts.size();
+            tiles_of((int)i, c->descs[i], tiles, c->variant, c->variant != VARIANT_SMEM);
             tiles_of((int)i, c->descs[i], mtiles, VARIANT_GLOBAL);
             ghost_chunks_of((int)i, c->descs[i], ghosts);
+            ll.tile_range.push_back({t0, (int)tiles.size() - t0});
+            ll.ghost_range.push_back({g0, (int)ghosts.size() - g0});
             ll.interior_points += (long long)c->descs[i].ncells[0] * c->descs[i].ncells[1] * c->descs[i].ncells[2];
         }
         CK(upload_vec(tiles, &ll.d_tiles, c->stream), "upload tiles");
@@ -709,38 +746,71 @@ int granite_ccz4_download_block(void* h, int i, double* host) {
 // stepping
 // ---------------------------------------------------------------------------
 
+// The fused stage kernel over one level: one launch over the whole work-list,
+// or (unbatched) one launch per block.
+static cudaError_t level_stage(Ctx* c, LevelLists& L, int precision, const StageArgs& a, long long* n) {
+    if (c->batched) {
+        ++*n;
+        return timed(c, GRANITE_KERNEL_STAGE, [&] {
+            return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, c->stream);
+        });
+    }
+    for (const auto& r : L.tile_range) {
+        ++*n;
+        cudaError_t e = timed(c, GRANITE_KERNEL_STAGE, [&] {
+            return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, L.d_tiles + r.first, r.second, a,
+                                c->stream);
+        });
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// A block-local ghost fill over one level (batched or per block).
+static cudaError_t level_ghost(Ctx* c, LevelLists& L, int mode, int slot, const unsigned char* mask, long long* n) {
+    if (c->batched) {
+        ++*n;
+        return timed(c, GRANITE_KERNEL_GHOST, [&] {
+            return launch_ghost_fill(mode, c->d_blocks, L.d_ghost, L.nghost, slot, mask, c->stream);
+        });
+    }
+    for (const auto& r : L.ghost_range) {
+        ++*n;
+        cudaError_t e = timed(c, GRANITE_KERNEL_GHOST, [&] {
+            return launch_ghost_fill(mode, c->d_blocks, L.d_ghost + r.first, r.second, slot, mask, c->stream);
+        });
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 static cudaError_t enqueue_level_step(Ctx* c, int level, double dt, int precision, int bc, bool prefill,
                                       long long* nl) {
     LevelLists& L = c->levels[level];
     const int level_mode = (bc == GRANITE_BC_PERIODIC) ? GHOST_PERIODIC : GHOST_ZERO_GRADIENT;
     const int outer_mode = (bc == GRANITE_BC_PERIODIC) ? GHOST_PERIODIC : GHOST_SOMMERFELD;
-    cudaStream_t s = c->stream;
     cudaError_t e;
     long long n = 0;
     // amr.cpp:319 level fill before the step (only when the state changed since the last one)
-    if (prefill) {
-        if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(level_mode, c->d_blocks, L.d_ghost, L.nghost, 0, nullptr, s); }))) return e;
-        ++n;
-    }
+    if (prefill && (e = level_ghost(c, L, level_mode, 0, nullptr, &n))) return e;
     StageArgs a = base_args(c);
     // stage 1: u1 = u + dt L(u)                       main.cpp:673
     a.in_sel = 0; a.n_sel = 0; a.out_sel = 1; a.final_stage = 0;
     a.a1 = 1.0; a.a2 = 0.0; a.a3dt = 1.0 * dt;
-    if ((e = timed(c, GRANITE_KERNEL_STAGE, [&] { return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, s); }))) return e;
-    if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(outer_mode, c->d_blocks, L.d_ghost, L.nghost, 1, nullptr, s); }))) return e;
+    if ((e = level_stage(c, L, precision, a, &n))) return e;
+    if ((e = level_ghost(c, L, outer_mode, 1, nullptr, &n))) return e;
     // stage 2: u2 = 3/4 u + 1/4 u1 + 1/4 dt L(u1)      main.cpp:679
     a.in_sel = 1; a.n_sel = 0; a.out_sel = 2;
     a.a1 = 0.75; a.a2 = 0.25; a.a3dt = 0.25 * dt;
-    if ((e = timed(c, GRANITE_KERNEL_STAGE, [&] { return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, s); }))) return e;
-    if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(outer_mode, c->d_blocks, L.d_ghost, L.nghost, 2, nullptr, s); }))) return e;
+    if ((e = level_stage(c, L, precision, a, &n))) return e;
+    if ((e = level_ghost(c, L, outer_mode, 2, nullptr, &n))) return e;
     // stage 3: u = 1/3 u + 2/3 u2 + 2/3 dt L(u2), floors, det/trace   main.cpp:685-687
     a.in_sel = 2; a.n_sel = 0; a.out_sel = 0; a.final_stage = 1;
     a.a1 = 1.0 / 3.0; a.a2 = 2.0 / 3.0; a.a3dt = (2.0 / 3.0) * dt;
-    if ((e = timed(c, GRANITE_KERNEL_STAGE, [&] { return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, s); }))) return e;
+    if ((e = level_stage(c, L, precision, a, &n))) return e;
     // main.cpp:689 outer BC on u is overwritten by the level fill of amr.cpp:329,
     // so only the level fill runs.
-    if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] { return launch_ghost_fill(level_mode, c->d_blocks, L.d_ghost, L.nghost, 0, nullptr, s); }))) return e;
-    n += 6;
+    if ((e = level_ghost(c, L, level_mode, 0, nullptr, &n))) return e;
     *nl = n;
     return cudaSuccess;
 }
@@ -757,7 +827,7 @@ int granite_ccz4_rk3_step(void* h, int level, double dt, int precision, int bc) 
     if (!std::isfinite(dt)) return fail(c, GRANITE_ERR_INVALID, "dt must be finite");
     CK(cudaSetDevice(c->device), "cudaSetDevice");
     const bool prefill = !c->level_ghosts_valid[level];
-    if (c->profiling) {
+    if (c->profiling || !c->batched) {
         long long nl = 0;
         cudaError_t e = enqueue_level_step(c, level, dt, precision, bc, prefill, &nl);
         if (e != cudaSuccess) return cuda_fail(c, e, "enqueue step");
@@ -891,10 +961,9 @@ int build_ghosts_mode(Ctx* c) {
                 copies.push_back(x);
             }
         CK(upload_xfer(copies, X[L].copy, c->stream), "upload copy boxes");
-        if (L == 0) continue;
         // prolongation into the six ghost slabs of each fine block
         std::vector<XferBox> pro;
-        for (int f : blocks) {
+        for (int f : (L > 0 ? blocks : std::vector<int>())) {
             const auto& fd = c->descs[f];
             Interval full[3], in[3];
             for (int d = 0; d < 3; ++d) {
@@ -931,7 +1000,47 @@ int build_ghosts_mode(Ctx* c) {
             }
         }
         CK(upload_xfer(pro, X[L].prolong, c->stream), "upload prolongation boxes");
+        // one source per ghost cell: same-level neighbour over coarse block over own fill
+        {
+            std::vector<GhostSrc> items;
+            X[L].src_range.clear();
+            for (int f : blocks) {
+                const long long first = (long long)items.size();
+                const auto& fd = c->descs[f];
+                const int T0 = fd.ncells[0] + 2 * NG, T1 = fd.ncells[1] + 2 * NG, T2 = fd.ncells[2] + 2 * NG;
+                std::vector<std::pair<int, int>> src((size_t)T0 * T1 * T2, {-1, -1});
+                auto each = [&](const XferBox& x, auto&& fn) {
+                    for (int k = 0; k < x.n[2]; ++k)
+                        for (int j = 0; j < x.n[1]; ++j)
+                            for (int i = 0; i < x.n[0]; ++i)
+                                fn(x.d0[0] + i + T0 * (x.d0[1] + j + T1 * (x.d0[2] + k)), i, j, k);
+                };
+                for (const auto& x : pro)
+                    if (x.dst == f) each(x, [&](int cell, int, int, int) { src[cell] = {x.src, -1}; });
+                for (const auto& x : copies)
+                    if (x.dst == f) {
+                        const auto& sd = c->descs[x.src];
+                        const int S0 = sd.ncells[0] + 2 * NG, S1 = sd.ncells[1] + 2 * NG;
+                        each(x, [&](int cell, int i, int j, int k) {
+                            src[cell] = {x.src, x.s0[0] + i + S0 * (x.s0[1] + j + S1 * (x.s0[2] + k))};
+                        });
+                    }
+                for (int k = 0; k < T2; ++k)
+                    for (int j = 0; j < T1; ++j)
+                        for (int i = 0; i < T0; ++i) {
+                            const bool interior = i >= NG && i < T0 - NG && j >= NG && j < T1 - NG && k >= NG &&
+                                k < T2 - NG;
+                            if (interior) continue;
+                            const int cell = i + T0 * (j + T1 * k);
+                            items.push_back(GhostSrc{f, cell, src[cell].first, src[cell].second});
+                        }
+                X[L].src_range.push_back({first, (long long)items.size() - first});
+            }
+            CK(upload_vec(items, &X[L].d_src, c->stream), "upload ghost sources");
+            X[L].nsrc = (long long)items.size();
+        }
         // restriction into level L-1 from level L
+        if (L == 0) continue;
         std::vector<XferBox> res;
         for (int cb : c->levels[L - 1].blocks)
             for (int f : blocks) {
@@ -1067,34 +1176,26 @@ cudaError_t fill_level(Ctx* c, int L, int slot, bool level_fill, int mode, long 
                 ++*n;
             }
             const int gm = L > 0 ? GHOST_ZERO_GRADIENT_MASKED : GHOST_ZERO_GRADIENT;
-            if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] {
-                     return launch_ghost_fill(gm, c->d_blocks, ll.d_ghost, ll.nghost, slot, X.d_facemask, c->stream);
-                 })))
-                return e;
-        } else {  // applyOuterBC on every block (main.cpp:351-521)
-            if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] {
-                     return launch_ghost_fill(GHOST_SOMMERFELD, c->d_blocks, ll.d_ghost, ll.nghost, slot, nullptr,
-                                              c->stream);
-                 })))
-                return e;
+            return level_ghost(c, ll, gm, slot, X.d_facemask, n);
         }
-        ++*n;
-        return cudaSuccess;
+        // applyOuterBC on every block (main.cpp:351-521)
+        return level_ghost(c, ll, GHOST_SOMMERFELD, slot, nullptr, n);
     }
-    // GRANITE_AMR_GHOSTS: block-local fill, then coarse data, then same-level neighbours
-    const int base = level_fill ? GHOST_ZERO_GRADIENT : GHOST_SOMMERFELD;
-    if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] {
-             return launch_ghost_fill(base, c->d_blocks, ll.d_ghost, ll.nghost, slot, nullptr, c->stream);
-         })))
-        return e;
-    ++*n;
-    if (L > 0 && X.prolong.nchunks) {
-        if ((e = xfer(c, XFER_PROLONG, X.prolong, slot, 0))) return e;
+    // GRANITE_AMR_GHOSTS: every ghost cell once, from a same-level neighbour if one
+    // covers it, else from the coarse level, else from the block's own fill
+    const int local = level_fill ? GHOST_ZERO_GRADIENT : GHOST_SOMMERFELD;
+    if (c->batched) {
         ++*n;
+        return timed(c, GRANITE_KERNEL_GHOST, [&] {
+            return launch_ghost_sources(c->d_blocks, X.d_src, X.nsrc, slot, local, c->stream);
+        });
     }
-    if (X.copy.nchunks) {
-        if ((e = xfer(c, XFER_COPY, X.copy, slot, slot))) return e;
+    for (const auto& r : X.src_range) {
         ++*n;
+        if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] {
+                 return launch_ghost_sources(c->d_blocks, X.d_src + r.first, r.second, slot, local, c->stream);
+             })))
+            return e;
     }
     return cudaSuccess;
 }
@@ -1110,10 +1211,7 @@ cudaError_t stage(Ctx* c, int L, int precision, int in, int out, double a1, doub
     a.a1 = a1;
     a.a2 = a2;
     a.a3dt = a3dt;
-    ++*n;
-    return timed(c, GRANITE_KERNEL_STAGE, [&] {
-        return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, ll.d_tiles, ll.ntiles, a, c->stream);
-    });
+    return level_stage(c, ll, precision, a, n);
 }
 
 // AMRHierarchy::subcycle(L) with the RK3 step as evolve_func, amr.cpp:303-350.
@@ -1123,13 +1221,7 @@ cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long lon
     if (mode == GRANITE_AMR_REFERENCE && L > 0) {  // amr.cpp:313-318 (the fill below repeats it exactly)
         if ((e = xfer(c, XFER_PROLONG, X.prolong, 0, 0))) return e;
         ++*n;
-        LevelLists& ll = c->levels[L];
-        if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] {
-                 return launch_ghost_fill(GHOST_ZERO_GRADIENT_MASKED, c->d_blocks, ll.d_ghost, ll.nghost, 0,
-                                          X.d_facemask, c->stream);
-             })))
-            return e;
-        ++*n;
+        if ((e = level_ghost(c, c->levels[L], GHOST_ZERO_GRADIENT_MASKED, 0, X.d_facemask, n))) return e;
     } else {
         if ((e = fill_level(c, L, 0, true, mode, n))) return e;  // amr.cpp:319
     }
@@ -1169,7 +1261,7 @@ int granite_ccz4_hierarchy_step(void* h, double dt_coarse, int precision, int am
         r = amr_mode == GRANITE_AMR_GHOSTS ? build_ghosts_mode(c) : build_reference_mode(c);
         if (r) return r;
     }
-    if (c->profiling) {
+    if (c->profiling || !c->batched) {
         long long n = 0;
         cudaError_t e = subcycle(c, 0, dt_coarse, precision, amr_mode, &n);
         if (e != cudaSuccess) return cuda_fail(c, e, "hierarchy step");

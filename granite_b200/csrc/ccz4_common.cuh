@@ -42,6 +42,8 @@ struct DevBlock {
 struct Tile {
     int block;
     int i0, j0, k0;  // interior-relative origin of the tile
+    int w;           // tile width along x for the global-load stage kernels (32, 16 or 8;
+                     // 128 threads cover w x 128/w points); 0 for fixed-shape kernels
 };
 
 // Arguments of one fused RHS launch.

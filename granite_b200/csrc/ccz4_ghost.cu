@@ -31,29 +31,45 @@ __device__ __forceinline__ double falloff(double finf, double fint, double ri, d
 
 __device__ __forceinline__ bool inside(int a, int n) { return a >= NG && a < NG + n; }
 
-// Value the reference's three passes leave in ghost cell (i,j,k): the last
-// pass that writes the cell wins, and each pass reads the value the earlier
-// passes left in the cell it copies from (main.cpp:395-463).
-__device__ double sommerfeld_value(const DevBlock& B, const double* __restrict__ f, double fi, int i, int j, int k) {
-    auto valX = [&](int a, int b, int c) -> double {  // after the x pass; b, c interior
-        if (inside(a, B.n[0])) return __ldg(f + cell_index(B, a, b, c));
-        const int ac = clampi(a, NG, NG + B.n[0] - 1);
-        const double y = coord(B, 1, b), z = coord(B, 2, c);
-        const double ri = sq3(coord(B, 0, ac), y, z), rg = sq3(coord(B, 0, a), y, z);
-        return falloff(fi, __ldg(f + cell_index(B, ac, b, c)), ri, rg);
-    };
-    auto valXY = [&](int a, int b, int c) -> double {  // after the y pass; c interior
-        if (inside(b, B.n[1])) return valX(a, b, c);
-        const int bc = clampi(b, NG, NG + B.n[1] - 1);
-        const double x = coord(B, 0, a), z = coord(B, 2, c);
-        const double ri = sq3(x, coord(B, 1, bc), z), rg = sq3(x, coord(B, 1, b), z);
-        return falloff(fi, valX(a, bc, c), ri, rg);
-    };
-    if (inside(k, B.n[2])) return valXY(i, j, k);
-    const int kc = clampi(k, NG, NG + B.n[2] - 1);
-    const double x = coord(B, 0, i), y = coord(B, 1, j);
-    const double ri = sq3(x, y, coord(B, 2, kc)), rg = sq3(x, y, coord(B, 2, k));
-    return falloff(fi, valXY(i, j, kc), ri, rg);
+// Value the reference's three 1/r passes leave in a ghost cell, with the
+// radii shared by all 22 fields: the passes a ghost
+// cell goes through (x, then y, then z, each only if that coordinate is a
+// ghost) read a chain of cells whose end is an interior cell; every pass is
+// finf + (f - finf) * r_in / r_out with its own pair of radii.
+struct FalloffChain {
+    int npass;
+    long long src;     // interior cell at the end of the chain
+    double ri[3], rg[3];
+};
+
+__device__ FalloffChain falloff_chain(const DevBlock& B, int i, int j, int k) {
+    FalloffChain ch;
+    ch.npass = 0;
+    const bool gx = !inside(i, B.n[0]), gy = !inside(j, B.n[1]), gz = !inside(k, B.n[2]);
+    const int ic = clampi(i, NG, NG + B.n[0] - 1), jc = clampi(j, NG, NG + B.n[1] - 1),
+              kc = clampi(k, NG, NG + B.n[2] - 1);
+    ch.src = cell_index(B, ic, jc, kc);
+    // coordinates seen by each pass (main.cpp:395-463)
+    const double xi = coord(B, 0, ic), xg = coord(B, 0, i);
+    const double yi = coord(B, 1, jc), yg = coord(B, 1, j);
+    const double zi = coord(B, 2, kc), zg = coord(B, 2, k);
+    const double yx = gy ? yi : yg, zx = gz ? zi : zg;  // the x pass runs at (i, jc or j, kc or k)
+    if (gx) {
+        ch.ri[ch.npass] = sq3(xi, yx, zx);
+        ch.rg[ch.npass] = sq3(xg, yx, zx);
+        ++ch.npass;
+    }
+    if (gy) {  // the y pass runs at (i, j, kc or k)
+        ch.ri[ch.npass] = sq3(xg, yi, zx);
+        ch.rg[ch.npass] = sq3(xg, yg, zx);
+        ++ch.npass;
+    }
+    if (gz) {
+        ch.ri[ch.npass] = sq3(xg, yg, zi);
+        ch.rg[ch.npass] = sq3(xg, yg, zg);
+        ++ch.npass;
+    }
+    return ch;
 }
 
 // r-th ghost cell of a block: z slabs first, then y slabs, then x slabs.
@@ -111,9 +127,12 @@ __global__ void ghost_fill_kernel(int mode, const DevBlock* __restrict__ blocks,
     double* base = B.buf[sel];
     const long long c = cell_index(B, i, j, k);
     if (mode == GHOST_SOMMERFELD) {
+        const FalloffChain ch = falloff_chain(B, i, j, k);
         for (int v = 0; v < NV; ++v) {
-            const double* f = base + (long long)v * B.stride;
-            base[(long long)v * B.stride + c] = sommerfeld_value(B, f, f_inf(v), i, j, k);
+            const double fi = f_inf(v);
+            double val = base[(long long)v * B.stride + ch.src];
+            for (int p = 0; p < ch.npass; ++p) val = falloff(fi, val, ch.ri[p], ch.rg[p]);
+            base[(long long)v * B.stride + c] = val;
         }
         return;
     }
@@ -222,7 +241,50 @@ __global__ void xfer_kernel(int kind, const DevBlock* __restrict__ blocks, const
     }
 }
 
+// One thread per listed ghost cell; each cell is written exactly once.
+__global__ void ghost_sources_kernel(const DevBlock* __restrict__ blocks, const GhostSrc* __restrict__ items,
+                                     long long n, int sel, int local_mode) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const GhostSrc it = items[t];
+    const DevBlock& D = blocks[it.dst_block];
+    double* db = D.buf[sel];
+    const int i = it.dst_cell % D.tx, j = (it.dst_cell / D.tx) % D.ty, k = it.dst_cell / (D.tx * D.ty);
+    if (it.src_block >= 0 && it.src_cell >= 0) {  // same-level neighbour
+        const DevBlock& S = blocks[it.src_block];
+        const double* sb = S.buf[sel];
+        for (int v = 0; v < NV; ++v) db[(long long)v * D.stride + it.dst_cell] = __ldg(sb + (long long)v * S.stride + it.src_cell);
+        return;
+    }
+    if (it.src_block >= 0) {  // coarse level
+        const DevBlock& C = blocks[it.src_block];
+        prolong_cell(D, C, i, j, k, db, C.buf[0]);
+        return;
+    }
+    if (local_mode == GHOST_SOMMERFELD) {
+        const FalloffChain ch = falloff_chain(D, i, j, k);
+        for (int v = 0; v < NV; ++v) {
+            const double fi = f_inf(v);
+            double val = db[(long long)v * D.stride + ch.src];
+            for (int p = 0; p < ch.npass; ++p) val = falloff(fi, val, ch.ri[p], ch.rg[p]);
+            db[(long long)v * D.stride + it.dst_cell] = val;
+        }
+        return;
+    }
+    const long long s = cell_index(D, clampi(i, NG, NG + D.n[0] - 1), clampi(j, NG, NG + D.n[1] - 1),
+                                   clampi(k, NG, NG + D.n[2] - 1));
+    for (int v = 0; v < NV; ++v) db[(long long)v * D.stride + it.dst_cell] = db[(long long)v * D.stride + s];
+}
+
 }  // namespace
+
+cudaError_t launch_ghost_sources(const DevBlock* blocks, const GhostSrc* items, long long nitems, int sel,
+                                 int local_mode, cudaStream_t stream) {
+    if (nitems <= 0) return cudaSuccess;
+    ghost_sources_kernel<<<(unsigned)((nitems + 255) / 256), 256, 0, stream>>>(blocks, items, nitems, sel,
+                                                                            local_mode);
+    return cudaGetLastError();
+}
 
 constexpr int GHOST_CHUNK = 256;
 

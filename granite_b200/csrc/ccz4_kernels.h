@@ -11,8 +11,9 @@ enum { EPI_STORE = 0, EPI_RK = 1 };
 
 // Kernel variants of the fused stage: 0 = stencils from global memory
 // (32x4x1 tiles), 1 = fields staged through shared memory with cp.async
-// (16x4x2 tiles). The constraint and KO kernels always use variant-0 tiles.
-enum { VARIANT_GLOBAL = 0, VARIANT_SMEM = 1, NUM_VARIANTS = 2 };
+// (16x4x2 tiles); 2, 3 = variant 0 with the registers capped at 168 / 128 per
+// thread (3 / 4 CTAs per SM). The constraint and KO kernels always use variant-0 tiles.
+enum { VARIANT_GLOBAL = 0, VARIANT_SMEM = 1, VARIANT_GLOBAL_R168 = 2, VARIANT_GLOBAL_R128 = 3, NUM_VARIANTS = 4 };
 
 // Tile shape of a stage-kernel variant (points per CTA along x, y, z).
 int stage_tile_dims(int variant, int* tx, int* ty, int* tz);
@@ -70,6 +71,20 @@ enum XferKind { XFER_COPY = 0, XFER_PROLONG = 1, XFER_RESTRICT = 2 };
 // Transfers of slot src_sel of the source blocks into slot dst_sel of the destinations.
 cudaError_t launch_xfer(int kind, const DevBlock* blocks, const XferBox* boxes, const BoxChunk* chunks,
                         int nchunks, int dst_sel, int src_sel, cudaStream_t stream);
+
+// One ghost cell of a level and where its value comes from (GRANITE_AMR_GHOSTS):
+//   src_block >= 0, src_cell >= 0: copy of that cell of a same-level block
+//   src_block >= 0, src_cell <  0: prolongation from that coarse block
+//   src_block <  0               : the block's own fill (zero-gradient or 1/r falloff)
+struct GhostSrc {
+    int dst_block, dst_cell, src_block, src_cell;
+};
+
+// Every listed ghost cell written once: copies and local fills read slot
+// `sel`, prolongations read slot 0 of the coarse block. local_mode:
+// GHOST_ZERO_GRADIENT or GHOST_SOMMERFELD.
+cudaError_t launch_ghost_sources(const DevBlock* blocks, const GhostSrc* items, long long nitems, int sel,
+                                 int local_mode, cudaStream_t stream);
 
 // Constraint monitor (ccz4.cpp:941-1159) over a tile work-list. Writes ham /
 // mom (single-block drop-in; may be null) and per-CTA partial sums of H^2 and

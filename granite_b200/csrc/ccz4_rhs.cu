@@ -536,13 +536,18 @@ __device__ __forceinline__ void stage_epilogue(const DevBlock& B, const StageArg
     for (int v = 0; v < NV; ++v) out[(long long)v * st + c] = r[v];
 }
 
-// Variant 0: stencils from global memory, one thread per point.
-template <typename P, int EPI, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TX* TY* TZ)
+// Variants 0, 2, 3: stencils from global memory, one thread per point; MINB
+// resident CTAs per SM requested from the register allocator (1: up to 255
+// registers, 3: up to 168, 4: up to 128).
+template <typename P, int EPI, int TX, int TY, int TZ, int MINB>
+__global__ void __launch_bounds__(TX* TY* TZ, MINB)
     ccz4_stage_kernel(const DevBlock* __restrict__ blocks, const Tile* __restrict__ tiles, StageArgs A) {
     const Tile t = tiles[blockIdx.x];
     const DevBlock& B = blocks[t.block];
-    const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y, k = t.k0 + threadIdx.z;
+    // 128 threads over a w x (128 / w) tile; w matches the block width (x fastest)
+    const int tid = threadIdx.x + TX * (threadIdx.y + TY * threadIdx.z);
+    const int w = t.w > 0 ? t.w : TX;
+    const int i = t.i0 + tid % w, j = t.j0 + tid / w, k = t.k0;
     if (i >= B.n[0] || j >= B.n[1] || k >= B.n[2]) return;
     const long long c = cell_index(B, i + NG, j + NG, k + NG);
     const double* __restrict__ uin = B.buf[A.in_sel];
@@ -637,11 +642,22 @@ cudaError_t configure_stage_kernels() {
     return configure_smem<float, EPI_RK>();
 }
 
-template <typename P, int EPI>
+template <typename P, int EPI, int MINB>
 static cudaError_t launch_global(const DevBlock* blocks, const Tile* tiles, int ntiles, const StageArgs& args,
                                  cudaStream_t stream) {
-    ccz4_stage_kernel<P, EPI, V0_TX, V0_TY, V0_TZ><<<ntiles, dim3(V0_TX, V0_TY, V0_TZ), 0, stream>>>(blocks, tiles, args);
+    ccz4_stage_kernel<P, EPI, V0_TX, V0_TY, V0_TZ, MINB>
+        <<<ntiles, dim3(V0_TX, V0_TY, V0_TZ), 0, stream>>>(blocks, tiles, args);
     return cudaGetLastError();
+}
+
+template <int MINB>
+static cudaError_t launch_global_any(int precision, int epi, const DevBlock* blocks, const Tile* tiles, int ntiles,
+                                     const StageArgs& args, cudaStream_t stream) {
+    if (precision == 0)
+        return epi == EPI_STORE ? launch_global<double, EPI_STORE, MINB>(blocks, tiles, ntiles, args, stream)
+                                : launch_global<double, EPI_RK, MINB>(blocks, tiles, ntiles, args, stream);
+    return epi == EPI_STORE ? launch_global<float, EPI_STORE, MINB>(blocks, tiles, ntiles, args, stream)
+                            : launch_global<float, EPI_RK, MINB>(blocks, tiles, ntiles, args, stream);
 }
 
 cudaError_t launch_stage(int variant, int precision, int epi, const DevBlock* blocks, const Tile* tiles, int ntiles,
@@ -654,11 +670,9 @@ cudaError_t launch_stage(int variant, int precision, int epi, const DevBlock* bl
         return epi == EPI_STORE ? launch_smem<float, EPI_STORE>(blocks, tiles, ntiles, args, stream)
                                 : launch_smem<float, EPI_RK>(blocks, tiles, ntiles, args, stream);
     }
-    if (precision == 0)
-        return epi == EPI_STORE ? launch_global<double, EPI_STORE>(blocks, tiles, ntiles, args, stream)
-                                : launch_global<double, EPI_RK>(blocks, tiles, ntiles, args, stream);
-    return epi == EPI_STORE ? launch_global<float, EPI_STORE>(blocks, tiles, ntiles, args, stream)
-                            : launch_global<float, EPI_RK>(blocks, tiles, ntiles, args, stream);
+    if (variant == VARIANT_GLOBAL_R168) return launch_global_any<3>(precision, epi, blocks, tiles, ntiles, args, stream);
+    if (variant == VARIANT_GLOBAL_R128) return launch_global_any<4>(precision, epi, blocks, tiles, ntiles, args, stream);
+    return launch_global_any<1>(precision, epi, blocks, tiles, ntiles, args, stream);
 }
 
 

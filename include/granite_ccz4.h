@@ -201,11 +201,21 @@ GRANITE_API int granite_ccz4_profile_get(void* ctx, int kernel_class, double* to
 /* Stage-kernel variant (set before granite_ccz4_commit; no counterpart in the
  * reference): GRANITE_VARIANT_GLOBAL reads stencils from global memory through
  * L1 (32x4x1 tiles); GRANITE_VARIANT_SMEM stages every field of a 16x4x2 tile
- * and its halo through shared memory with cp.async (the default). */
+ * and its halo through shared memory with cp.async. GRANITE_VARIANT_GLOBAL is the
+ * default; in a committed hierarchy its tiles are w x 128/w points with w in {32, 16, 8}
+ * chosen per block to leave the fewest idle threads. */
 #define GRANITE_VARIANT_GLOBAL 0
 #define GRANITE_VARIANT_SMEM 1
+#define GRANITE_VARIANT_GLOBAL_R168 2 /* GLOBAL with at most 168 registers (3 CTAs / SM) */
+#define GRANITE_VARIANT_GLOBAL_R128 3 /* GLOBAL with at most 128 registers (4 CTAs / SM) */
 GRANITE_API int granite_ccz4_set_kernel_variant(void* ctx, int variant);
 GRANITE_API int granite_ccz4_get_kernel_variant(const void* ctx, int* variant);
+
+/* Batching (no counterpart in the reference): 1 (default) = one launch per
+ * level and RK stage over all blocks, each step replayed as one CUDA graph;
+ * 0 = one launch per block and stage, issued eagerly, as a per-block drop-in
+ * of the reference's per-GridBlock operator calls would run. */
+GRANITE_API int granite_ccz4_set_batching(void* ctx, int batched);
 
 /* The context's cudaStream_t, for callers that order their own work or events
  * against the library's. */

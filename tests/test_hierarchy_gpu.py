@@ -122,6 +122,26 @@ def test_hierarchy_graph_replay_deterministic(gb, oracle_lib):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("mode", ["ghosts", "reference"])
+def test_unbatched_equals_batched(gb, oracle_lib, mode):
+    # per-block eager launches compute exactly what the batched graph does
+    h, geoms, levels = small_hierarchy(seed=13, levels=2)
+    states = [oracle_lib.init_brill_lindquist(g, h.masses, h.positions, r_floor=0.5 * g.dx[0]) for g in geoms]
+    dt = 0.25 * geoms[0].dx[0]
+    amr = gb.AMR_GHOSTS if mode == "ghosts" else gb.AMR_REFERENCE
+    outs = []
+    for batched in (True, False):
+        ev, blocks = gpu_hierarchy(gb, geoms, levels, states)
+        ev.set_batching(batched)
+        for _ in range(2):
+            ev.hierarchy_step(dt, gb.PRECISION_FP64, amr)
+        ev.download()
+        outs.append([b.array.copy() for b in blocks])
+        ev.close()
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+
+
 def test_hierarchy_mixed_close_to_fp64(gb, oracle_lib):
     h, geoms, levels = small_hierarchy(seed=11, levels=2)
     states = [oracle.add_noise(oracle_lib.init_brill_lindquist(g, h.masses, h.positions, r_floor=0.5 * g.dx[0]),

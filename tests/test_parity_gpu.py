@@ -75,7 +75,9 @@ def gb():
     return granite_b200
 
 
-VARIANTS = [0, 1]  # stencils from global memory / staged through shared memory
+# stencils from global memory / staged through shared memory / global with 168 and
+# 128 registers per thread
+VARIANTS = [0, 1, 2, 3]
 
 
 def evo(gb, p: Params, precision=0, variant=None):
