@@ -339,8 +339,8 @@ def main():
     ap.add_argument("--workload", default="binary_bl_4level", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="headline precision (default: mixed for hierarchies, fp64 for single blocks)")
-    ap.add_argument("--variant", default="global",
-                    choices=["global", "smem", "global_r168", "global_r128"],
+    ap.add_argument("--variant", default="tma",
+                    choices=["global", "smem", "global_r168", "global_r128", "tma"],
                     help="stage-kernel variant: stencils from global memory (optionally register-capped) "
                          "or staged in shared memory")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -371,7 +371,8 @@ def main():
 
     import granite_b200 as gb
     variant = gb.VARIANT_NAMES[args.variant]
-    kname = "ccz4_stage_smem_kernel" if variant == gb.VARIANT_SMEM else "ccz4_stage_kernel"
+    kname = {gb.VARIANT_SMEM: "ccz4_stage_smem_kernel", gb.VARIANT_TMA: "ccz4_stage_tma_kernel"}.get(
+        variant, "ccz4_stage_kernel")
     prec = gb.PRECISION_MIXED if precision == "mixed" else gb.PRECISION_FP64
     run = Runner(gb, args.workload, w, prec, variant, local)
     compare = None

@@ -31,8 +31,8 @@ BC_PERIODIC = 1
 AMR_REFERENCE = 0
 AMR_GHOSTS = 1
 KERNEL_STAGE, KERNEL_GHOST, KERNEL_TRANSFER, KERNEL_CONSTRAINTS = 0, 1, 2, 3
-VARIANT_GLOBAL, VARIANT_SMEM, VARIANT_GLOBAL_R168, VARIANT_GLOBAL_R128 = 0, 1, 2, 3
-VARIANT_NAMES = {"global": 0, "smem": 1, "global_r168": 2, "global_r128": 3}
+VARIANT_GLOBAL, VARIANT_SMEM, VARIANT_GLOBAL_R168, VARIANT_GLOBAL_R128, VARIANT_TMA = 0, 1, 2, 3, 4
+VARIANT_NAMES = {"global": 0, "smem": 1, "global_r168": 2, "global_r128": 3, "tma": 4}
 
 _ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "no sm_100 device", -4: "out of memory",
            -5: "non-finite state", -6: "unsupported", -7: "timeout"}

@@ -5,14 +5,18 @@
 // stage buffers), per-level tile work-lists for the batched RHS launches,
 // ghost-cell chunk lists for the fills, and a cache of CUDA graphs, one per
 // (level, precision, boundary, dt) step shape.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -23,7 +27,50 @@
 
 using namespace granite_b200;
 
+namespace granite_b200 {
+
+// Tensor map of one block buffer for the TMA stage kernel: 4-D (x, y, z,
+// field) over the cells incl. ghosts, FP64, box = 16x4x4 tile + 4-cell halo,
+// no swizzle, zero fill outside the block. The driver's encoder is looked up
+// once through the runtime (no link against libcuda).
+bool encode_block_tmap(void* map128, const double* base, const DevBlock& d) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        else
+            cudaGetLastError();
+    });
+    if (!encode || !base) return false;
+    // global address 16-byte aligned, every stride a multiple of 16 bytes (x extent even)
+    if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (d.tx & 1) != 0) return false;
+    if (d.tx < TMA_BOX[0] || d.ty < TMA_BOX[1] || d.tz < TMA_BOX[2]) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)d.tx, (cuuint64_t)d.ty, (cuuint64_t)d.tz, (cuuint64_t)NV};
+    const cuuint64_t strides[3] = {(cuuint64_t)d.tx * sizeof(double), (cuuint64_t)d.tx * d.ty * sizeof(double),
+                                   (cuuint64_t)d.stride * sizeof(double)};
+    const cuuint32_t box[4] = {(cuuint32_t)TMA_BOX[0], (cuuint32_t)TMA_BOX[1], (cuuint32_t)TMA_BOX[2], 1};
+    const cuuint32_t estride[4] = {1, 1, 1, 1};
+    const CUresult r = encode(static_cast<CUtensorMap*>(map128), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
+                              const_cast<double*>(base), dims, strides, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+}  // namespace granite_b200
+
 namespace {
+
+static_assert(sizeof(CUtensorMap) == 128, "tensor maps are 128 bytes");
+static_assert(alignof(CUtensorMap) >= 64, "tensor maps are 64-byte aligned");
+
+// The global-load kernels pick their tile width per block; the others use fixed tiles.
+bool adaptive_tiles(int variant) { return variant != VARIANT_SMEM && variant != VARIANT_TMA; }
 
 struct Graph {
     cudaGraphExec_t exec = nullptr;
@@ -32,7 +79,9 @@ struct Graph {
 
 struct LevelLists {
     std::vector<int> blocks;
-    Tile* d_tiles = nullptr;   // stage-kernel tiles (shape of the context's variant)
+    int variant = VARIANT_GLOBAL;  // stage kernel of this level: the context's variant, or GLOBAL
+                                   // when a block cannot be mapped for TMA
+    Tile* d_tiles = nullptr;   // stage-kernel tiles (shape of the level's variant)
     int ntiles = 0;
     Tile* d_mtiles = nullptr;  // constraint-monitor tiles (variant-0 shape)
     int nmtiles = 0;
@@ -89,12 +138,15 @@ long long cells_of(const granite_block_desc& b) {
 struct Ctx {
     granite_ccz4_params p{};
     int device = 0;
-    int variant = VARIANT_GLOBAL;  // stage-kernel variant (granite_ccz4_set_kernel_variant)
+    int variant = VARIANT_TMA;     // stage-kernel variant (granite_ccz4_set_kernel_variant)
     bool batched = true;           // one launch per level and stage + CUDA graphs (else per block, eager)
     cudaStream_t stream = nullptr;
     std::string err;
     long long launches = 0;
     unsigned long long* d_nonfinite = nullptr;
+    unsigned int* d_errflag = nullptr;   // set by a TMA stage kernel whose bounded wait gave up
+    CUtensorMap* d_tmaps = nullptr;      // TMA variant: 3 maps per resident block (slot 0, 1, 2)
+    CUtensorMap* s_tmap = nullptr;       // TMA variant: map of the stateless single-block input
 
     // stateless scratch (grow-only)
     double* s_u = nullptr;
@@ -228,13 +280,14 @@ void ghost_chunks_of(int block, const granite_block_desc& b, std::vector<GhostIt
 
 StageArgs base_args(const Ctx* c) {
     StageArgs a{};
-    a.ko_on = c->p.ko_sigma > 0.0 ? 1 : 0;
     a.chi_c = c->p.chi_blend_center;
     a.chi_w = c->p.chi_blend_width;
     a.kappa1 = c->p.kappa1;
     a.kappa2 = c->p.kappa2;
     a.eta = c->p.eta;
     a.nonfinite = c->d_nonfinite;
+    a.tmaps = c->d_tmaps;
+    a.errflag = c->d_errflag;
     return a;
 }
 
@@ -266,14 +319,26 @@ int ensure_scratch(Ctx* c, size_t cells, int ntiles) {
     return GRANITE_OK;
 }
 
-// Stage one block into the stateless scratch: descriptor + tile list.
-int stage_single(Ctx* c, const granite_block_desc* b, double* u_dev, int* ntiles, cudaStream_t s, int variant) {
-    std::vector<Tile> t;
-    tiles_of(0, *b, t, variant);
-    int r = ensure_scratch(c, (size_t)cells_of(*b), (int)t.size());
+// Stage one block into the stateless scratch: descriptor + tile list (+ the
+// tensor map of its buffer for the TMA variant). *used = the variant the
+// tiles were built for (TMA falls back to GLOBAL for a buffer it cannot map).
+int stage_single(Ctx* c, const granite_block_desc* b, double* u_dev, int* ntiles, cudaStream_t s, int variant,
+                 int* used = nullptr) {
+    int r = ensure_scratch(c, (size_t)cells_of(*b), 1);
     if (r) return r;
     DevBlock d = make_devblock(*b, c->p.ko_sigma);
     d.buf[0] = u_dev ? u_dev : c->s_u;
+    if (variant == VARIANT_TMA) {
+        CUtensorMap m;
+        if (encode_block_tmap(&m, d.buf[0], d))
+            CK(cudaMemcpyAsync(c->s_tmap, &m, sizeof(m), cudaMemcpyHostToDevice, s), "upload tensor map");
+        else
+            variant = VARIANT_GLOBAL;
+    }
+    if (used) *used = variant;
+    std::vector<Tile> t;
+    tiles_of(0, *b, t, variant);
+    if ((r = ensure_scratch(c, (size_t)cells_of(*b), (int)t.size()))) return r;
     CK(cudaMemcpyAsync(c->s_desc, &d, sizeof(d), cudaMemcpyHostToDevice, s), "upload block descriptor");
     CK(cudaMemcpyAsync(c->s_tiles, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice, s), "upload tiles");
     *ntiles = (int)t.size();
@@ -424,6 +489,9 @@ int granite_ccz4_create(const granite_ccz4_params* p, void** out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_nonfinite, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(c->d_nonfinite, 0, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_errflag, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemset(c->d_errflag, 0, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMalloc(&c->s_tmap, sizeof(CUtensorMap));
     if (e == cudaSuccess) e = cudaMalloc(&c->s_desc, sizeof(DevBlock));
     if (e == cudaSuccess) e = cudaMalloc(&c->s_sum, 2 * sizeof(double));
     if (e != cudaSuccess) {
@@ -471,6 +539,9 @@ int granite_ccz4_destroy(void* h) {
     cudaFree(c->s_partials);
     cudaFree(c->s_sum);
     cudaFree(c->d_nonfinite);
+    cudaFree(c->d_errflag);
+    cudaFree(c->d_tmaps);
+    cudaFree(c->s_tmap);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return GRANITE_OK;
@@ -484,11 +555,24 @@ int granite_ccz4_last_error(const void* h, char* buf, size_t len) {
     return GRANITE_OK;
 }
 
+// Report (and clear) a bounded wait of the TMA stage kernel that gave up.
+static int check_errflag(Ctx* c) {
+    unsigned int v = 0;
+    CK(cudaMemcpyAsync(&v, c->d_errflag, sizeof(v), cudaMemcpyDeviceToHost, c->stream), "read error flag");
+    CK(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    if (v) {
+        CK(cudaMemsetAsync(c->d_errflag, 0, sizeof(v), c->stream), "reset error flag");
+        CK(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+        return fail(c, GRANITE_ERR_CUDA, "stage kernel: a tensor-map tile load did not complete within its wait limit");
+    }
+    return GRANITE_OK;
+}
+
 int granite_ccz4_sync(void* h) {
     Ctx* c = static_cast<Ctx*>(h);
     if (!c) return GRANITE_ERR_INVALID;
     CK(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
-    return GRANITE_OK;
+    return check_errflag(c);
 }
 
 int granite_ccz4_launch_count(const void* h, long long* n) {
@@ -526,8 +610,8 @@ int granite_ccz4_compute_rhs_device(void* h, const granite_block_desc* b, const 
     if (nm != 0 && nm != 4) return fail(c, GRANITE_ERR_INVALID, "matter sources: pass all four or none");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     CK(cudaSetDevice(c->device), "cudaSetDevice");
-    int nt = 0;
-    if ((r = stage_single(c, b, const_cast<double*>(u_dev), &nt, s, c->variant))) return r;
+    int nt = 0, variant = VARIANT_GLOBAL;
+    if ((r = stage_single(c, b, const_cast<double*>(u_dev), &nt, s, c->variant, &variant))) return r;
     StageArgs a = base_args(c);
     a.in_sel = 0;
     a.rhs = rhs_dev;
@@ -535,7 +619,8 @@ int granite_ccz4_compute_rhs_device(void* h, const granite_block_desc* b, const 
     a.Si = Si;
     a.Sij = Sij;
     a.S = S;
-    CK(launch_stage(c->variant, precision, EPI_STORE, c->s_desc, c->s_tiles, nt, a, s), "launch RHS");
+    a.tmaps = c->s_tmap;  // block 0, slot 0
+    CK(launch_stage(variant, precision, EPI_STORE, c->s_desc, c->s_tiles, nt, a, s), "launch RHS");
     c->launches += 1;
     return GRANITE_OK;
 }
@@ -574,7 +659,7 @@ int granite_ccz4_compute_rhs_host(void* h, const granite_block_desc* b, const do
     if (r) return r;
     CK(cudaMemcpyAsync(rhs, c->s_rhs, N * NV * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H rhs");
     CK(cudaStreamSynchronize(s), "sync");
-    return GRANITE_OK;
+    return check_errflag(c);
 }
 
 int granite_ccz4_apply_dissipation_host(void* h, const granite_block_desc* b, const double* u, double* rhs) {
@@ -676,17 +761,32 @@ int granite_ccz4_commit(void* h) {
     }
     CK(cudaMemsetAsync(c->arena, 0, total, c->stream), "memset arena");
     CK(upload_vec(c->hblocks, &c->d_blocks, c->stream), "upload block table");
+    // TMA variant: one tensor map per (block, slot); a block that cannot be
+    // mapped sends its whole level to the global-load kernel
+    std::vector<char> mapped(c->descs.size(), 0);
+    if (c->variant == VARIANT_TMA) {
+        std::vector<CUtensorMap> maps(3 * c->descs.size());
+        for (size_t i = 0; i < c->descs.size(); ++i) {
+            bool ok = true;
+            for (int sl = 0; sl < 3; ++sl) ok = ok && encode_block_tmap(&maps[3 * i + sl], c->hblocks[i].buf[sl], c->hblocks[i]);
+            mapped[i] = ok;
+        }
+        CK(upload_vec(maps, &c->d_tmaps, c->stream), "upload tensor maps");
+    }
     c->levels.assign(maxlev + 1, LevelLists());
     c->level_ghosts_valid.assign(maxlev + 1, false);
     for (int L = 0; L <= maxlev; ++L) {
         std::vector<Tile> tiles, mtiles;
         std::vector<GhostItem> ghosts;
         LevelLists& ll = c->levels[L];
+        ll.variant = c->variant;
+        for (size_t i = 0; i < c->descs.size(); ++i)
+            if (c->descs[i].level == L && c->variant == VARIANT_TMA && !mapped[i]) ll.variant = VARIANT_GLOBAL;
         for (size_t i = 0; i < c->descs.size(); ++i) {
             if (c->descs[i].level != L) continue;
             ll.blocks.push_back((int)i);
             const int t0 = (int)tiles.size(), g0 = (int)ghosts.size();
-            tiles_of((int)i, c->descs[i], tiles, c->variant, c->variant != VARIANT_SMEM);
+            tiles_of((int)i, c->descs[i], tiles, ll.variant, adaptive_tiles(ll.variant));
             tiles_of((int)i, c->descs[i], mtiles, VARIANT_GLOBAL);
             ghost_chunks_of((int)i, c->descs[i], ghosts);
             ll.tile_range.push_back({t0, (int)tiles.size() - t0});
@@ -752,13 +852,13 @@ static cudaError_t level_stage(Ctx* c, LevelLists& L, int precision, const Stage
     if (c->batched) {
         ++*n;
         return timed(c, GRANITE_KERNEL_STAGE, [&] {
-            return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, c->stream);
+            return launch_stage(L.variant, precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, c->stream);
         });
     }
     for (const auto& r : L.tile_range) {
         ++*n;
         cudaError_t e = timed(c, GRANITE_KERNEL_STAGE, [&] {
-            return launch_stage(c->variant, precision, EPI_RK, c->d_blocks, L.d_tiles + r.first, r.second, a,
+            return launch_stage(L.variant, precision, EPI_RK, c->d_blocks, L.d_tiles + r.first, r.second, a,
                                 c->stream);
         });
         if (e != cudaSuccess) return e;

@@ -53,12 +53,13 @@ struct StageArgs {
     int out_sel;     // slot written
     int final_stage; // 1: apply the algebraic constraints after the floors
     double a1, a2, a3dt;  // out = a1 u^n + a2 u_in + a3dt L(u_in)
-    int ko_on;       // ko_sigma > 0
     double chi_c, chi_w, kappa1, kappa2, eta;
     // standalone RHS output (EPI_STORE): rhs base per block is given by rhs_ptr
     double* rhs;     // single-block RHS destination (EPI_STORE only)
     const double* rho; const double* Si; const double* Sij; const double* S;  // matter (nullable)
     unsigned long long* nonfinite;  // floor hits on non-finite chi/alpha (nullable)
+    const void* tmaps;     // TMA variant: CUtensorMap of (block b, slot s) at tmaps[3 b + s]
+    unsigned int* errflag; // TMA variant: set to 1 when a bounded mbarrier wait gives up (nullable)
 };
 
 __host__ __device__ inline long long cell_index(const DevBlock& b, int i, int j, int k) {

@@ -48,7 +48,7 @@ __device__ void constraint_point(const DevBlock& B, const double* __restrict__ u
     double dg[6][3], Rt[6];
 #pragma unroll
     for (int a = 0; a < 6; ++a) {
-        FieldDer<P> fd = field_der<P, true>(B, FP(GXX + a), beta0, 0.0, false);
+        FieldDer<P> fd = field_der_noko<P, true>(B, FP(GXX + a), beta0, 0.0);
 #pragma unroll
         for (int d = 0; d < 3; ++d) dg[a][d] = fd.d[d];
         Rt[a] = -0.5 * (gtu[0] * fd.h[0] + gtu[3] * fd.h[3] + gtu[5] * fd.h[5] +
@@ -74,7 +74,7 @@ __device__ void constraint_point(const DevBlock& B, const double* __restrict__ u
     double dGh[3][3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        FieldDer<P> fd = field_der<P, false>(B, FP(GHX + a), beta0, 0.0, false);
+        FieldDer<P> fd = field_der_noko<P, false>(B, FP(GHX + a), beta0, 0.0);
 #pragma unroll
         for (int d = 0; d < 3; ++d) dGh[a][d] = fd.d[d];
     }
@@ -107,7 +107,7 @@ __device__ void constraint_point(const DevBlock& B, const double* __restrict__ u
                 Rt[sy(i, j)] += t;
             }
     }
-    FieldDer<P> fchi = field_der<P, true>(B, FP(CHI), beta0, 0.0, false);
+    FieldDer<P> fchi = field_der_noko<P, true>(B, FP(CHI), beta0, 0.0);
     const double c_half = 0.5 / (chi + 1e-30), c_quart = 0.25 / ((chi * chi) + 1e-30);
     double DDchi[6];
 #pragma unroll
@@ -148,12 +148,12 @@ __device__ void constraint_point(const DevBlock& B, const double* __restrict__ u
     double dA[6][3], dK[3];
 #pragma unroll
     for (int a = 0; a < 6; ++a) {
-        FieldDer<P> fd = field_der<P, false>(B, FP(AXX + a), beta0, 0.0, false);
+        FieldDer<P> fd = field_der_noko<P, false>(B, FP(AXX + a), beta0, 0.0);
 #pragma unroll
         for (int d = 0; d < 3; ++d) dA[a][d] = fd.d[d];
     }
     {
-        FieldDer<P> fd = field_der<P, false>(B, FP(KTR), beta0, 0.0, false);
+        FieldDer<P> fd = field_der_noko<P, false>(B, FP(KTR), beta0, 0.0);
 #pragma unroll
         for (int d = 0; d < 3; ++d) dK[d] = fd.d[d];
     }

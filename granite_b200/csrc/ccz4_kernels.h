@@ -12,11 +12,25 @@ enum { EPI_STORE = 0, EPI_RK = 1 };
 // Kernel variants of the fused stage: 0 = stencils from global memory
 // (32x4x1 tiles), 1 = fields staged through shared memory with cp.async
 // (16x4x2 tiles); 2, 3 = variant 0 with the registers capped at 168 / 128 per
-// thread (3 / 4 CTAs per SM). The constraint and KO kernels always use variant-0 tiles.
-enum { VARIANT_GLOBAL = 0, VARIANT_SMEM = 1, VARIANT_GLOBAL_R168 = 2, VARIANT_GLOBAL_R128 = 3, NUM_VARIANTS = 4 };
+// thread (3 / 4 CTAs per SM); 4 = persistent CTAs that stream every field of
+// a 16x4x4 tile and its halo into a ring of shared-memory slots with TMA
+// (cp.async.bulk.tensor) and mbarriers. The constraint and KO kernels always
+// use variant-0 tiles.
+enum {
+    VARIANT_GLOBAL = 0, VARIANT_SMEM = 1, VARIANT_GLOBAL_R168 = 2, VARIANT_GLOBAL_R128 = 3, VARIANT_TMA = 4,
+    NUM_VARIANTS = 5
+};
 
 // Tile shape of a stage-kernel variant (points per CTA along x, y, z).
 int stage_tile_dims(int variant, int* tx, int* ty, int* tz);
+
+// TMA variant: the box (cells incl. the 4-cell halo) one tensor-map load brings
+// in per field, and the tensor map of one 22-field block buffer
+// (dims x, y, z, field; cells incl. ghosts). Returns false when the buffer
+// cannot be described (odd x extent, misaligned base, box larger than the
+// block); such blocks use the global-load kernel.
+constexpr int TMA_BOX[3] = {16 + 8, 4 + 8, 4 + 8};
+bool encode_block_tmap(void* map128, const double* base, const DevBlock& d);
 
 // Per-device kernel attributes (shared-memory opt-in); call with the device current.
 cudaError_t configure_stage_kernels();

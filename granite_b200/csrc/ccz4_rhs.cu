@@ -22,6 +22,11 @@
 // then the Christoffel/Ricci/gauge/KO algebra runs in FP32. chi, the inverse
 // conformal metric, the 1/chi factors, the evolved state and the RK3 combine
 // stay FP64.
+//
+// Control flow: the per-point body is one straight-line sequence (the KO term
+// is always evaluated -- its weights sigma/(64 dx) w_s are zero when KO is off
+// -- and the upwind side is a select, not a branch), so the compiler can
+// schedule the stencil loads of later fields across earlier ones.
 #include "ccz4_common.cuh"
 #include "ccz4_kernels.h"
 #include "ccz4_stencil.cuh"
@@ -45,10 +50,10 @@ struct GlobalSource {
     const DevBlock& B;
     const double* __restrict__ u;
     long long c;
-    bool ko;
     template <bool HESS>
     __device__ __forceinline__ FieldDer<P> der(int v, const double beta[3], P w) {
-        return field_der<P, HESS>(B, u + (long long)v * B.stride + c, beta, w, ko);
+        const long long off[3] = {1, B.tx, (long long)B.tx * B.ty};
+        return field_der_l<P, HESS, true>(B, GlobalLoad{u + (long long)v * B.stride + c}, off, beta, w);
     }
 };
 
@@ -121,7 +126,6 @@ struct SmemSource {
     long long origin;              // global cell index of the tile origin
     int lin;                       // shared offset of this thread's point in a box
     int next;                      // index in FIELD_ORDER of the next field to consume
-    bool ko;
 
     __device__ __forceinline__ void issue(int k) {
         if (k < NV) {
@@ -145,8 +149,127 @@ struct SmemSource {
         const long long off[3] = {1, G::BX, G::BX * G::BY};
         const SharedLoad L{sm + (next % NBUF) * G::BOX + lin};
         ++next;
-        if (ko) return field_der_l<P, HESS, true>(B, L, off, beta, w);
-        return field_der_l<P, HESS, false>(B, L, off, beta, w);
+        return field_der_l<P, HESS, true>(B, L, off, beta, w);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// TMA ring: a persistent CTA walks its tiles (blockIdx.x, + gridDim.x, ...)
+// and consumes a stream of items q = (tile round q / NV, field FIELD_ORDER[q % NV]).
+// Item q is one 24x12x12-cell box (the 16x4x4 tile and its 4-cell halo) of one
+// field, brought into ring slot q % NBUF by a single tensor-map load that
+// completes on that slot's mbarrier. Thread 0 issues item q + NBUF - 1 when
+// the CTA starts on item q, so loads run NBUF - 1 fields ahead and across tile
+// boundaries. Rows of 24 doubles put the 16-wide x rows of a warp in distinct
+// shared-memory banks for every stencil offset.
+// ---------------------------------------------------------------------------
+constexpr int V4_TX = 16, V4_TY = 4, V4_TZ = 4, V4_NT = V4_TX * V4_TY * V4_TZ;
+static_assert(TMA_BOX[0] == V4_TX + 8 && TMA_BOX[1] == V4_TY + 8 && TMA_BOX[2] == V4_TZ + 8, "box = tile + halo");
+
+template <int NBUF>
+struct TmaRing {
+    static constexpr int BX = TMA_BOX[0], BY = TMA_BOX[1], BZ = TMA_BOX[2];
+    static constexpr int BOX = BX * BY * BZ;
+    static constexpr unsigned BYTES = BOX * sizeof(double);  // complete_tx count of one item
+    static_assert(BYTES % 128 == 0, "slots stay 128-byte aligned");
+    static constexpr size_t SMEM = (size_t)NBUF * BYTES + NBUF * sizeof(unsigned long long) + 128;
+};
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// One box of a 4-D tensor map (x, y, z, field) into shared memory.
+__device__ __forceinline__ void tma_load_box(unsigned dst, const void* map, int x, int y, int z, int f,
+                                             unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(dst),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(f), "r"(bar)
+        : "memory");
+}
+
+// Wait limit of one ring slot: 2 s of wall time, then the kernel records the
+// failure in StageArgs::errflag and stops waiting (results are then garbage
+// and the host reports the error).
+constexpr unsigned long long TMA_WAIT_NS = 2000000000ull;
+
+template <typename P, int NBUF>
+struct TmaSource {
+    using R = TmaRing<NBUF>;
+    const DevBlock* blocks;
+    const Tile* tiles;
+    const unsigned char* maps;  // CUtensorMap array, 128 bytes each
+    int ntiles, in_sel;
+    double* ring;      // NBUF slots of R::BOX doubles
+    unsigned bar0;     // shared address of the slot mbarriers (8 bytes apart)
+    const DevBlock* B; // block of the current tile (stencil coefficients)
+    int lin;           // this thread's point within a slot
+    int next;          // next item to consume
+    bool failed;       // a wait of this thread gave up (at item fail_q); thread 0 then stops issuing
+    unsigned int* err;
+    int fail_q;
+
+    // thread 0 only
+    __device__ __forceinline__ void issue(int q) const {
+        const int ti = blockIdx.x + (q / NV) * gridDim.x;
+        if (ti >= ntiles) return;
+        const Tile t = tiles[ti];
+        const int s = q % NBUF;
+        const unsigned bar = bar0 + 8u * s;
+        mbar_expect_tx(bar, R::BYTES);
+        // box origin = tile origin - 4 cells = interior index (cells incl. ghosts start 4 lower)
+        tma_load_box(smem_addr(ring + (size_t)s * R::BOX), maps + (size_t)(3 * t.block + in_sel) * 128, t.i0, t.j0,
+                     t.k0, FIELD_ORDER[q % NV], bar);
+    }
+    __device__ __forceinline__ void wait(int q) {
+        if (failed) return;
+        const unsigned bar = bar0 + 8u * (q % NBUF), parity = (q / NBUF) & 1;
+        unsigned long long t0 = 0;
+        for (unsigned it = 1;; ++it) {
+            if (mbar_try_wait(bar, parity)) return;
+            if ((it & 255u) == 0) {
+                const unsigned long long now = global_ns();
+                if (t0 == 0) {
+                    t0 = now;
+                } else if (now - t0 > TMA_WAIT_NS) {
+                    failed = true;
+                    fail_q = q;
+                    if (err) atomicExch(err, 1u);
+                    return;
+                }
+            }
+        }
+    }
+    // Every thread of the CTA calls der() for every item in order (the call
+    // carries the CTA barrier that frees the slot the next load overwrites).
+    template <bool HESS>
+    __device__ __forceinline__ FieldDer<P> der(int /*v*/, const double beta[3], P w) {
+        __syncthreads();
+        if (threadIdx.x == 0 && !failed) issue(next + NBUF - 1);
+        wait(next);
+        const SharedLoad L{ring + (size_t)(next % NBUF) * R::BOX + lin};
+        ++next;
+        const long long off[3] = {1, R::BX, R::BX * R::BY};
+        return field_der_l<P, HESS, true>(*B, L, off, beta, w);
     }
 };
 
@@ -551,7 +674,7 @@ __global__ void __launch_bounds__(TX* TY* TZ, MINB)
     if (i >= B.n[0] || j >= B.n[1] || k >= B.n[2]) return;
     const long long c = cell_index(B, i + NG, j + NG, k + NG);
     const double* __restrict__ uin = B.buf[A.in_sel];
-    GlobalSource<P> S{B, uin, c, A.ko_on != 0};
+    GlobalSource<P> S{B, uin, c};
     double L[NV];
     ccz4_point<P>(B, uin, c, A, S, L);
     stage_epilogue<EPI>(B, A, c, L);
@@ -584,7 +707,7 @@ __global__ void __launch_bounds__(TX* TY* TZ, 2)
     __syncthreads();
     const double* __restrict__ uin = B.buf[A.in_sel];
     SmemSource<P, TX, TY, TZ, NBUF> S{B, uin, smem, table, cell_index(B, gi0, gj0, gk0),
-                                      (lx + 4) + G::BX * ((ly + 4) + G::BY * (lz + 4)), 0, A.ko_on != 0};
+                                      (lx + 4) + G::BX * ((ly + 4) + G::BY * (lz + 4)), 0};
     S.start();
     // pointwise loads of threads outside the block use a valid cell; their results are dropped
     const int ic = i < B.n[0] ? i : B.n[0] - 1, jc = j < B.n[1] ? j : B.n[1] - 1, kc = k < B.n[2] ? k : B.n[2] - 1;
@@ -595,14 +718,68 @@ __global__ void __launch_bounds__(TX* TY* TZ, 2)
     stage_epilogue<EPI>(B, A, c, L);
 }
 
+// Variant 4: persistent CTAs (grid <= SMs x resident CTAs), one 16x4x4 tile
+// at a time, every field streamed through the TMA ring. Threads of partial
+// tiles (past the block edge) compute on the zero-filled box and store nothing.
+template <typename P, int EPI, int NBUF>
+__global__ void __launch_bounds__(V4_NT, 1)
+    ccz4_stage_tma_kernel(const DevBlock* __restrict__ blocks, const Tile* __restrict__ tiles, int ntiles,
+                          StageArgs A) {
+    using R = TmaRing<NBUF>;
+    extern __shared__ unsigned char smem_raw[];
+    double* ring = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    const unsigned bar0 = smem_addr(ring + (size_t)NBUF * R::BOX);
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < NBUF; ++s) mbar_init(bar0 + 8u * s, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    const int lx = tid % V4_TX, ly = (tid / V4_TX) % V4_TY, lz = tid / (V4_TX * V4_TY);
+    TmaSource<P, NBUF> S{blocks, tiles, static_cast<const unsigned char*>(A.tmaps), ntiles, A.in_sel, ring, bar0,
+                         nullptr, (lx + 4) + R::BX * ((ly + 4) + R::BY * (lz + 4)), 0, false,
+                         A.errflag, 0};
+    if (tid == 0)
+        for (int q = 0; q < NBUF - 1; ++q) S.issue(q);
+    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+        const Tile t = tiles[ti];
+        const DevBlock& B = blocks[t.block];
+        S.B = &B;
+        const int i = t.i0 + lx, j = t.j0 + ly, k = t.k0 + lz;
+        const bool valid = i < B.n[0] && j < B.n[1] && k < B.n[2];
+        // pointwise loads of threads outside the block use a valid cell; their results are dropped
+        const int ic = min(i, B.n[0] - 1), jc = min(j, B.n[1] - 1), kc = min(k, B.n[2] - 1);
+        const long long c = cell_index(B, ic + NG, jc + NG, kc + NG);
+        const double* __restrict__ uin = B.buf[A.in_sel];
+        double L[NV];
+        ccz4_point<P>(B, uin, c, A, S, L);
+        if (valid) stage_epilogue<EPI>(B, A, c, L);
+    }
+    // Every issued item was consumed (issue() skips items past this CTA's last
+    // tile), so no copy into the ring is in flight when the CTA exits. If
+    // thread 0 gave up waiting at item f, it issued nothing after item
+    // f + NBUF - 1: give those loads one more bounded wait before exiting.
+    if (S.failed && tid == 0) {
+        const int f = S.fail_q;
+        S.failed = false;
+        for (int q = f; q < f + NBUF && !S.failed; ++q)
+            if (blockIdx.x + (q / NV) * (int)gridDim.x < ntiles) S.wait(q);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Launchers
 // ---------------------------------------------------------------------------
 constexpr int V0_TX = 32, V0_TY = 4, V0_TZ = 1;
 constexpr int V1_TX = 16, V1_TY = 4, V1_TZ = 2, V1_NBUF = 3;
+constexpr int V4_NBUF = 4;
 
 int stage_tile_dims(int variant, int* tx, int* ty, int* tz) {
-    if (variant == 1) {
+    if (variant == VARIANT_TMA) {
+        *tx = V4_TX;
+        *ty = V4_TY;
+        *tz = V4_TZ;
+    } else if (variant == 1) {
         *tx = V1_TX;
         *ty = V1_TY;
         *tz = V1_TZ;
@@ -632,14 +809,53 @@ static cudaError_t configure_smem() {
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// Persistent grid of the TMA variant on each device: SMs x resident CTAs.
+constexpr int MAX_DEVICES = 64;
+static int g_tma_grid[MAX_DEVICES][2][2];  // [device][precision][epi]
+
+template <typename P, int EPI>
+static cudaError_t configure_tma(int dev, int nsm) {
+    auto k = ccz4_stage_tma_kernel<P, EPI, V4_NBUF>;
+    constexpr size_t bytes = TmaRing<V4_NBUF>::SMEM;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, V4_NT, bytes))) return e;
+    g_tma_grid[dev][sizeof(P) == 8 ? 0 : 1][EPI] = nsm * (per_sm > 0 ? per_sm : 1);
+    return cudaSuccess;
+}
+
+template <typename P, int EPI>
+static cudaError_t launch_tma(const DevBlock* blocks, const Tile* tiles, int ntiles, const StageArgs& args,
+                              cudaStream_t stream) {
+    if (!args.tmaps) return cudaErrorInvalidValue;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const int cap = (dev >= 0 && dev < MAX_DEVICES) ? g_tma_grid[dev][sizeof(P) == 8 ? 0 : 1][EPI] : 0;
+    if (cap <= 0) return cudaErrorInvalidConfiguration;  // configure_stage_kernels() not run on this device
+    const int grid = ntiles < cap ? ntiles : cap;
+    ccz4_stage_tma_kernel<P, EPI, V4_NBUF><<<grid, V4_NT, TmaRing<V4_NBUF>::SMEM, stream>>>(blocks, tiles, ntiles, args);
+    return cudaGetLastError();
+}
+
 // Opt the shared-memory variants into more than 48 KB of dynamic shared memory
-// on the current device (called once per context at creation).
+// on the current device and size the persistent grid (called once per context
+// at creation).
 cudaError_t configure_stage_kernels() {
     cudaError_t e;
     if ((e = configure_smem<double, EPI_STORE>())) return e;
     if ((e = configure_smem<double, EPI_RK>())) return e;
     if ((e = configure_smem<float, EPI_STORE>())) return e;
-    return configure_smem<float, EPI_RK>();
+    if ((e = configure_smem<float, EPI_RK>())) return e;
+    int dev = 0, nsm = 0;
+    if ((e = cudaGetDevice(&dev))) return e;
+    if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev))) return e;
+    if ((e = configure_tma<double, EPI_STORE>(dev, nsm))) return e;
+    if ((e = configure_tma<double, EPI_RK>(dev, nsm))) return e;
+    if ((e = configure_tma<float, EPI_STORE>(dev, nsm))) return e;
+    return configure_tma<float, EPI_RK>(dev, nsm);
 }
 
 template <typename P, int EPI, int MINB>
@@ -663,6 +879,13 @@ static cudaError_t launch_global_any(int precision, int epi, const DevBlock* blo
 cudaError_t launch_stage(int variant, int precision, int epi, const DevBlock* blocks, const Tile* tiles, int ntiles,
                          const StageArgs& args, cudaStream_t stream) {
     if (ntiles <= 0) return cudaSuccess;
+    if (variant == VARIANT_TMA) {
+        if (precision == 0)
+            return epi == EPI_STORE ? launch_tma<double, EPI_STORE>(blocks, tiles, ntiles, args, stream)
+                                    : launch_tma<double, EPI_RK>(blocks, tiles, ntiles, args, stream);
+        return epi == EPI_STORE ? launch_tma<float, EPI_STORE>(blocks, tiles, ntiles, args, stream)
+                                : launch_tma<float, EPI_RK>(blocks, tiles, ntiles, args, stream);
+    }
     if (variant == 1) {
         if (precision == 0)
             return epi == EPI_STORE ? launch_smem<double, EPI_STORE>(blocks, tiles, ntiles, args, stream)

@@ -44,31 +44,30 @@ struct AxisDer {
 
 // Reference-order evaluation (P = double). `ko` accumulates the KO sum across
 // the three axes exactly as ccz4.cpp:912-926 does.
+//
+// The upwind derivative is evaluated without a branch: both +-4 arms are
+// loaded and the side is selected. The beta < 0 form of ccz4.cpp:109-152,
+// inv12h (-25 f0 + 48 f+1 - 36 f+2 + 16 f+3 - 3 f+4), rounded left to right,
+// is bit for bit the negation of the beta >= 0 form applied to the + side
+// (round-to-nearest is odd-symmetric; only the sign of an exact zero differs).
 template <bool WANT_D2, bool WANT_KO, typename L>
 __device__ __forceinline__ AxisDer<double> axis_exact(const L& f, long long s, double f0,
                                                      double beta, double inv12h, double inv12h2,
                                                      const double* kw, double& ko) {
     const double fm1 = f(-s), fp1 = f(s);
     const double fm2 = f(-2 * s), fp2 = f(2 * s);
+    const double fm3 = f(-3 * s), fp3 = f(3 * s);
+    const double fm4 = f(-4 * s), fp4 = f(4 * s);
     AxisDer<double> r;
     // inv12h * (-f[+2] + 8 f[+1] - 8 f[-1] + f[-2])
     r.d1 = RN_MUL(inv12h, RN_ADD(RN_SUB(RN_ADD(-fp2, RN_MUL(8.0, fp1)), RN_MUL(8.0, fm1)), fm2));
-    double fm3 = 0.0, fp3 = 0.0;
-    if (WANT_KO || beta >= 0.0) fm3 = f(-3 * s);
-    if (WANT_KO || !(beta >= 0.0)) fp3 = f(3 * s);
-    if (beta >= 0.0) {
-        const double fm4 = f(-4 * s);
-        // inv12h * (25 f0 - 48 f-1 + 36 f-2 - 16 f-3 + 3 f-4)
-        r.up = RN_MUL(inv12h, RN_ADD(RN_SUB(RN_ADD(RN_SUB(RN_MUL(25.0, f0), RN_MUL(48.0, fm1)), RN_MUL(36.0, fm2)),
-                                            RN_MUL(16.0, fm3)),
-                                     RN_MUL(3.0, fm4)));
-    } else {
-        const double fp4 = f(4 * s);
-        // inv12h * (-25 f0 + 48 f+1 - 36 f+2 + 16 f+3 - 3 f+4)
-        r.up = RN_MUL(inv12h, RN_SUB(RN_ADD(RN_SUB(RN_ADD(RN_MUL(-25.0, f0), RN_MUL(48.0, fp1)), RN_MUL(36.0, fp2)),
-                                            RN_MUL(16.0, fp3)),
-                                     RN_MUL(3.0, fp4)));
-    }
+    const bool pos = beta >= 0.0;
+    const double g1 = pos ? fm1 : fp1, g2 = pos ? fm2 : fp2, g3 = pos ? fm3 : fp3, g4 = pos ? fm4 : fp4;
+    // inv12h * (25 f0 - 48 g1 + 36 g2 - 16 g3 + 3 g4), g = the - side for beta >= 0
+    const double up = RN_MUL(inv12h, RN_ADD(RN_SUB(RN_ADD(RN_SUB(RN_MUL(25.0, f0), RN_MUL(48.0, g1)), RN_MUL(36.0, g2)),
+                                                   RN_MUL(16.0, g3)),
+                                            RN_MUL(3.0, g4)));
+    r.up = pos ? up : -up;
     if (WANT_D2) {
         // inv12h2 * (-f[+2] + 16 f[+1] - 30 f0 + 16 f[-1] - f[-2])
         r.d2 = RN_MUL(inv12h2, RN_SUB(RN_ADD(RN_SUB(RN_ADD(-fp2, RN_MUL(16.0, fp1)), RN_MUL(30.0, f0)),
@@ -90,29 +89,24 @@ __device__ __forceinline__ AxisDer<double> axis_exact(const L& f, long long s, d
     return r;
 }
 
-// Pair-difference evaluation (P = float).
+// Pair-difference evaluation (P = float); the upwind side is selected without
+// a branch as in axis_exact.
 template <bool WANT_D2, bool WANT_KO, typename L>
 __device__ __forceinline__ AxisDer<float> axis_pairs(const L& f, long long s, double f0,
                                                     double beta, double inv12h, double inv12h2, double kocf,
                                                     float& ko) {
     const double fm1 = f(-s), fp1 = f(s);
     const double fm2 = f(-2 * s), fp2 = f(2 * s);
+    const double fm3 = f(-3 * s), fp3 = f(3 * s);
+    const double fm4 = f(-4 * s), fp4 = f(4 * s);
     AxisDer<float> r;
     const float a1 = (float)(fp1 - fm1), a2 = (float)(fp2 - fm2);
     r.d1 = (float)inv12h * (8.0f * a1 - a2);
-    double e;
-    double fm3 = 0.0, fp3 = 0.0;
-    if (WANT_KO || beta >= 0.0) fm3 = f(-3 * s);
-    if (WANT_KO || !(beta >= 0.0)) fp3 = f(3 * s);
-    if (beta >= 0.0) {
-        const double fm4 = f(-4 * s);
-        // 25 f0 - 48 f-1 + 36 f-2 - 16 f-3 + 3 f-4 with weights summing to zero
-        e = 48.0 * (f0 - fm1) - 36.0 * (f0 - fm2) + 16.0 * (f0 - fm3) - 3.0 * (f0 - fm4);
-    } else {
-        const double fp4 = f(4 * s);
-        e = -48.0 * (f0 - fp1) + 36.0 * (f0 - fp2) - 16.0 * (f0 - fp3) + 3.0 * (f0 - fp4);
-    }
-    r.up = (float)inv12h * (float)e;
+    const bool pos = beta >= 0.0;
+    const double g1 = pos ? fm1 : fp1, g2 = pos ? fm2 : fp2, g3 = pos ? fm3 : fp3, g4 = pos ? fm4 : fp4;
+    // 25 f0 - 48 g1 + 36 g2 - 16 g3 + 3 g4 with weights summing to zero; negated for the + side
+    const double e = 48.0 * (f0 - g1) - 36.0 * (f0 - g2) + 16.0 * (f0 - g3) - 3.0 * (f0 - g4);
+    r.up = (float)inv12h * (float)(pos ? e : -e);
     const float t1 = (float)((fp1 - f0) + (fm1 - f0));
     const float t2 = (float)((fp2 - f0) + (fm2 - f0));
     r.d2 = WANT_D2 ? (float)inv12h2 * (16.0f * t1 - t2) : 0.0f;
@@ -179,14 +173,12 @@ __device__ __forceinline__ FieldDer<P> field_der_l(const DevBlock& B, const L& f
     return r;
 }
 
-// Field derivatives straight from global memory.
+// Field derivatives straight from global memory, without the KO term.
 template <typename P, bool HESS>
-__device__ __forceinline__ FieldDer<P> field_der(const DevBlock& B, const double* __restrict__ f,
-                                                 const double beta[3], P w, bool ko_on) {
+__device__ __forceinline__ FieldDer<P> field_der_noko(const DevBlock& B, const double* __restrict__ f,
+                                                      const double beta[3], P w) {
     const long long off[3] = {1, B.tx, (long long)B.tx * B.ty};
-    const GlobalLoad L{f};
-    if (ko_on) return field_der_l<P, HESS, true>(B, L, off, beta, w);
-    return field_der_l<P, HESS, false>(B, L, off, beta, w);
+    return field_der_l<P, HESS, false>(B, GlobalLoad{f}, off, beta, w);
 }
 
 __device__ __forceinline__ int sy(int a, int b) {

@@ -201,13 +201,20 @@ GRANITE_API int granite_ccz4_profile_get(void* ctx, int kernel_class, double* to
 /* Stage-kernel variant (set before granite_ccz4_commit; no counterpart in the
  * reference): GRANITE_VARIANT_GLOBAL reads stencils from global memory through
  * L1 (32x4x1 tiles); GRANITE_VARIANT_SMEM stages every field of a 16x4x2 tile
- * and its halo through shared memory with cp.async. GRANITE_VARIANT_GLOBAL is the
- * default; in a committed hierarchy its tiles are w x 128/w points with w in {32, 16, 8}
- * chosen per block to leave the fewest idle threads. */
+ * and its halo through shared memory with cp.async. In a committed hierarchy the
+ * GLOBAL tiles are w x 128/w points with w in {32, 16, 8} chosen per block to
+ * leave the fewest idle threads. GRANITE_VARIANT_TMA (the default) runs one
+ * persistent CTA per SM that streams every field of a 16x4x4 tile and its
+ * 4-cell halo into a ring of shared-memory slots with tensor-map (TMA) loads;
+ * blocks it cannot map (odd x extent, fewer than 16 x or 4 y/z interior cells)
+ * send their level to GRANITE_VARIANT_GLOBAL. A TMA load that does not complete
+ * within its wait limit makes the next granite_ccz4_sync return GRANITE_ERR_CUDA.
+ * All variants compute identical FP64 results. */
 #define GRANITE_VARIANT_GLOBAL 0
 #define GRANITE_VARIANT_SMEM 1
 #define GRANITE_VARIANT_GLOBAL_R168 2 /* GLOBAL with at most 168 registers (3 CTAs / SM) */
 #define GRANITE_VARIANT_GLOBAL_R128 3 /* GLOBAL with at most 128 registers (4 CTAs / SM) */
+#define GRANITE_VARIANT_TMA 4
 GRANITE_API int granite_ccz4_set_kernel_variant(void* ctx, int variant);
 GRANITE_API int granite_ccz4_get_kernel_variant(const void* ctx, int* variant);
 

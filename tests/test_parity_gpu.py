@@ -76,8 +76,8 @@ def gb():
 
 
 # stencils from global memory / staged through shared memory / global with 168 and
-# 128 registers per thread
-VARIANTS = [0, 1, 2, 3]
+# 128 registers per thread / streamed through a TMA ring by persistent CTAs
+VARIANTS = [0, 1, 2, 3, 4]
 
 
 def evo(gb, p: Params, precision=0, variant=None):
