@@ -1134,6 +1134,11 @@ int build_ghosts_mode(Ctx* c) {
                             const int cell = i + T0 * (j + T1 * k);
                             items.push_back(GhostSrc{f, cell, src[cell].first, src[cell].second});
                         }
+                // copies, then prolongations, then local fills (each in cell order): warps
+                // take one branch of the kernel and their stores stay coalesced
+                auto kind = [](const GhostSrc& g) { return g.src_block < 0 ? 2 : (g.src_cell < 0 ? 1 : 0); };
+                std::stable_sort(items.begin() + first, items.end(),
+                                 [&](const GhostSrc& a, const GhostSrc& b) { return kind(a) < kind(b); });
                 X[L].src_range.push_back({first, (long long)items.size() - first});
             }
             CK(upload_vec(items, &X[L].d_src, c->stream), "upload ghost sources");

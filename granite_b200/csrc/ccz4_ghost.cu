@@ -192,6 +192,7 @@ __device__ void prolong_cell(const DevBlock& F, const DevBlock& C, int i, int j,
     const long long o110 = cell_index(C, c1[0], c1[1], c0[2]), o101 = cell_index(C, c1[0], c0[1], c1[2]);
     const long long o011 = cell_index(C, c0[0], c1[1], c1[2]), o111 = cell_index(C, c1[0], c1[1], c1[2]);
     const long long fc = cell_index(F, i, j, k);
+#pragma unroll 4
     for (int v = 0; v < NV; ++v) {
         const double* q = cb + (long long)v * C.stride;
         double val = __dmul_rn(w000, __ldg(q + o000));
@@ -241,7 +242,9 @@ __global__ void xfer_kernel(int kind, const DevBlock* __restrict__ blocks, const
     }
 }
 
-// One thread per listed ghost cell; each cell is written exactly once.
+// One thread per listed ghost cell; each cell is written exactly once. The
+// cells a launch reads (interior cells of this level, coarse slot 0) are never
+// written by it, so every value of a cell is loaded before any is stored.
 __global__ void ghost_sources_kernel(const DevBlock* __restrict__ blocks, const GhostSrc* __restrict__ items,
                                      long long n, int sel, int local_mode) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -249,31 +252,42 @@ __global__ void ghost_sources_kernel(const DevBlock* __restrict__ blocks, const 
     const GhostSrc it = items[t];
     const DevBlock& D = blocks[it.dst_block];
     double* db = D.buf[sel];
+    const long long dst = it.dst_cell, dstr = D.stride;
     const int i = it.dst_cell % D.tx, j = (it.dst_cell / D.tx) % D.ty, k = it.dst_cell / (D.tx * D.ty);
-    if (it.src_block >= 0 && it.src_cell >= 0) {  // same-level neighbour
-        const DevBlock& S = blocks[it.src_block];
-        const double* sb = S.buf[sel];
-        for (int v = 0; v < NV; ++v) db[(long long)v * D.stride + it.dst_cell] = __ldg(sb + (long long)v * S.stride + it.src_cell);
-        return;
-    }
-    if (it.src_block >= 0) {  // coarse level
+    if (it.src_block >= 0 && it.src_cell < 0) {  // coarse level
         const DevBlock& C = blocks[it.src_block];
         prolong_cell(D, C, i, j, k, db, C.buf[0]);
         return;
     }
-    if (local_mode == GHOST_SOMMERFELD) {
+    const double* src;
+    long long sstr;
+    if (it.src_block >= 0) {  // same-level neighbour
+        const DevBlock& S = blocks[it.src_block];
+        src = S.buf[sel] + it.src_cell;
+        sstr = S.stride;
+    } else if (local_mode == GHOST_SOMMERFELD) {
         const FalloffChain ch = falloff_chain(D, i, j, k);
+        double v_[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) v_[v] = __ldg(db + v * dstr + ch.src);
+#pragma unroll
         for (int v = 0; v < NV; ++v) {
             const double fi = f_inf(v);
-            double val = db[(long long)v * D.stride + ch.src];
+            double val = v_[v];
             for (int p = 0; p < ch.npass; ++p) val = falloff(fi, val, ch.ri[p], ch.rg[p]);
-            db[(long long)v * D.stride + it.dst_cell] = val;
+            db[v * dstr + dst] = val;
         }
         return;
+    } else {  // zero gradient
+        src = db + cell_index(D, clampi(i, NG, NG + D.n[0] - 1), clampi(j, NG, NG + D.n[1] - 1),
+                              clampi(k, NG, NG + D.n[2] - 1));
+        sstr = dstr;
     }
-    const long long s = cell_index(D, clampi(i, NG, NG + D.n[0] - 1), clampi(j, NG, NG + D.n[1] - 1),
-                                   clampi(k, NG, NG + D.n[2] - 1));
-    for (int v = 0; v < NV; ++v) db[(long long)v * D.stride + it.dst_cell] = db[(long long)v * D.stride + s];
+    double v_[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) v_[v] = __ldg(src + v * sstr);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) db[v * dstr + dst] = v_[v];
 }
 
 }  // namespace
