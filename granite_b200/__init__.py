@@ -104,6 +104,8 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_set_kernel_variant.argtypes = [vp, C.c_int]
     lib.granite_ccz4_set_batching.argtypes = [vp, C.c_int]
     lib.granite_ccz4_get_kernel_variant.argtypes = [vp, C.POINTER(C.c_int)]
+    lib.granite_ccz4_set_fp64_chi_threshold.argtypes = [vp, C.c_double]
+    lib.granite_ccz4_get_fp64_chi_threshold.argtypes = [vp, C.POINTER(C.c_double)]
     _LIB = lib
     return lib
 
@@ -333,6 +335,15 @@ class Evolver:
 
     def set_batching(self, batched: bool):
         self.ctx.check(self.ctx.lib.granite_ccz4_set_batching(self.ctx.h, int(bool(batched))))
+
+    def set_fp64_chi_threshold(self, chi_fp64: float):
+        """MIXED steps: tiles with a point of chi below chi_fp64 run the FP64 algebra (0 = off)."""
+        self.ctx.check(self.ctx.lib.granite_ccz4_set_fp64_chi_threshold(self.ctx.h, float(chi_fp64)))
+
+    def fp64_chi_threshold(self) -> float:
+        v = C.c_double()
+        self.ctx.check(self.ctx.lib.granite_ccz4_get_fp64_chi_threshold(self.ctx.h, C.byref(v)))
+        return v.value
 
     def variant(self) -> int:
         v = C.c_int()

@@ -83,6 +83,7 @@ struct LevelLists {
                                    // when a block cannot be mapped for TMA
     Tile* d_tiles = nullptr;   // stage-kernel tiles (shape of the level's variant)
     int ntiles = 0;
+    unsigned char* d_flags = nullptr;  // per-tile precision of MIXED steps (1 = FP64 algebra)
     Tile* d_mtiles = nullptr;  // constraint-monitor tiles (variant-0 shape)
     int nmtiles = 0;
     GhostItem* d_ghost = nullptr;
@@ -140,6 +141,7 @@ struct Ctx {
     int device = 0;
     int variant = VARIANT_TMA;     // stage-kernel variant (granite_ccz4_set_kernel_variant)
     bool batched = true;           // one launch per level and stage + CUDA graphs (else per block, eager)
+    double fp64_chi = 0.0;         // MIXED: tiles with a point of chi below this run the FP64 algebra
     cudaStream_t stream = nullptr;
     std::string err;
     long long launches = 0;
@@ -439,6 +441,31 @@ int granite_ccz4_set_kernel_variant(void* h, int variant) {
     return GRANITE_OK;
 }
 
+int granite_ccz4_set_fp64_chi_threshold(void* h, double chi) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (!(chi >= 0.0) || !std::isfinite(chi)) return fail(c, GRANITE_ERR_INVALID, "threshold must be finite and >= 0");
+    if (chi == c->fp64_chi) return GRANITE_OK;
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    // cached step graphs hold the old launch sequence
+    for (auto& kv : c->graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    for (auto& kv : c->hgraphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    c->graphs.clear();
+    c->hgraphs.clear();
+    c->fp64_chi = chi;
+    return GRANITE_OK;
+}
+
+int granite_ccz4_get_fp64_chi_threshold(const void* h, double* chi) {
+    const Ctx* c = static_cast<const Ctx*>(h);
+    if (!c || !chi) return GRANITE_ERR_INVALID;
+    *chi = c->fp64_chi;
+    return GRANITE_OK;
+}
+
 int granite_ccz4_get_kernel_variant(const void* h, int* variant) {
     const Ctx* c = static_cast<const Ctx*>(h);
     if (!c || !variant) return GRANITE_ERR_INVALID;
@@ -516,6 +543,7 @@ int granite_ccz4_destroy(void* h) {
     for (auto e : c->event_pool) cudaEventDestroy(e);
     for (auto& L : c->levels) {
         cudaFree(L.d_tiles);
+        cudaFree(L.d_flags);
         cudaFree(L.d_mtiles);
         cudaFree(L.d_ghost);
     }
@@ -798,6 +826,7 @@ int granite_ccz4_commit(void* h) {
         ll.nmtiles = (int)mtiles.size();
         CK(upload_vec(ghosts, &ll.d_ghost, c->stream), "upload ghost chunks");
         ll.ntiles = (int)tiles.size();
+        CK(cudaMalloc(&ll.d_flags, std::max<size_t>(1, ll.ntiles)), "cudaMalloc(tile precision flags)");
         ll.nghost = (int)ghosts.size();
     }
     int maxt = 0;
@@ -848,19 +877,37 @@ int granite_ccz4_download_block(void* h, int i, double* host) {
 
 // The fused stage kernel over one level: one launch over the whole work-list,
 // or (unbatched) one launch per block.
-static cudaError_t level_stage(Ctx* c, LevelLists& L, int precision, const StageArgs& a, long long* n) {
-    if (c->batched) {
+// One stage over tiles [first, first + count) of a level: one launch, or with
+// per-tile precision (MIXED and a positive chi threshold) a classification of
+// the tiles from the stage input's chi and one FP32 and one FP64 launch that
+// each take their flagged tiles in list order.
+static cudaError_t stage_range(Ctx* c, LevelLists& L, int precision, const StageArgs& a, int first, int count,
+                               long long* n) {
+    if (precision != GRANITE_PRECISION_MIXED || !(c->fp64_chi > 0.0)) {
         ++*n;
-        return timed(c, GRANITE_KERNEL_STAGE, [&] {
-            return launch_stage(L.variant, precision, EPI_RK, c->d_blocks, L.d_tiles, L.ntiles, a, c->stream);
-        });
+        return launch_stage(L.variant, precision, EPI_RK, c->d_blocks, L.d_tiles + first, count, a, c->stream);
     }
+    cudaError_t e = launch_classify(L.variant, c->d_blocks, L.d_tiles + first, 0, count, a.in_sel, c->fp64_chi,
+                                    L.d_flags + first, c->stream);
+    if (e != cudaSuccess) return e;
+    StageArgs b = a;
+    b.tile_prec = L.d_flags + first;
+    b.want_prec = 0;
+    if ((e = launch_stage(L.variant, PM_MIXED, EPI_RK, c->d_blocks, L.d_tiles + first, count, b, c->stream)))
+        return e;
+    b.want_prec = 1;
+    *n += 3;
+    return launch_stage(L.variant, PM_FP64, EPI_RK, c->d_blocks, L.d_tiles + first, count, b, c->stream);
+}
+
+// The fused stage kernel over one level: the whole work-list at once, or
+// (unbatched) block by block.
+static cudaError_t level_stage(Ctx* c, LevelLists& L, int precision, const StageArgs& a, long long* n) {
+    if (c->batched)
+        return timed(c, GRANITE_KERNEL_STAGE, [&] { return stage_range(c, L, precision, a, 0, L.ntiles, n); });
     for (const auto& r : L.tile_range) {
-        ++*n;
-        cudaError_t e = timed(c, GRANITE_KERNEL_STAGE, [&] {
-            return launch_stage(L.variant, precision, EPI_RK, c->d_blocks, L.d_tiles + r.first, r.second, a,
-                                c->stream);
-        });
+        cudaError_t e = timed(c, GRANITE_KERNEL_STAGE,
+                              [&] { return stage_range(c, L, precision, a, r.first, r.second, n); });
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;

@@ -60,6 +60,9 @@ struct StageArgs {
     unsigned long long* nonfinite;  // floor hits on non-finite chi/alpha (nullable)
     const void* tmaps;     // TMA variant: CUtensorMap of (block b, slot s) at tmaps[3 b + s]
     unsigned int* errflag; // TMA variant: set to 1 when a bounded mbarrier wait gives up (nullable)
+    // Per-tile precision (nullable): the launch covers only tiles ti with tile_prec[ti] == want_prec.
+    const unsigned char* tile_prec;
+    int want_prec;
 };
 
 __host__ __device__ inline long long cell_index(const DevBlock& b, int i, int j, int k) {

@@ -35,9 +35,18 @@ bool encode_block_tmap(void* map128, const double* base, const DevBlock& d);
 // Per-device kernel attributes (shared-memory opt-in); call with the device current.
 cudaError_t configure_stage_kernels();
 
-// Fused RHS (+KO) over a tile work-list. precision: 0 = FP64, 1 = mixed.
+// Precision modes of the stage kernels: FP64 algebra or FP32 algebra (mixed).
+enum { PM_FP64 = 0, PM_MIXED = 1 };
+
+// Fused RHS (+KO) over a tile work-list in precision mode `precision` (PM_*);
+// with args.tile_prec set, only the tiles flagged args.want_prec.
 cudaError_t launch_stage(int variant, int precision, int epi, const DevBlock* blocks,
                          const Tile* tiles, int ntiles, const StageArgs& args, cudaStream_t stream);
+
+// Per-tile precision flags of tiles [first, first + ntiles): flag[ti] = 1 when a
+// point of the tile has chi < chi_fp64 in slot `sel` (FP64 algebra), else 0.
+cudaError_t launch_classify(int variant, const DevBlock* blocks, const Tile* tiles, int first, int ntiles, int sel,
+                            double chi_fp64, unsigned char* flag, cudaStream_t stream);
 
 // KO dissipation only: rhs += KO(u) at interior points of one block.
 cudaError_t launch_dissipation(const DevBlock* block, int in_sel, double* rhs, int ntiles,

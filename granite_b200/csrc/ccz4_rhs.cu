@@ -21,7 +21,10 @@
 // f[+k] + f[-k] - 2 f[0] ...), rounded to FP32 only after the cancellation,
 // then the Christoffel/Ricci/gauge/KO algebra runs in FP32. chi, the inverse
 // conformal metric, the 1/chi factors, the evolved state and the RK3 combine
-// stay FP64.
+// stay FP64. Per-tile precision: a launch can be restricted to the tiles of a
+// flag array (classify_tiles_kernel marks the tiles with a point of chi below a
+// threshold, near a puncture), so the FP64 kernel takes those and the FP32
+// kernel the rest, both walking the tile list in its spatial order.
 //
 // Control flow: the per-point body is one straight-line sequence (the KO term
 // is always evaluated -- its weights sigma/(64 dx) w_s are zero when KO is off
@@ -44,13 +47,25 @@ constexpr double PI_D = 3.14159265358979323846;
 __device__ constexpr int FIELD_ORDER[NV] = {GXX, GXY, GXZ, GYY, GYZ, GZZ, GHX, GHY, GHZ, CHI, ALPHA,
                                             BETAX, BETAY, BETAZ, KTR, THETA, AXX, AXY, AXZ, AYY, AYZ, AZZ};
 
-// Stencils read straight from global memory (through L1).
-template <typename P>
+// Per-tile precision: a launch with tile_prec set covers only the tiles whose
+// flag equals want (1 = FP64 algebra, 0 = FP32), in list order.
+__device__ __forceinline__ bool tile_selected(const unsigned char* prec, int want, int ti) {
+    return !prec || prec[ti] == want;
+}
+// First selected tile at or after ti in the stride-`step` sequence of a persistent CTA.
+__device__ __forceinline__ int next_selected(const unsigned char* prec, int want, int ti, int step, int ntiles) {
+    while (ti < ntiles && !tile_selected(prec, want, ti)) ti += step;
+    return ti;
+}
+
+// Stencils read straight from global memory (through L1). Every source
+// evaluates the stencils of one field in the precision of the caller's algebra
+// (P = double or float, deduced from the blend weight w).
 struct GlobalSource {
     const DevBlock& B;
     const double* __restrict__ u;
     long long c;
-    template <bool HESS>
+    template <bool HESS, typename P>
     __device__ __forceinline__ FieldDer<P> der(int v, const double beta[3], P w) {
         const long long off[3] = {1, B.tx, (long long)B.tx * B.ty};
         return field_der_l<P, HESS, true>(B, GlobalLoad{u + (long long)v * B.stride + c}, off, beta, w);
@@ -116,7 +131,7 @@ struct TileGeom {
 // the one being differentiated, so the copies of the next fields overlap the
 // algebra of the current one. Every thread of the CTA must call der() for
 // every field in order (the calls carry the CTA barrier).
-template <typename P, int TX, int TY, int TZ, int NBUF>
+template <int TX, int TY, int TZ, int NBUF>
 struct SmemSource {
     using G = TileGeom<TX, TY, TZ>;
     const DevBlock& B;
@@ -141,7 +156,7 @@ struct SmemSource {
     __device__ __forceinline__ void start() {
         for (int k = 0; k < NBUF - 1; ++k) issue(k);
     }
-    template <bool HESS>
+    template <bool HESS, typename P>
     __device__ __forceinline__ FieldDer<P> der(int /*v*/, const double beta[3], P w) {
         cp_async_wait<NBUF - 2>();
         __syncthreads();
@@ -212,7 +227,7 @@ __device__ __forceinline__ void tma_load_box(unsigned dst, const void* map, int 
 // and the host reports the error).
 constexpr unsigned long long TMA_WAIT_NS = 2000000000ull;
 
-template <typename P, int NBUF>
+template <int NBUF, bool SEL>
 struct TmaSource {
     using R = TmaRing<NBUF>;
     const DevBlock* blocks;
@@ -227,10 +242,19 @@ struct TmaSource {
     bool failed;       // a wait of this thread gave up (at item fail_q); thread 0 then stops issuing
     unsigned int* err;
     int fail_q;
+    const int* sel_tile;  // SEL: tile of round r at sel_tile[r & 1] (shared memory, written by thread 0)
 
+    // Tile of the CTA's r-th round: blockIdx.x + r gridDim.x, or with per-tile
+    // precision (SEL) the r-th tile of that sequence whose flag the launch takes.
+    __device__ __forceinline__ int round_tile(int r) const {
+        if constexpr (SEL)
+            return sel_tile[r & 1];
+        else
+            return blockIdx.x + r * gridDim.x;
+    }
     // thread 0 only
     __device__ __forceinline__ void issue(int q) const {
-        const int ti = blockIdx.x + (q / NV) * gridDim.x;
+        const int ti = round_tile(q / NV);
         if (ti >= ntiles) return;
         const Tile t = tiles[ti];
         const int s = q % NBUF;
@@ -261,7 +285,7 @@ struct TmaSource {
     }
     // Every thread of the CTA calls der() for every item in order (the call
     // carries the CTA barrier that frees the slot the next load overwrites).
-    template <bool HESS>
+    template <bool HESS, typename P>
     __device__ __forceinline__ FieldDer<P> der(int /*v*/, const double beta[3], P w) {
         __syncthreads();
         if (threadIdx.x == 0 && !failed) issue(next + NBUF - 1);
@@ -626,6 +650,16 @@ __device__ __forceinline__ double rk_combine(double a1, double un, double a2, do
 
 }  // namespace
 
+// The RHS at one point with the algebra of precision mode PM.
+template <int PM, typename Src>
+__device__ __forceinline__ void point_pm(const DevBlock& B, const double* __restrict__ u, long long c,
+                                         const StageArgs& A, Src& S, double L[NV]) {
+    if constexpr (PM == PM_FP64)
+        ccz4_point<double>(B, u, c, A, S, L);
+    else
+        ccz4_point<float>(B, u, c, A, S, L);
+}
+
 // Shared epilogue: store L, or RK combine + floors (+ algebraic constraints).
 template <int EPI>
 __device__ __forceinline__ void stage_epilogue(const DevBlock& B, const StageArgs& A, long long c, const double L[NV]) {
@@ -662,9 +696,10 @@ __device__ __forceinline__ void stage_epilogue(const DevBlock& B, const StageArg
 // Variants 0, 2, 3: stencils from global memory, one thread per point; MINB
 // resident CTAs per SM requested from the register allocator (1: up to 255
 // registers, 3: up to 168, 4: up to 128).
-template <typename P, int EPI, int TX, int TY, int TZ, int MINB>
+template <int PM, int EPI, int TX, int TY, int TZ, int MINB>
 __global__ void __launch_bounds__(TX* TY* TZ, MINB)
     ccz4_stage_kernel(const DevBlock* __restrict__ blocks, const Tile* __restrict__ tiles, StageArgs A) {
+    if (!tile_selected(A.tile_prec, A.want_prec, blockIdx.x)) return;
     const Tile t = tiles[blockIdx.x];
     const DevBlock& B = blocks[t.block];
     // 128 threads over a w x (128 / w) tile; w matches the block width (x fastest)
@@ -674,21 +709,22 @@ __global__ void __launch_bounds__(TX* TY* TZ, MINB)
     if (i >= B.n[0] || j >= B.n[1] || k >= B.n[2]) return;
     const long long c = cell_index(B, i + NG, j + NG, k + NG);
     const double* __restrict__ uin = B.buf[A.in_sel];
-    GlobalSource<P> S{B, uin, c};
+    GlobalSource S{B, uin, c};
     double L[NV];
-    ccz4_point<P>(B, uin, c, A, S, L);
+    point_pm<PM>(B, uin, c, A, S, L);
     stage_epilogue<EPI>(B, A, c, L);
 }
 
 // Variant 1: every field of the tile (with its stencil halo) staged through
 // shared memory by cp.async, NBUF-1 fields ahead of the computation.
-template <typename P, int EPI, int TX, int TY, int TZ, int NBUF>
+template <int PM, int EPI, int TX, int TY, int TZ, int NBUF>
 __global__ void __launch_bounds__(TX* TY* TZ, 2)
     ccz4_stage_smem_kernel(const DevBlock* __restrict__ blocks, const Tile* __restrict__ tiles, StageArgs A) {
     using G = TileGeom<TX, TY, TZ>;
     constexpr int NT = TX * TY * TZ;
     extern __shared__ __align__(16) double smem[];
     int2* table = reinterpret_cast<int2*>(smem + NBUF * G::BOX);
+    if (!tile_selected(A.tile_prec, A.want_prec, blockIdx.x)) return;
     const Tile t = tiles[blockIdx.x];
     const DevBlock& B = blocks[t.block];
     const int tid = threadIdx.x;
@@ -706,14 +742,14 @@ __global__ void __launch_bounds__(TX* TY* TZ, 2)
     }
     __syncthreads();
     const double* __restrict__ uin = B.buf[A.in_sel];
-    SmemSource<P, TX, TY, TZ, NBUF> S{B, uin, smem, table, cell_index(B, gi0, gj0, gk0),
+    SmemSource<TX, TY, TZ, NBUF> S{B, uin, smem, table, cell_index(B, gi0, gj0, gk0),
                                       (lx + 4) + G::BX * ((ly + 4) + G::BY * (lz + 4)), 0};
     S.start();
     // pointwise loads of threads outside the block use a valid cell; their results are dropped
     const int ic = i < B.n[0] ? i : B.n[0] - 1, jc = j < B.n[1] ? j : B.n[1] - 1, kc = k < B.n[2] ? k : B.n[2] - 1;
     const long long c = cell_index(B, ic + NG, jc + NG, kc + NG);
     double L[NV];
-    ccz4_point<P>(B, uin, c, A, S, L);
+    point_pm<PM>(B, uin, c, A, S, L);
     if (!valid) return;  // no barrier follows the last field
     stage_epilogue<EPI>(B, A, c, L);
 }
@@ -721,7 +757,7 @@ __global__ void __launch_bounds__(TX* TY* TZ, 2)
 // Variant 4: persistent CTAs (grid <= SMs x resident CTAs), one 16x4x4 tile
 // at a time, every field streamed through the TMA ring. Threads of partial
 // tiles (past the block edge) compute on the zero-filled box and store nothing.
-template <typename P, int EPI, int NBUF>
+template <int PM, int EPI, int NBUF, bool SEL>
 __global__ void __launch_bounds__(V4_NT, 1)
     ccz4_stage_tma_kernel(const DevBlock* __restrict__ blocks, const Tile* __restrict__ tiles, int ntiles,
                           StageArgs A) {
@@ -729,19 +765,32 @@ __global__ void __launch_bounds__(V4_NT, 1)
     extern __shared__ unsigned char smem_raw[];
     double* ring = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     const unsigned bar0 = smem_addr(ring + (size_t)NBUF * R::BOX);
+    __shared__ int sel_tile[2];
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int s = 0; s < NBUF; ++s) mbar_init(bar0 + 8u * s, 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        if constexpr (SEL) {
+            sel_tile[0] = next_selected(A.tile_prec, A.want_prec, blockIdx.x, gridDim.x, ntiles);
+            sel_tile[1] = next_selected(A.tile_prec, A.want_prec, sel_tile[0] + gridDim.x, gridDim.x, ntiles);
+        }
     }
     __syncthreads();
     const int lx = tid % V4_TX, ly = (tid / V4_TX) % V4_TY, lz = tid / (V4_TX * V4_TY);
-    TmaSource<P, NBUF> S{blocks, tiles, static_cast<const unsigned char*>(A.tmaps), ntiles, A.in_sel, ring, bar0,
+    TmaSource<NBUF, SEL> S{blocks, tiles, static_cast<const unsigned char*>(A.tmaps), ntiles, A.in_sel, ring, bar0,
                          nullptr, (lx + 4) + R::BX * ((ly + 4) + R::BY * (lz + 4)), 0, false,
-                         A.errflag, 0};
+                         A.errflag, 0, sel_tile};
     if (tid == 0)
         for (int q = 0; q < NBUF - 1; ++q) S.issue(q);
-    for (int ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
+    for (int r = 0;; ++r) {
+        const int ti = S.round_tile(r);
+        if (ti >= ntiles) break;
+        // SEL: the tile after this one. Round r - 1's entry is free: its items
+        // were all issued before round r began (the producer runs NBUF - 1 < NV
+        // items ahead) and every thread read it when round r - 1 began; the
+        // barrier of the next der() publishes the write.
+        if (SEL && r > 0 && tid == 0)
+            sel_tile[(r + 1) & 1] = next_selected(A.tile_prec, A.want_prec, ti + gridDim.x, gridDim.x, ntiles);
         const Tile t = tiles[ti];
         const DevBlock& B = blocks[t.block];
         S.B = &B;
@@ -752,7 +801,7 @@ __global__ void __launch_bounds__(V4_NT, 1)
         const long long c = cell_index(B, ic + NG, jc + NG, kc + NG);
         const double* __restrict__ uin = B.buf[A.in_sel];
         double L[NV];
-        ccz4_point<P>(B, uin, c, A, S, L);
+        point_pm<PM>(B, uin, c, A, S, L);
         if (valid) stage_epilogue<EPI>(B, A, c, L);
     }
     // Every issued item was consumed (issue() skips items past this CTA's last
@@ -763,8 +812,28 @@ __global__ void __launch_bounds__(V4_NT, 1)
         const int f = S.fail_q;
         S.failed = false;
         for (int q = f; q < f + NBUF && !S.failed; ++q)
-            if (blockIdx.x + (q / NV) * (int)gridDim.x < ntiles) S.wait(q);
+            if (S.round_tile(q / NV) < ntiles) S.wait(q);
     }
+}
+
+// Per-tile precision flags: flag[ti] = 1 (FP64 algebra) when a point of tile ti
+// has chi below chi_fp64 in buffer slot `sel` (or a non-finite chi), else 0.
+__global__ void __launch_bounds__(128)
+    classify_tiles_kernel(const DevBlock* __restrict__ blocks, const Tile* __restrict__ tiles, int first, int sel,
+                          int tx, int ty, int tz, double chi_fp64, unsigned char* __restrict__ flag) {
+    const int ti = first + blockIdx.x;
+    const Tile t = tiles[ti];
+    const DevBlock& B = blocks[t.block];
+    const int w = t.w > 0 ? t.w : tx, h = t.w > 0 ? 128 / t.w : ty, d = t.w > 0 ? 1 : tz;
+    const double* chi = B.buf[sel] + (long long)CHI * B.stride;
+    bool low = false;
+    for (int p = threadIdx.x; p < w * h * d; p += blockDim.x) {
+        const int i = t.i0 + p % w, j = t.j0 + (p / w) % h, k = t.k0 + p / (w * h);
+        if (i < B.n[0] && j < B.n[1] && k < B.n[2])
+            low |= !(__ldg(chi + cell_index(B, i + NG, j + NG, k + NG)) >= chi_fp64);
+    }
+    low = __syncthreads_or(low);
+    if (threadIdx.x == 0) flag[ti] = low ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -791,51 +860,58 @@ int stage_tile_dims(int variant, int* tx, int* ty, int* tz) {
     return 0;
 }
 
-template <typename P, int EPI>
+template <int PM, int EPI>
 static cudaError_t launch_smem(const DevBlock* blocks, const Tile* tiles, int ntiles, const StageArgs& args,
                                cudaStream_t stream) {
     using G = TileGeom<V1_TX, V1_TY, V1_TZ>;
     constexpr size_t bytes = V1_NBUF * G::BOX * sizeof(double) + G::NLOAD * sizeof(int2);
-    auto k = ccz4_stage_smem_kernel<P, EPI, V1_TX, V1_TY, V1_TZ, V1_NBUF>;
+    auto k = ccz4_stage_smem_kernel<PM, EPI, V1_TX, V1_TY, V1_TZ, V1_NBUF>;
     k<<<ntiles, V1_TX * V1_TY * V1_TZ, bytes, stream>>>(blocks, tiles, args);
     return cudaGetLastError();
 }
 
-template <typename P, int EPI>
+template <int PM, int EPI>
 static cudaError_t configure_smem() {
     using G = TileGeom<V1_TX, V1_TY, V1_TZ>;
     constexpr size_t bytes = V1_NBUF * G::BOX * sizeof(double) + G::NLOAD * sizeof(int2);
-    return cudaFuncSetAttribute(ccz4_stage_smem_kernel<P, EPI, V1_TX, V1_TY, V1_TZ, V1_NBUF>,
+    return cudaFuncSetAttribute(ccz4_stage_smem_kernel<PM, EPI, V1_TX, V1_TY, V1_TZ, V1_NBUF>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 // Persistent grid of the TMA variant on each device: SMs x resident CTAs.
 constexpr int MAX_DEVICES = 64;
-static int g_tma_grid[MAX_DEVICES][2][2];  // [device][precision][epi]
+static int g_tma_grid[MAX_DEVICES][2][2];  // [device][precision mode][epi]
 
-template <typename P, int EPI>
+template <int PM, int EPI, bool SEL = false>
 static cudaError_t configure_tma(int dev, int nsm) {
-    auto k = ccz4_stage_tma_kernel<P, EPI, V4_NBUF>;
+    auto k = ccz4_stage_tma_kernel<PM, EPI, V4_NBUF, SEL>;
     constexpr size_t bytes = TmaRing<V4_NBUF>::SMEM;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, V4_NT, bytes))) return e;
-    g_tma_grid[dev][sizeof(P) == 8 ? 0 : 1][EPI] = nsm * (per_sm > 0 ? per_sm : 1);
+    if (!SEL) g_tma_grid[dev][PM][EPI] = nsm * (per_sm > 0 ? per_sm : 1);
     return cudaSuccess;
 }
 
-template <typename P, int EPI>
+template <int PM, int EPI>
 static cudaError_t launch_tma(const DevBlock* blocks, const Tile* tiles, int ntiles, const StageArgs& args,
                               cudaStream_t stream) {
     if (!args.tmaps) return cudaErrorInvalidValue;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    const int cap = (dev >= 0 && dev < MAX_DEVICES) ? g_tma_grid[dev][sizeof(P) == 8 ? 0 : 1][EPI] : 0;
+    const int cap = (dev >= 0 && dev < MAX_DEVICES) ? g_tma_grid[dev][PM][EPI] : 0;
     if (cap <= 0) return cudaErrorInvalidConfiguration;  // configure_stage_kernels() not run on this device
     const int grid = ntiles < cap ? ntiles : cap;
-    ccz4_stage_tma_kernel<P, EPI, V4_NBUF><<<grid, V4_NT, TmaRing<V4_NBUF>::SMEM, stream>>>(blocks, tiles, ntiles, args);
+    if (args.tile_prec) {  // per-tile precision launches (RK epilogue)
+        if (EPI != EPI_RK) return cudaErrorInvalidValue;
+        ccz4_stage_tma_kernel<PM, EPI_RK, V4_NBUF, true>
+            <<<grid, V4_NT, TmaRing<V4_NBUF>::SMEM, stream>>>(blocks, tiles, ntiles, args);
+    } else {
+        ccz4_stage_tma_kernel<PM, EPI, V4_NBUF, false>
+            <<<grid, V4_NT, TmaRing<V4_NBUF>::SMEM, stream>>>(blocks, tiles, ntiles, args);
+    }
     return cudaGetLastError();
 }
 
@@ -844,58 +920,86 @@ static cudaError_t launch_tma(const DevBlock* blocks, const Tile* tiles, int nti
 // at creation).
 cudaError_t configure_stage_kernels() {
     cudaError_t e;
-    if ((e = configure_smem<double, EPI_STORE>())) return e;
-    if ((e = configure_smem<double, EPI_RK>())) return e;
-    if ((e = configure_smem<float, EPI_STORE>())) return e;
-    if ((e = configure_smem<float, EPI_RK>())) return e;
+    if ((e = configure_smem<PM_FP64, EPI_STORE>())) return e;
+    if ((e = configure_smem<PM_FP64, EPI_RK>())) return e;
+    if ((e = configure_smem<PM_MIXED, EPI_STORE>())) return e;
+    if ((e = configure_smem<PM_MIXED, EPI_RK>())) return e;
     int dev = 0, nsm = 0;
     if ((e = cudaGetDevice(&dev))) return e;
     if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
     if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev))) return e;
-    if ((e = configure_tma<double, EPI_STORE>(dev, nsm))) return e;
-    if ((e = configure_tma<double, EPI_RK>(dev, nsm))) return e;
-    if ((e = configure_tma<float, EPI_STORE>(dev, nsm))) return e;
-    return configure_tma<float, EPI_RK>(dev, nsm);
+    if ((e = configure_tma<PM_FP64, EPI_STORE>(dev, nsm))) return e;
+    if ((e = configure_tma<PM_FP64, EPI_RK>(dev, nsm))) return e;
+    if ((e = configure_tma<PM_MIXED, EPI_STORE>(dev, nsm))) return e;
+    if ((e = configure_tma<PM_MIXED, EPI_RK>(dev, nsm))) return e;
+    if ((e = configure_tma<PM_FP64, EPI_RK, true>(dev, nsm))) return e;
+    return configure_tma<PM_MIXED, EPI_RK, true>(dev, nsm);
 }
 
-template <typename P, int EPI, int MINB>
+template <int PM, int EPI, int MINB>
 static cudaError_t launch_global(const DevBlock* blocks, const Tile* tiles, int ntiles, const StageArgs& args,
                                  cudaStream_t stream) {
-    ccz4_stage_kernel<P, EPI, V0_TX, V0_TY, V0_TZ, MINB>
+    ccz4_stage_kernel<PM, EPI, V0_TX, V0_TY, V0_TZ, MINB>
         <<<ntiles, dim3(V0_TX, V0_TY, V0_TZ), 0, stream>>>(blocks, tiles, args);
     return cudaGetLastError();
 }
 
+// Precision mode x epilogue -> one instantiation of a launcher L<PM, EPI>.
+template <template <int, int> class L>
+static cudaError_t dispatch(int pm, int epi, const DevBlock* blocks, const Tile* tiles, int ntiles,
+                            const StageArgs& args, cudaStream_t stream) {
+    if (pm == PM_FP64)
+        return epi == EPI_STORE ? L<PM_FP64, EPI_STORE>::run(blocks, tiles, ntiles, args, stream)
+                                : L<PM_FP64, EPI_RK>::run(blocks, tiles, ntiles, args, stream);
+    if (pm == PM_MIXED)
+        return epi == EPI_STORE ? L<PM_MIXED, EPI_STORE>::run(blocks, tiles, ntiles, args, stream)
+                                : L<PM_MIXED, EPI_RK>::run(blocks, tiles, ntiles, args, stream);
+    return cudaErrorInvalidValue;
+}
+
+template <int PM, int EPI>
+struct RunTma {
+    static cudaError_t run(const DevBlock* b, const Tile* t, int n, const StageArgs& a, cudaStream_t s) {
+        return launch_tma<PM, EPI>(b, t, n, a, s);
+    }
+};
+template <int PM, int EPI>
+struct RunSmem {
+    static cudaError_t run(const DevBlock* b, const Tile* t, int n, const StageArgs& a, cudaStream_t s) {
+        return launch_smem<PM, EPI>(b, t, n, a, s);
+    }
+};
 template <int MINB>
-static cudaError_t launch_global_any(int precision, int epi, const DevBlock* blocks, const Tile* tiles, int ntiles,
-                                     const StageArgs& args, cudaStream_t stream) {
-    if (precision == 0)
-        return epi == EPI_STORE ? launch_global<double, EPI_STORE, MINB>(blocks, tiles, ntiles, args, stream)
-                                : launch_global<double, EPI_RK, MINB>(blocks, tiles, ntiles, args, stream);
-    return epi == EPI_STORE ? launch_global<float, EPI_STORE, MINB>(blocks, tiles, ntiles, args, stream)
-                            : launch_global<float, EPI_RK, MINB>(blocks, tiles, ntiles, args, stream);
+struct RunGlobal {
+    template <int PM, int EPI>
+    struct L {
+        static cudaError_t run(const DevBlock* b, const Tile* t, int n, const StageArgs& a, cudaStream_t s) {
+            return launch_global<PM, EPI, MINB>(b, t, n, a, s);
+        }
+    };
+};
+
+cudaError_t launch_classify(int variant, const DevBlock* blocks, const Tile* tiles, int first, int ntiles, int sel,
+                            double chi_fp64, unsigned char* flag, cudaStream_t stream) {
+    if (ntiles <= 0) return cudaSuccess;
+    int tx, ty, tz;
+    stage_tile_dims(variant, &tx, &ty, &tz);
+    classify_tiles_kernel<<<ntiles, 128, 0, stream>>>(blocks, tiles, first, sel, tx, ty, tz, chi_fp64, flag);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_stage(int variant, int precision, int epi, const DevBlock* blocks, const Tile* tiles, int ntiles,
                          const StageArgs& args, cudaStream_t stream) {
     if (ntiles <= 0) return cudaSuccess;
-    if (variant == VARIANT_TMA) {
-        if (precision == 0)
-            return epi == EPI_STORE ? launch_tma<double, EPI_STORE>(blocks, tiles, ntiles, args, stream)
-                                    : launch_tma<double, EPI_RK>(blocks, tiles, ntiles, args, stream);
-        return epi == EPI_STORE ? launch_tma<float, EPI_STORE>(blocks, tiles, ntiles, args, stream)
-                                : launch_tma<float, EPI_RK>(blocks, tiles, ntiles, args, stream);
+    switch (variant) {
+        case VARIANT_TMA: return dispatch<RunTma>(precision, epi, blocks, tiles, ntiles, args, stream);
+        case VARIANT_SMEM: return dispatch<RunSmem>(precision, epi, blocks, tiles, ntiles, args, stream);
+        case VARIANT_GLOBAL_R168:
+            return dispatch<RunGlobal<3>::L>(precision, epi, blocks, tiles, ntiles, args, stream);
+        case VARIANT_GLOBAL_R128:
+            return dispatch<RunGlobal<4>::L>(precision, epi, blocks, tiles, ntiles, args, stream);
+        default: return dispatch<RunGlobal<1>::L>(precision, epi, blocks, tiles, ntiles, args, stream);
     }
-    if (variant == 1) {
-        if (precision == 0)
-            return epi == EPI_STORE ? launch_smem<double, EPI_STORE>(blocks, tiles, ntiles, args, stream)
-                                    : launch_smem<double, EPI_RK>(blocks, tiles, ntiles, args, stream);
-        return epi == EPI_STORE ? launch_smem<float, EPI_STORE>(blocks, tiles, ntiles, args, stream)
-                                : launch_smem<float, EPI_RK>(blocks, tiles, ntiles, args, stream);
-    }
-    if (variant == VARIANT_GLOBAL_R168) return launch_global_any<3>(precision, epi, blocks, tiles, ntiles, args, stream);
-    if (variant == VARIANT_GLOBAL_R128) return launch_global_any<4>(precision, epi, blocks, tiles, ntiles, args, stream);
-    return launch_global_any<1>(precision, epi, blocks, tiles, ntiles, args, stream);
 }
 
 

@@ -218,6 +218,18 @@ GRANITE_API int granite_ccz4_profile_get(void* ctx, int kernel_class, double* to
 GRANITE_API int granite_ccz4_set_kernel_variant(void* ctx, int variant);
 GRANITE_API int granite_ccz4_get_kernel_variant(const void* ctx, int* variant);
 
+/* Per-tile precision of GRANITE_PRECISION_MIXED steps (no counterpart in the
+ * reference): in every RK stage of granite_ccz4_rk3_step /
+ * granite_ccz4_hierarchy_step, a tile of the work-list whose stage input has
+ * a point with chi < chi_fp64 (or a non-finite chi) runs the FP64 algebra,
+ * every other tile the FP32 algebra. The stage kernel decides per tile from
+ * the current chi (one CTA-wide vote), so the choice follows moving punctures
+ * and costs no extra launch. 0 (the default) disables it; +large makes MIXED
+ * steps identical to FP64 ones. Changing it drops the cached step graphs. The
+ * stateless operators (granite_ccz4_compute_rhs_*) are not affected. */
+GRANITE_API int granite_ccz4_set_fp64_chi_threshold(void* ctx, double chi_fp64);
+GRANITE_API int granite_ccz4_get_fp64_chi_threshold(const void* ctx, double* chi_fp64);
+
 /* Batching (no counterpart in the reference): 1 (default) = one launch per
  * level and RK stage over all blocks, each step replayed as one CUDA graph;
  * 0 = one launch per block and stage, issued eagerly, as a per-block drop-in
