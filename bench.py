@@ -347,8 +347,9 @@ def main():
                          "or staged in shared memory")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison run")
-    ap.add_argument("--fp64-chi", type=float, default=0.0,
-                    help="mixed precision: tiles with a point of chi below this run the FP64 algebra (0 = off)")
+    ap.add_argument("--fp64-chi", type=float, default=0.5,
+                    help="mixed precision: tiles with a point of chi below this run the FP64 algebra "
+                         "(0 = FP32 algebra everywhere)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -402,6 +403,16 @@ def main():
     ms, launches = timed_steps(torch, dist, world, local, run, args.steps)
     clocks = sampler.stop()
     value = run.points_per_step * args.steps * world / (ms / 1000.0)
+    fp32_line = None
+    if prec == gb.PRECISION_MIXED and args.fp64_chi > 0.0:
+        # the same mixed steps with the FP32 algebra on every tile (no FP64 pass)
+        run.ev.set_fp64_chi_threshold(0.0)
+        for _ in range(2):
+            run.step()
+        fms, _ = timed_steps(torch, dist, world, local, run, args.steps)
+        run.ev.set_fp64_chi_threshold(args.fp64_chi)
+        fp32_line = {"value": run.points_per_step * args.steps * world / (fms / 1000.0),
+                     "ms_per_step": fms / args.steps}
     cmp_line = None
     if compare is not None:
         cms, _ = timed_steps(torch, dist, world, local, compare, args.steps)
@@ -473,6 +484,8 @@ def main():
                 "cpu_baseline": cb, "clocks": clocks, "gpu_launches": launches}
         if cmp_line:
             line["fp64_plain"] = cmp_line
+        if fp32_line:
+            line["fp32_algebra_all_tiles"] = fp32_line
         if acc:
             line["accuracy_mixed_vs_fp64"] = acc
         print(json.dumps(line))

@@ -23,8 +23,8 @@
 // conformal metric, the 1/chi factors, the evolved state and the RK3 combine
 // stay FP64. Per-tile precision: a launch can be restricted to the tiles of a
 // flag array (classify_tiles_kernel marks the tiles with a point of chi below a
-// threshold, near a puncture), so the FP64 kernel takes those and the FP32
-// kernel the rest, both walking the tile list in its spatial order.
+// threshold, near a puncture), so an FP64 pass recomputes those tiles after
+// (or beside) the FP32 pass, walking the tile list in its spatial order.
 //
 // Control flow: the per-point body is one straight-line sequence (the KO term
 // is always evaluated -- its weights sigma/(64 dx) w_s are zero when KO is off
@@ -904,7 +904,7 @@ static cudaError_t launch_tma(const DevBlock* blocks, const Tile* tiles, int nti
     const int cap = (dev >= 0 && dev < MAX_DEVICES) ? g_tma_grid[dev][PM][EPI] : 0;
     if (cap <= 0) return cudaErrorInvalidConfiguration;  // configure_stage_kernels() not run on this device
     const int grid = ntiles < cap ? ntiles : cap;
-    if (args.tile_prec) {  // per-tile precision launches (RK epilogue)
+    if (args.tile_prec) {  // per-tile precision passes (RK epilogue)
         if (EPI != EPI_RK) return cudaErrorInvalidValue;
         ccz4_stage_tma_kernel<PM, EPI_RK, V4_NBUF, true>
             <<<grid, V4_NT, TmaRing<V4_NBUF>::SMEM, stream>>>(blocks, tiles, ntiles, args);
