@@ -891,7 +891,9 @@ int granite_ccz4_download_block(void* h, int i, double* host) {
 static cudaError_t stage_range(Ctx* c, LevelLists& L, int precision, const StageArgs& a, int first, int count,
                                long long* n) {
     const Tile* tiles = L.d_tiles + first;
-    const bool split = precision == GRANITE_PRECISION_MIXED && c->fp64_chi > 0.0;
+    // (the TMA kernel keeps a CTA's selected tiles in shared memory: bounded count)
+    const bool split = precision == GRANITE_PRECISION_MIXED && c->fp64_chi > 0.0 &&
+        (L.variant != VARIANT_TMA || (long long)count <= (long long)tma_grid() * TMA_SEL_CAP);
     if (!split) {
         ++*n;
         return launch_stage(L.variant, precision, EPI_RK, c->d_blocks, tiles, count, a, c->stream);
@@ -914,7 +916,7 @@ static cudaError_t stage_range(Ctx* c, LevelLists& L, int precision, const Stage
     }
     b.want_prec = 1;
     *n += 3;
-    return launch_stage(L.variant, PM_FP64, EPI_RK, c->d_blocks, tiles, count, b, c->stream);
+    return launch_stage(L.variant, PM_FP64F, EPI_RK, c->d_blocks, tiles, count, b, c->stream);
 }
 
 // The fused stage kernel over one level: the whole work-list at once, or

@@ -30,13 +30,21 @@ int stage_tile_dims(int variant, int* tx, int* ty, int* tz);
 // cannot be described (odd x extent, misaligned base, box larger than the
 // block); such blocks use the global-load kernel.
 constexpr int TMA_BOX[3] = {16 + 8, 4 + 8, 4 + 8};
+// Per-tile precision launches of the TMA kernel keep each CTA's selected tiles
+// in shared memory: at most TMA_SEL_CAP per CTA, i.e. ntiles <= grid x TMA_SEL_CAP.
+constexpr int TMA_SEL_CAP = 2048;
+// The persistent grid of the TMA kernel on the current device (0 before configure_stage_kernels).
+int tma_grid();
 bool encode_block_tmap(void* map128, const double* base, const DevBlock& d);
 
 // Per-device kernel attributes (shared-memory opt-in); call with the device current.
 cudaError_t configure_stage_kernels();
 
-// Precision modes of the stage kernels: FP64 algebra or FP32 algebra (mixed).
-enum { PM_FP64 = 0, PM_MIXED = 1 };
+// Precision modes of the stage kernels: FP64 algebra with the reference-order
+// FP64 stencils, FP32 algebra (mixed), or FP64 algebra with pair-difference
+// FP64 stencils (PM_FP64F, RK epilogue only: the FP64 pass of the per-tile
+// precision, where parity is with the FP64 path to rounding, not bit for bit).
+enum { PM_FP64 = 0, PM_MIXED = 1, PM_FP64F = 2 };
 
 // Fused RHS (+KO) over a tile work-list in precision mode `precision` (PM_*);
 // with args.tile_prec set, only the tiles flagged args.want_prec.

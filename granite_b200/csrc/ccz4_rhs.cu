@@ -52,11 +52,6 @@ __device__ constexpr int FIELD_ORDER[NV] = {GXX, GXY, GXZ, GYY, GYZ, GZZ, GHX, G
 __device__ __forceinline__ bool tile_selected(const unsigned char* prec, int want, int ti) {
     return !prec || prec[ti] == want;
 }
-// First selected tile at or after ti in the stride-`step` sequence of a persistent CTA.
-__device__ __forceinline__ int next_selected(const unsigned char* prec, int want, int ti, int step, int ntiles) {
-    while (ti < ntiles && !tile_selected(prec, want, ti)) ti += step;
-    return ti;
-}
 
 // Stencils read straight from global memory (through L1). Every source
 // evaluates the stencils of one field in the precision of the caller's algebra
@@ -65,10 +60,11 @@ struct GlobalSource {
     const DevBlock& B;
     const double* __restrict__ u;
     long long c;
-    template <bool HESS, typename P>
+    template <bool HESS, bool EXACT, typename P>
     __device__ __forceinline__ FieldDer<P> der(int v, const double beta[3], P w) {
         const long long off[3] = {1, B.tx, (long long)B.tx * B.ty};
-        return field_der_l<P, HESS, true>(B, GlobalLoad{u + (long long)v * B.stride + c}, off, beta, w);
+        return field_der_l<P, HESS, true, GlobalLoad, EXACT>(B, GlobalLoad{u + (long long)v * B.stride + c}, off,
+                                                             beta, w);
     }
 };
 
@@ -156,7 +152,7 @@ struct SmemSource {
     __device__ __forceinline__ void start() {
         for (int k = 0; k < NBUF - 1; ++k) issue(k);
     }
-    template <bool HESS, typename P>
+    template <bool HESS, bool EXACT, typename P>
     __device__ __forceinline__ FieldDer<P> der(int /*v*/, const double beta[3], P w) {
         cp_async_wait<NBUF - 2>();
         __syncthreads();
@@ -164,7 +160,7 @@ struct SmemSource {
         const long long off[3] = {1, G::BX, G::BX * G::BY};
         const SharedLoad L{sm + (next % NBUF) * G::BOX + lin};
         ++next;
-        return field_der_l<P, HESS, true>(B, L, off, beta, w);
+        return field_der_l<P, HESS, true, SharedLoad, EXACT>(B, L, off, beta, w);
     }
 };
 
@@ -227,6 +223,11 @@ __device__ __forceinline__ void tma_load_box(unsigned dst, const void* map, int 
 // and the host reports the error).
 constexpr unsigned long long TMA_WAIT_NS = 2000000000ull;
 
+// Per-tile precision launches: the CTA's selected tiles, in order, and their
+// count at [TMA_SEL_CAP] (shared memory at a fixed address, so the per-point
+// body keeps no register for them).
+__shared__ int g_sel_list[TMA_SEL_CAP + 1];
+
 template <int NBUF, bool SEL>
 struct TmaSource {
     using R = TmaRing<NBUF>;
@@ -242,13 +243,12 @@ struct TmaSource {
     bool failed;       // a wait of this thread gave up (at item fail_q); thread 0 then stops issuing
     unsigned int* err;
     int fail_q;
-    const int* sel_tile;  // SEL: tile of round r at sel_tile[r & 1] (shared memory, written by thread 0)
 
     // Tile of the CTA's r-th round: blockIdx.x + r gridDim.x, or with per-tile
     // precision (SEL) the r-th tile of that sequence whose flag the launch takes.
     __device__ __forceinline__ int round_tile(int r) const {
         if constexpr (SEL)
-            return sel_tile[r & 1];
+            return r < g_sel_list[TMA_SEL_CAP] ? g_sel_list[r] : ntiles;
         else
             return blockIdx.x + r * gridDim.x;
     }
@@ -285,7 +285,7 @@ struct TmaSource {
     }
     // Every thread of the CTA calls der() for every item in order (the call
     // carries the CTA barrier that frees the slot the next load overwrites).
-    template <bool HESS, typename P>
+    template <bool HESS, bool EXACT, typename P>
     __device__ __forceinline__ FieldDer<P> der(int /*v*/, const double beta[3], P w) {
         __syncthreads();
         if (threadIdx.x == 0 && !failed) issue(next + NBUF - 1);
@@ -293,14 +293,15 @@ struct TmaSource {
         const SharedLoad L{ring + (size_t)(next % NBUF) * R::BOX + lin};
         ++next;
         const long long off[3] = {1, R::BX, R::BX * R::BY};
-        return field_der_l<P, HESS, true>(*B, L, off, beta, w);
+        return field_der_l<P, HESS, true, SharedLoad, EXACT>(*B, L, off, beta, w);
     }
 };
 
 // ---------------------------------------------------------------------------
 // RHS at one interior point. Returns L(u) for the 22 fields in `out` (FP64).
 // ---------------------------------------------------------------------------
-template <typename P, typename Src>
+// EXACT: FP64 stencils in the reference's operation order (P = double only).
+template <typename P, bool EXACT, typename Src>
 __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __restrict__ u,
                                            long long c, const StageArgs& A, Src& S, double out[NV]) {
     const long long st = B.stride;
@@ -352,9 +353,13 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     P dg[6][3];     // d_k gt_ij
     P Rt[6];        // conformal Ricci (ccz4.cpp:465-516), accumulated term by term
     P agt[6], kgt[6];  // advection and KO of gt
-#pragma unroll
+    // Kept as a loop (one copy of the Hessian-field stencil code instead of
+    // six): the per-point body is otherwise longer than the instruction caches
+    // hold, and instruction fetch stalls the warps. The four arrays it fills
+    // (36 values) live in L1-cached local memory for the loop's duration.
+#pragma unroll 1
     for (int a = 0; a < 6; ++a) {
-        FieldDer<P> fd = S.template der<true>(GXX + a, beta, w);
+        FieldDer<P> fd = S.template der<true, EXACT>(GXX + a, beta, w);
 #pragma unroll
         for (int d = 0; d < 3; ++d) dg[a][d] = fd.d[d];
         // term 1: -1/2 gtu^{lm} d_l d_m gt_ij
@@ -391,7 +396,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     P aGh[3], kGh[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        FieldDer<P> fd = S.template der<false>(GHX + a, beta, w);
+        FieldDer<P> fd = S.template der<false, EXACT>(GHX + a, beta, w);
 #pragma unroll
         for (int d = 0; d < 3; ++d) dGh[a][d] = fd.d[d];
         aGh[a] = fd.adv;
@@ -430,7 +435,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     }
 
     // ---- chi: Ricci chi-part (ccz4.cpp:518-541) -----------------------------
-    FieldDer<P> fchi = S.template der<true>(CHI, beta, w);
+    FieldDer<P> fchi = S.template der<true, EXACT>(CHI, beta, w);
     const P chiP = (P)chi;
     // 0.5/(chi+1e-30) and 0.25/(chi^2+1e-30) in FP64 (small chi near the puncture)
     const P c_half = (P)(0.5 / (chi + 1e-30));
@@ -464,7 +469,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     Rs *= chiP;
 
     // ---- lapse -------------------------------------------------------------
-    FieldDer<P> fal = S.template der<true>(ALPHA, beta, w);
+    FieldDer<P> fal = S.template der<true, EXACT>(ALPHA, beta, w);
     P DDa[6];
 #pragma unroll
     for (int ij = 0; ij < 6; ++ij)
@@ -486,7 +491,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     for (int d = 0; d < 3; ++d) ddiv[d] = (P)0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        FieldDer<P> fb = S.template der<true>(BETAX + a, beta, w);
+        FieldDer<P> fb = S.template der<true, EXACT>(BETAX + a, beta, w);
 #pragma unroll
         for (int d = 0; d < 3; ++d) db[a][d] = fb.d[d];
         T5[a] = gtu[0] * fb.h[0] + gtu[3] * fb.h[3] + gtu[5] * fb.h[5] +
@@ -541,7 +546,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
         }
     // K (ccz4.cpp:650-652)
     {
-        FieldDer<P> fK = S.template der<false>(KTR, beta, w);
+        FieldDer<P> fK = S.template der<false, EXACT>(KTR, beta, w);
         const P k1 = (P)A.kappa1, k2 = (P)A.kappa2;
         out[KTR] = (double)((-phys_lap_alpha + alpha * (AtAt + K * K / (P)3) + (P)4 * PI * alpha * (rho + Str) +
                             k1 * ((P)1 - k2) * alpha * Theta + fK.adv) + fK.ko);
@@ -567,7 +572,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     }
     // Theta (ccz4.cpp:662-665)
     {
-        FieldDer<P> fT = S.template der<false>(THETA, beta, w);
+        FieldDer<P> fT = S.template der<false, EXACT>(THETA, beta, w);
         const P k1 = (P)A.kappa1, k2 = (P)A.kappa2;
         out[THETA] = (double)(((P)0.5 * alpha * (Rs - AtAt + (P)2 * K * K / (P)3 - (P)16 * PI * rho) -
                               alpha * k1 * ((P)2 + k2) * Theta + fT.adv) + fT.ko);
@@ -581,7 +586,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
 #pragma unroll
             for (int j = i; j < 3; ++j) {
                 const int ij = sy(i, j);
-                FieldDer<P> fA = S.template der<false>(AXX + ij, beta, w);
+                FieldDer<P> fA = S.template der<false, EXACT>(AXX + ij, beta, w);
                 koA[ij] = fA.ko;
                 const P t1 = chiP * (-DDa[ij] + alpha * (Ric[ij] - (P)8 * PI * Sij[ij]));
                 const P Asq = At[sy(i, 0)] * Am[0][j] + At[sy(i, 1)] * Am[1][j] + At[sy(i, 2)] * Am[2][j];
@@ -655,9 +660,11 @@ template <int PM, typename Src>
 __device__ __forceinline__ void point_pm(const DevBlock& B, const double* __restrict__ u, long long c,
                                          const StageArgs& A, Src& S, double L[NV]) {
     if constexpr (PM == PM_FP64)
-        ccz4_point<double>(B, u, c, A, S, L);
+        ccz4_point<double, true>(B, u, c, A, S, L);
+    else if constexpr (PM == PM_FP64F)
+        ccz4_point<double, false>(B, u, c, A, S, L);
     else
-        ccz4_point<float>(B, u, c, A, S, L);
+        ccz4_point<float, false>(B, u, c, A, S, L);
 }
 
 // Shared epilogue: store L, or RK combine + floors (+ algebraic constraints).
@@ -673,10 +680,18 @@ __device__ __forceinline__ void stage_epilogue(const DevBlock& B, const StageArg
     const double* __restrict__ un = B.buf[A.n_sel];
     double* __restrict__ out = B.buf[A.out_sel];
     double r[NV];
+    if (A.in_sel == A.n_sel) {  // stage 1 reads u^n as both the stage input and u^n: load it once
 #pragma unroll
-    for (int v = 0; v < NV; ++v)
-        r[v] = rk_combine(A.a1, __ldg(un + (long long)v * st + c), A.a2, __ldg(uin + (long long)v * st + c),
-                          A.a3dt, L[v]);
+        for (int v = 0; v < NV; ++v) {
+            const double unv = __ldg(un + (long long)v * st + c);
+            r[v] = rk_combine(A.a1, unv, A.a2, unv, A.a3dt, L[v]);
+        }
+    } else {
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+            r[v] = rk_combine(A.a1, __ldg(un + (long long)v * st + c), A.a2, __ldg(uin + (long long)v * st + c),
+                              A.a3dt, L[v]);
+    }
     // floors, main.cpp:592-606
     {
         double& chi = r[CHI];
@@ -765,32 +780,49 @@ __global__ void __launch_bounds__(V4_NT, 1)
     extern __shared__ unsigned char smem_raw[];
     double* ring = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     const unsigned bar0 = smem_addr(ring + (size_t)NBUF * R::BOX);
-    __shared__ int sel_tile[2];
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int s = 0; s < NBUF; ++s) mbar_init(bar0 + 8u * s, 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-        if constexpr (SEL) {
-            sel_tile[0] = next_selected(A.tile_prec, A.want_prec, blockIdx.x, gridDim.x, ntiles);
-            sel_tile[1] = next_selected(A.tile_prec, A.want_prec, sel_tile[0] + gridDim.x, gridDim.x, ntiles);
+    }
+    // SEL: the CTA's tiles blockIdx.x + m gridDim.x whose flag equals want_prec,
+    // compacted in order into shared memory once (ballot scan over 256 candidates
+    // at a time); the host keeps ntiles <= gridDim.x * TMA_SEL_CAP.
+    __shared__ int warp_cnt[V4_NT / 32];
+    if constexpr (SEL) {
+        int nsel = 0;
+        const int ncand = ntiles > (int)blockIdx.x ? (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+        const int lane = tid & 31, warp = tid >> 5;
+        for (int m0 = 0; m0 < ncand; m0 += V4_NT) {
+            const int m = m0 + tid;
+            const int ti = blockIdx.x + m * gridDim.x;
+            const bool take = m < ncand && A.tile_prec[ti] == A.want_prec;
+            const unsigned bal = __ballot_sync(0xffffffffu, take);
+            if (lane == 0) warp_cnt[warp] = __popc(bal);
+            __syncthreads();
+            int off = 0, tot = 0;
+#pragma unroll
+            for (int w = 0; w < V4_NT / 32; ++w) {
+                off += w < warp ? warp_cnt[w] : 0;
+                tot += warp_cnt[w];
+            }
+            const int pos = nsel + off + __popc(bal & ((1u << lane) - 1u));
+            if (take && pos < TMA_SEL_CAP) g_sel_list[pos] = ti;
+            nsel += tot;
+            __syncthreads();
         }
+        if (tid == 0) g_sel_list[TMA_SEL_CAP] = nsel < TMA_SEL_CAP ? nsel : TMA_SEL_CAP;  // (host keeps it below)
     }
     __syncthreads();
     const int lx = tid % V4_TX, ly = (tid / V4_TX) % V4_TY, lz = tid / (V4_TX * V4_TY);
     TmaSource<NBUF, SEL> S{blocks, tiles, static_cast<const unsigned char*>(A.tmaps), ntiles, A.in_sel, ring, bar0,
                          nullptr, (lx + 4) + R::BX * ((ly + 4) + R::BY * (lz + 4)), 0, false,
-                         A.errflag, 0, sel_tile};
+                         A.errflag, 0};
     if (tid == 0)
         for (int q = 0; q < NBUF - 1; ++q) S.issue(q);
     for (int r = 0;; ++r) {
         const int ti = S.round_tile(r);
         if (ti >= ntiles) break;
-        // SEL: the tile after this one. Round r - 1's entry is free: its items
-        // were all issued before round r began (the producer runs NBUF - 1 < NV
-        // items ahead) and every thread read it when round r - 1 began; the
-        // barrier of the next der() publishes the write.
-        if (SEL && r > 0 && tid == 0)
-            sel_tile[(r + 1) & 1] = next_selected(A.tile_prec, A.want_prec, ti + gridDim.x, gridDim.x, ntiles);
         const Tile t = tiles[ti];
         const DevBlock& B = blocks[t.block];
         S.B = &B;
@@ -880,7 +912,7 @@ static cudaError_t configure_smem() {
 
 // Persistent grid of the TMA variant on each device: SMs x resident CTAs.
 constexpr int MAX_DEVICES = 64;
-static int g_tma_grid[MAX_DEVICES][2][2];  // [device][precision mode][epi]
+static int g_tma_grid[MAX_DEVICES][3][2];  // [device][precision mode][epi]
 
 template <int PM, int EPI, bool SEL = false>
 static cudaError_t configure_tma(int dev, int nsm) {
@@ -892,6 +924,12 @@ static cudaError_t configure_tma(int dev, int nsm) {
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, V4_NT, bytes))) return e;
     if (!SEL) g_tma_grid[dev][PM][EPI] = nsm * (per_sm > 0 ? per_sm : 1);
     return cudaSuccess;
+}
+
+int tma_grid() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return 0;
+    return g_tma_grid[dev][PM_MIXED][EPI_RK];
 }
 
 template <int PM, int EPI>
@@ -924,6 +962,7 @@ cudaError_t configure_stage_kernels() {
     if ((e = configure_smem<PM_FP64, EPI_RK>())) return e;
     if ((e = configure_smem<PM_MIXED, EPI_STORE>())) return e;
     if ((e = configure_smem<PM_MIXED, EPI_RK>())) return e;
+    if ((e = configure_smem<PM_FP64F, EPI_RK>())) return e;
     int dev = 0, nsm = 0;
     if ((e = cudaGetDevice(&dev))) return e;
     if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
@@ -932,7 +971,9 @@ cudaError_t configure_stage_kernels() {
     if ((e = configure_tma<PM_FP64, EPI_RK>(dev, nsm))) return e;
     if ((e = configure_tma<PM_MIXED, EPI_STORE>(dev, nsm))) return e;
     if ((e = configure_tma<PM_MIXED, EPI_RK>(dev, nsm))) return e;
+    if ((e = configure_tma<PM_FP64F, EPI_RK>(dev, nsm))) return e;
     if ((e = configure_tma<PM_FP64, EPI_RK, true>(dev, nsm))) return e;
+    if ((e = configure_tma<PM_FP64F, EPI_RK, true>(dev, nsm))) return e;
     return configure_tma<PM_MIXED, EPI_RK, true>(dev, nsm);
 }
 
@@ -954,6 +995,7 @@ static cudaError_t dispatch(int pm, int epi, const DevBlock* blocks, const Tile*
     if (pm == PM_MIXED)
         return epi == EPI_STORE ? L<PM_MIXED, EPI_STORE>::run(blocks, tiles, ntiles, args, stream)
                                 : L<PM_MIXED, EPI_RK>::run(blocks, tiles, ntiles, args, stream);
+    if (pm == PM_FP64F && epi == EPI_RK) return L<PM_FP64F, EPI_RK>::run(blocks, tiles, ntiles, args, stream);
     return cudaErrorInvalidValue;
 }
 

@@ -89,44 +89,49 @@ __device__ __forceinline__ AxisDer<double> axis_exact(const L& f, long long s, d
     return r;
 }
 
-// Pair-difference evaluation (P = float); the upwind side is selected without
-// a branch as in axis_exact.
-template <bool WANT_D2, bool WANT_KO, typename L>
-__device__ __forceinline__ AxisDer<float> axis_pairs(const L& f, long long s, double f0,
-                                                    double beta, double inv12h, double inv12h2, double kocf,
-                                                    float& ko) {
+// Pair-difference evaluation; the upwind side is selected without a branch as
+// in axis_exact. The pair differences and their weighted sums stay FP64
+// (small, exactly cancelled numbers) and each stencil result is rounded to P
+// once: for P = float one conversion per derivative instead of one per pair;
+// for P = double this is the contraction-friendly FP64 form (no reference
+// operation order) used where bit parity with the host code is not required.
+template <bool WANT_D2, bool WANT_KO, typename P, typename L>
+__device__ __forceinline__ AxisDer<P> axis_pairs(const L& f, long long s, double f0,
+                                                double beta, double inv12h, double inv12h2, double kocf,
+                                                P& ko) {
     const double fm1 = f(-s), fp1 = f(s);
     const double fm2 = f(-2 * s), fp2 = f(2 * s);
     const double fm3 = f(-3 * s), fp3 = f(3 * s);
     const double fm4 = f(-4 * s), fp4 = f(4 * s);
-    AxisDer<float> r;
-    const float a1 = (float)(fp1 - fm1), a2 = (float)(fp2 - fm2);
-    r.d1 = (float)inv12h * (8.0f * a1 - a2);
+    AxisDer<P> r;
+    // 8 (f+1 - f-1) - (f+2 - f-2)
+    r.d1 = (P)inv12h * (P)(8.0 * (fp1 - fm1) - (fp2 - fm2));
     const bool pos = beta >= 0.0;
     const double g1 = pos ? fm1 : fp1, g2 = pos ? fm2 : fp2, g3 = pos ? fm3 : fp3, g4 = pos ? fm4 : fp4;
     // 25 f0 - 48 g1 + 36 g2 - 16 g3 + 3 g4 with weights summing to zero; negated for the + side
     const double e = 48.0 * (f0 - g1) - 36.0 * (f0 - g2) + 16.0 * (f0 - g3) - 3.0 * (f0 - g4);
-    r.up = (float)inv12h * (float)(pos ? e : -e);
-    const float t1 = (float)((fp1 - f0) + (fm1 - f0));
-    const float t2 = (float)((fp2 - f0) + (fm2 - f0));
-    r.d2 = WANT_D2 ? (float)inv12h2 * (16.0f * t1 - t2) : 0.0f;
+    r.up = (P)inv12h * (P)(pos ? e : -e);
+    const double t1 = (fp1 - f0) + (fm1 - f0);
+    const double t2 = (fp2 - f0) + (fm2 - f0);
+    r.d2 = WANT_D2 ? (P)inv12h2 * (P)(16.0 * t1 - t2) : (P)0;
     if (WANT_KO) {
-        const float t3 = (float)((fp3 - f0) + (fm3 - f0));
+        const double t3 = (fp3 - f0) + (fm3 - f0);
         // (f-3 + f+3) - 6 (f-2 + f+2) + 15 (f-1 + f+1) - 20 f0
-        ko += (float)kocf * (t3 - 6.0f * t2 + 15.0f * t1);
+        ko += (P)kocf * (P)(t3 - 6.0 * t2 + 15.0 * t1);
     }
     return r;
 }
 
-// 2nd-order mixed derivative, ccz4.cpp:185-222: inv4hh * (f++ - f+- - f-+ + f--)
-template <typename P, typename L>
+// 2nd-order mixed derivative, ccz4.cpp:185-222: inv4hh * (f++ - f+- - f-+ + f--),
+// in the reference's order (EXACT) or from pair differences.
+template <typename P, bool EXACT, typename L>
 __device__ __forceinline__ P dmix(const L& f, long long sa, long long sb, double inv4hh) {
     const double pp = f(sa + sb), pm = f(sa - sb);
     const double mp = f(-sa + sb), mm = f(-sa - sb);
-    if constexpr (sizeof(P) == 8)
+    if constexpr (EXACT)
         return RN_MUL(inv4hh, RN_ADD(RN_SUB(RN_SUB(pp, pm), mp), mm));
     else
-        return (float)inv4hh * (float)((pp - pm) - (mp - mm));
+        return (P)inv4hh * (P)((pp - pm) - (mp - mm));
 }
 
 // Everything one field contributes: gradient, blended advection, KO, and
@@ -139,9 +144,11 @@ struct FieldDer {
     P h[6]; // xx xy xz yy yz zz
 };
 
-template <typename P, bool HESS, bool KO, typename L>
+// EXACT (P = double only): every stencil in the reference's operation order.
+template <typename P, bool HESS, bool KO, typename L, bool EXACT = (sizeof(P) == 8)>
 __device__ __forceinline__ FieldDer<P> field_der_l(const DevBlock& B, const L& f, const long long off[3],
                                                    const double beta[3], P w) {
+    static_assert(!EXACT || sizeof(P) == 8, "reference-order stencils are FP64");
     const double f0 = f(0);
     FieldDer<P> r;
     P up[3];
@@ -149,10 +156,10 @@ __device__ __forceinline__ FieldDer<P> field_der_l(const DevBlock& B, const L& f
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         AxisDer<P> a;
-        if constexpr (sizeof(P) == 8)
+        if constexpr (EXACT)
             a = axis_exact<HESS, KO>(f, off[d], f0, beta[d], B.inv12h[d], B.inv12h2[d], B.kow[d], ko);
         else
-            a = axis_pairs<HESS, KO>(f, off[d], f0, beta[d], B.inv12h[d], B.inv12h2[d], B.kocf[d], ko);
+            a = axis_pairs<HESS, KO, P>(f, off[d], f0, beta[d], B.inv12h[d], B.inv12h2[d], B.kocf[d], ko);
         r.d[d] = a.d1;
         up[d] = a.up;
         if (HESS) r.h[d == 0 ? 0 : (d == 1 ? 3 : 5)] = a.d2;
@@ -163,9 +170,9 @@ __device__ __forceinline__ FieldDer<P> field_der_l(const DevBlock& B, const L& f
     r.adv = w * up_sum + ((P)1 - w) * cen_sum;
     r.ko = ko;
     if (HESS) {
-        r.h[1] = dmix<P, L>(f, off[0], off[1], B.inv4hh[0]);
-        r.h[2] = dmix<P, L>(f, off[0], off[2], B.inv4hh[1]);
-        r.h[4] = dmix<P, L>(f, off[1], off[2], B.inv4hh[2]);
+        r.h[1] = dmix<P, EXACT, L>(f, off[0], off[1], B.inv4hh[0]);
+        r.h[2] = dmix<P, EXACT, L>(f, off[0], off[2], B.inv4hh[1]);
+        r.h[4] = dmix<P, EXACT, L>(f, off[1], off[2], B.inv4hh[2]);
     } else {
 #pragma unroll
         for (int a = 0; a < 6; ++a) r.h[a] = (P)0;

@@ -220,12 +220,14 @@ GRANITE_API int granite_ccz4_get_kernel_variant(const void* ctx, int* variant);
 
 /* Per-tile precision of GRANITE_PRECISION_MIXED steps (no counterpart in the
  * reference): in every RK stage of granite_ccz4_rk3_step /
- * granite_ccz4_hierarchy_step, a tile of the work-list whose stage input has
- * a point with chi < chi_fp64 (or a non-finite chi) runs the FP64 algebra,
- * every other tile the FP32 algebra. The stage kernel decides per tile from
- * the current chi (one CTA-wide vote), so the choice follows moving punctures
- * and costs no extra launch. 0 (the default) disables it; +large makes MIXED
- * steps identical to FP64 ones. Changing it drops the cached step graphs. The
+ * granite_ccz4_hierarchy_step a classification kernel flags the tiles whose
+ * stage input has a point with chi < chi_fp64 (or a non-finite chi); those
+ * tiles are computed with the FP64 algebra (FP64 pair-difference stencils:
+ * equal to GRANITE_PRECISION_FP64 to rounding, not bit for bit), every other
+ * tile with the FP32 algebra. The flags come from the current chi on the
+ * device, so the choice follows moving punctures and stays inside the step's
+ * CUDA graph. 0 (the default) disables it; a value above every chi runs the
+ * FP64 algebra on every tile. Changing it drops the cached step graphs. The
  * stateless operators (granite_ccz4_compute_rhs_*) are not affected. */
 GRANITE_API int granite_ccz4_set_fp64_chi_threshold(void* ctx, double chi_fp64);
 GRANITE_API int granite_ccz4_get_fp64_chi_threshold(const void* ctx, double* chi_fp64);
