@@ -47,6 +47,9 @@ sys.path.insert(0, ROOT)
 METRIC = "CCZ4 RK3 point-updates/s on 1 B200: mixed/batched vs FP64 plain, equal accuracy"
 UNIT = "point-updates/s"
 BYTES_PER_POINT_UPDATE = 1408  # 3 stages: (2 + 3 + 3) x 22 fields x 8 B
+# reference-equivalent flops per point-update: 3 RHS + KO evaluations as ccz4.cpp
+# is written (10,395 each, op-counted) + the RK combine (22 fields x 3 stages x 4)
+FLOPS_PER_POINT_UPDATE = 3 * 10395 + 22 * 3 * 4
 NV = 22
 GROUPS = [[0], [1, 2, 3, 4, 5, 6], [7, 8, 9, 10, 11, 12], [13], [14, 15, 16], [17], [18], [19, 20, 21]]
 
@@ -297,11 +300,19 @@ def roofline(gb, run: Runner, workload, prof_steps, kernel):
     achieved = total_bytes / (st_ms / 1000.0) / 1e9
     per_launch = total_bytes / max(st_n, 1)
     traffic = ncu_traffic(workload, kernel)
+    # the bound that applies to this kernel: its FP64 / FP32 pipes (HBM is ~10 % busy)
+    fp64_peak = gb.measure_fma_rate(run.ev.params.device, 0)
+    fp32_peak = gb.measure_fma_rate(run.ev.params.device, 1)
+    flops = FLOPS_PER_POINT_UPDATE * run.points_per_step * prof_steps / (st_ms / 1000.0) / 1e12
+    compute = {"unit": "TFLOP/s", "achieved": flops, "flops_per_point_update": FLOPS_PER_POINT_UPDATE,
+               "flops": "reference-equivalent (ccz4.cpp as written, op-counted), per point-update",
+               "peak_fp64": fp64_peak, "peak_fp32": fp32_peak, "frac_of_fp64": flops / fp64_peak,
+               "peak_source": "measured here: register-only FMA kernel at full occupancy"}
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "peak_source": peak_kind, "kernel": kernel,
             "avg_launch_ms": st_ms / max(st_n, 1), "launches_per_step": st_n / prof_steps,
             "algorithmic_bytes_per_launch": per_launch,
-            "stage_share_of_step": st_ms / max(st_ms + gh_ms + xf_ms, 1e-12)}
+            "stage_share_of_step": st_ms / max(st_ms + gh_ms + xf_ms, 1e-12), "compute": compute}
 
 
 def accuracy(gb, a: Runner, b: Runner, steps: int):

@@ -105,6 +105,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_set_batching.argtypes = [vp, C.c_int]
     lib.granite_ccz4_get_kernel_variant.argtypes = [vp, C.POINTER(C.c_int)]
     lib.granite_ccz4_set_fp64_chi_threshold.argtypes = [vp, C.c_double]
+    lib.granite_ccz4_measure_fma_rate.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
     lib.granite_ccz4_get_fp64_chi_threshold.argtypes = [vp, C.POINTER(C.c_double)]
     _LIB = lib
     return lib
@@ -119,6 +120,16 @@ def _dp(a):
 # ---------------------------------------------------------------------------
 # GridBlock (include/granite/core/grid.hpp:44-162)
 # ---------------------------------------------------------------------------
+
+def measure_fma_rate(device: int = 0, precision: int = 0) -> float:
+    """Sustained FMA rate of a device in TFLOP/s: FP64 (precision 0) or FP32 (1)."""
+    lib = load_library()
+    v = C.c_double()
+    rc = lib.granite_ccz4_measure_fma_rate(int(device), int(precision), C.byref(v))
+    if rc != 0:
+        raise GraniteError(rc, "granite_ccz4_measure_fma_rate failed")
+    return v.value
+
 
 class GridBlock:
     """Field-major block storage with the reference GridBlock layout.

@@ -879,15 +879,10 @@ int granite_ccz4_download_block(void* h, int i, double* host) {
 // or (unbatched) one launch per block.
 // One stage over tiles [first, first + count) of a level: one launch, or with
 // per-tile precision (MIXED and a positive chi threshold) a classification of
-// the tiles from the stage input's chi (flag 1: a point below the threshold)
-// and an FP64 pass over the flagged tiles:
-//  - stages that write a buffer they do not read (1 and 2): the plain FP32
-//    kernel over every tile, then the FP64 pass overwrites the flagged tiles'
-//    outputs (both read only the stage input and u^n, so the stream order makes
-//    the FP64 values final; the ~1 % flagged tiles are computed twice, and the
-//    FP64 pass does not count non-finite floor hits again);
-//  - the last stage, which updates u^n in place: the FP32 kernel over the
-//    unflagged tiles only, then the FP64 pass (disjoint tiles).
+// the tiles from the stage input's chi (flag 1: a point below the threshold),
+// then the FP32 kernel over the unflagged tiles and the FP64 kernel over the
+// flagged ones. The two passes write disjoint tiles, so the in-place last
+// stage is safe and no tile is computed twice.
 static cudaError_t stage_range(Ctx* c, LevelLists& L, int precision, const StageArgs& a, int first, int count,
                                long long* n) {
     const Tile* tiles = L.d_tiles + first;
@@ -899,21 +894,12 @@ static cudaError_t stage_range(Ctx* c, LevelLists& L, int precision, const Stage
         return launch_stage(L.variant, precision, EPI_RK, c->d_blocks, tiles, count, a, c->stream);
     }
     unsigned char* flags = L.d_flags + first;
-    const bool in_place = a.out_sel == a.n_sel || a.out_sel == a.in_sel;
-    cudaError_t e;
+    cudaError_t e = launch_classify(L.variant, c->d_blocks, tiles, 0, count, a.in_sel, c->fp64_chi, flags, c->stream);
+    if (e != cudaSuccess) return e;
     StageArgs b = a;
     b.tile_prec = flags;
-    if (in_place) {
-        if ((e = launch_classify(L.variant, c->d_blocks, tiles, 0, count, a.in_sel, c->fp64_chi, flags, c->stream)))
-            return e;
-        b.want_prec = 0;
-        if ((e = launch_stage(L.variant, PM_MIXED, EPI_RK, c->d_blocks, tiles, count, b, c->stream))) return e;
-    } else {
-        if ((e = launch_stage(L.variant, PM_MIXED, EPI_RK, c->d_blocks, tiles, count, a, c->stream))) return e;
-        if ((e = launch_classify(L.variant, c->d_blocks, tiles, 0, count, a.in_sel, c->fp64_chi, flags, c->stream)))
-            return e;
-        b.nonfinite = nullptr;
-    }
+    b.want_prec = 0;
+    if ((e = launch_stage(L.variant, PM_MIXED, EPI_RK, c->d_blocks, tiles, count, b, c->stream))) return e;
     b.want_prec = 1;
     *n += 3;
     return launch_stage(L.variant, PM_FP64F, EPI_RK, c->d_blocks, tiles, count, b, c->stream);

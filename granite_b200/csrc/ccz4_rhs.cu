@@ -23,8 +23,8 @@
 // conformal metric, the 1/chi factors, the evolved state and the RK3 combine
 // stay FP64. Per-tile precision: a launch can be restricted to the tiles of a
 // flag array (classify_tiles_kernel marks the tiles with a point of chi below a
-// threshold, near a puncture), so an FP64 pass recomputes those tiles after
-// (or beside) the FP32 pass, walking the tile list in its spatial order.
+// threshold, near a puncture): the FP64 kernel takes those tiles and the FP32
+// kernel the others, both walking the tile list in its spatial order.
 //
 // Control flow: the per-point body is one straight-line sequence (the KO term
 // is always evaluated -- its weights sigma/(64 dx) w_s are zero when KO is off

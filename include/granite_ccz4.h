@@ -195,6 +195,11 @@ GRANITE_API int granite_ccz4_nonfinite_count(void* ctx, long long* count);
  * last reset (it synchronises the stream). No counterpart in the reference
  * (which has no timers). */
 GRANITE_API int granite_ccz4_set_profiling(void* ctx, int enabled);
+/* Sustained FMA rate of a device in TFLOP/s (2 flops per FMA), FP64
+ * (GRANITE_PRECISION_FP64) or FP32 (GRANITE_PRECISION_MIXED), from a
+ * register-only kernel at full occupancy: the compute roofline the stage
+ * kernels are measured against. No counterpart in the reference. */
+GRANITE_API int granite_ccz4_measure_fma_rate(int device, int precision, double* tflops);
 GRANITE_API int granite_ccz4_profile_reset(void* ctx);
 GRANITE_API int granite_ccz4_profile_get(void* ctx, int kernel_class, double* total_ms,
                                          long long* launches);

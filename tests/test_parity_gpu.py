@@ -325,3 +325,11 @@ def test_nonfinite_state_is_floored_and_counted(gb, oracle_lib):
     out, ev = run_steps(gb, g, u, Params(), 0.01, 1, gb.BC_REFERENCE)
     assert ev.nonfinite_count() > 0
     np.testing.assert_array_equal(np.isfinite(out), np.isfinite(ref))
+
+
+def test_fma_rate_probe(gb):
+    # the compute roofline bench.py reports: FP64 and FP32 FMA rates of the device
+    f64 = gb.measure_fma_rate(0, gb.PRECISION_FP64)
+    f32 = gb.measure_fma_rate(0, gb.PRECISION_MIXED)
+    assert 1.0 < f64 < 1000.0 and 1.0 < f32 < 1000.0
+    assert f32 >= f64
