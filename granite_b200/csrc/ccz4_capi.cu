@@ -116,6 +116,11 @@ struct LevelXfer {
     GhostSrc* d_src = nullptr;            // one source per ghost cell of the level (GHOSTS)
     long long nsrc = 0;
     std::vector<std::pair<long long, long long>> src_range;  // per block: first item, count
+    // the ghost cells the stage stencils read (faces, and edges one cell deep for the
+    // mixed derivatives; never corners): the fills of the RK stage buffers
+    GhostSrc* d_src_stage = nullptr;
+    long long nsrc_stage = 0;
+    std::vector<std::pair<long long, long long>> src_range_stage;
 };
 
 // device copy of a host vector (nullptr for an empty one)
@@ -556,6 +561,7 @@ int granite_ccz4_destroy(void* h) {
             for (auto& r : X.restrict_) free_xfer(r);
             cudaFree(X.d_facemask);
             cudaFree(X.d_src);
+            cudaFree(X.d_src_stage);
         }
     cudaFree(c->d_blocks);
     cudaFree(c->arena);
@@ -1154,8 +1160,9 @@ int build_ghosts_mode(Ctx* c) {
         CK(upload_xfer(pro, X[L].prolong, c->stream), "upload prolongation boxes");
         // one source per ghost cell: same-level neighbour over coarse block over own fill
         {
-            std::vector<GhostSrc> items;
+            std::vector<GhostSrc> items, sitems;
             X[L].src_range.clear();
+            X[L].src_range_stage.clear();
             for (int f : blocks) {
                 const long long first = (long long)items.size();
                 const auto& fd = c->descs[f];
@@ -1192,9 +1199,21 @@ int build_ghosts_mode(Ctx* c) {
                 std::stable_sort(items.begin() + first, items.end(),
                                  [&](const GhostSrc& a, const GhostSrc& b) { return kind(a) < kind(b); });
                 X[L].src_range.push_back({first, (long long)items.size() - first});
+                // the subset the stencils of a stage read: depth into the ghost layer per axis
+                const long long sfirst = (long long)sitems.size();
+                auto depth = [](int a, int T) { return a < NG ? NG - a : (a >= T - NG ? a - (T - NG) + 1 : 0); };
+                for (long long q = first; q < (long long)items.size(); ++q) {
+                    const int cell = items[q].dst_cell;
+                    const int di = depth(cell % T0, T0), dj = depth((cell / T0) % T1, T1), dk = depth(cell / (T0 * T1), T2);
+                    const int outside = (di > 0) + (dj > 0) + (dk > 0);
+                    if (outside == 1 || (outside == 2 && std::max(di, std::max(dj, dk)) == 1)) sitems.push_back(items[q]);
+                }
+                X[L].src_range_stage.push_back({sfirst, (long long)sitems.size() - sfirst});
             }
             CK(upload_vec(items, &X[L].d_src, c->stream), "upload ghost sources");
             X[L].nsrc = (long long)items.size();
+            CK(upload_vec(sitems, &X[L].d_src_stage, c->stream), "upload stage ghost sources");
+            X[L].nsrc_stage = (long long)sitems.size();
         }
         // restriction into level L-1 from level L
         if (L == 0) continue;
@@ -1339,18 +1358,23 @@ cudaError_t fill_level(Ctx* c, int L, int slot, bool level_fill, int mode, long 
         return level_ghost(c, ll, GHOST_SOMMERFELD, slot, nullptr, n);
     }
     // GRANITE_AMR_GHOSTS: every ghost cell once, from a same-level neighbour if one
-    // covers it, else from the coarse level, else from the block's own fill
+    // covers it, else from the coarse level, else from the block's own fill. The
+    // state (slot 0) gets every ghost cell (finer levels prolong from it, callers
+    // read it); an RK stage buffer only the cells the stage stencils read.
     const int local = level_fill ? GHOST_ZERO_GRADIENT : GHOST_SOMMERFELD;
+    const bool all = slot == 0;
+    const GhostSrc* src = all ? X.d_src : X.d_src_stage;
+    const auto& ranges = all ? X.src_range : X.src_range_stage;
     if (c->batched) {
         ++*n;
         return timed(c, GRANITE_KERNEL_GHOST, [&] {
-            return launch_ghost_sources(c->d_blocks, X.d_src, X.nsrc, slot, local, c->stream);
+            return launch_ghost_sources(c->d_blocks, src, all ? X.nsrc : X.nsrc_stage, slot, local, c->stream);
         });
     }
-    for (const auto& r : X.src_range) {
+    for (const auto& r : ranges) {
         ++*n;
         if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] {
-                 return launch_ghost_sources(c->d_blocks, X.d_src + r.first, r.second, slot, local, c->stream);
+                 return launch_ghost_sources(c->d_blocks, src + r.first, r.second, slot, local, c->stream);
              })))
             return e;
     }
