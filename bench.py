@@ -188,73 +188,116 @@ class ClockSampler:
 # CPU reference (bounded samples)
 # ---------------------------------------------------------------------------
 
-def reference_sample(w, seconds_target: float):
-    """The compiled reference (Release flags, OpenMP on all cores) advancing blocks of
-    the workload by whole RK3 steps (reference boundaries per block) until
-    ~seconds_target of CPU work; returns a cpu_baseline object."""
+def reference_impl():
+    """The compiled reference (Release flags, OpenMP on all cores), else the C restatement."""
     import oracle
-    from oracle import Geom, Params
     if oracle.reference_available("fast"):
-        impl, kind = oracle.Reference("fast"), "reference"
-        cores = impl.max_threads()
-    else:
-        impl, kind = oracle.Oracle(), "port"
-        cores = os.cpu_count()
+        impl = oracle.Reference("fast")
+        return impl, "reference", impl.max_threads()
+    return oracle.Oracle(), "port", os.cpu_count()
+
+
+def reference_jobs(w):
+    """Endless sequence of (geometry, state, dt, bc) units of the workload for the
+    reference: hierarchy blocks taken round-robin over the levels (so every level's
+    sizes appear), each as a single block; or the workload's single block."""
+    import oracle
+    from oracle import Geom
     o = oracle.Oracle()
     if w["kind"] == "hier":
         import granite_b200 as gb
         h = (gb.make_binary_hierarchy if w["builder"] == "binary" else gb.make_triple_hierarchy)()
-        # blocks taken round-robin over the levels, so every level's sizes appear
         per = [[b for b in h.blocks if b.level == L] for L in range(h.num_levels)]
         order = [per[L][i] for i in range(max(len(p) for p in per)) for L in range(h.num_levels) if i < len(per[L])]
-
-        def block_jobs():
+        while True:
             for b in order:
                 g = Geom(b.ncells, b.lo, b.hi)
                 u = o.init_brill_lindquist(g, h.masses, h.positions, r_floor=0.5 * g.dx[0])
                 yield g, oracle.add_noise(u, 1e-10, 12345), 0.25 * h.level_dx[b.level], 0
-
-        jobs = block_jobs()
-        desc = "one RK3 step of each of {} blocks of the hierarchy ({} interior points), each as a single block"
+    n, lo, hi = w["n"], w["lo"], w["hi"]
+    g = Geom((n, n, n), (lo, lo, lo), (hi, hi, hi))
+    if w["data"] == "bl":
+        u = oracle.add_noise(o.init_brill_lindquist(g, [1.0], [[0.0, 0.0, 0.0]], r_floor=0.5 * g.dx[0]), 1e-10, 12345)
     else:
-        n, lo, hi = w["n"], w["lo"], w["hi"]
-        g = Geom((n, n, n), (lo, lo, lo), (hi, hi, hi))
-        if w["data"] == "bl":
-            u = oracle.add_noise(o.init_brill_lindquist(g, [1.0], [[0.0, 0.0, 0.0]], r_floor=0.5 * g.dx[0]),
-                                 1e-10, 12345)
-        else:
-            u = o.init_gauge_wave(g, -0.1, 1.0)
-        jobs = [(g, u, 0.25 * g.dx[0], w["bc"])] * 1000
-        desc = "{} RK3 step(s) of the full workload block ({} interior points per step)"
-    total, pts, used, npts_block = 0.0, 0, 0, 0
-    for g, u, dt, bc in jobs:
-        npts_block = int(np.prod(g.n))
-        t = time.perf_counter()
-        impl.rk3_steps(Params(), g, u, dt, 1, bc)
-        total += time.perf_counter() - t
-        pts += int(np.prod(g.n))
+        u = o.init_gauge_wave(g, -0.1, 1.0)
+    while True:
+        yield g, u, 0.25 * g.dx[0], w["bc"]
+
+
+def reference_unit(impl, job):
+    """One RK3 step of one unit by the reference; returns (seconds, interior points)."""
+    from oracle import Params
+    g, u, dt, bc = job
+    t = time.perf_counter()
+    impl.rk3_steps(Params(), g, u, dt, 1, bc)
+    return time.perf_counter() - t, int(np.prod(g.n))
+
+
+def reference_sample(w, seconds_target: float):
+    """The reference advancing units of the workload by whole RK3 steps until
+    ~seconds_target of CPU work; returns a cpu_baseline object."""
+    impl, kind, cores = reference_impl()
+    total, pts, used = 0.0, 0, 0
+    for job in reference_jobs(w):
+        dt_s, n = reference_unit(impl, job)
+        total += dt_s
+        pts += n
         used += 1
         if total >= seconds_target:
             break
-    sample = desc.format(used, pts if w["kind"] == "hier" else npts_block)
+    what = "blocks of the hierarchy, each as a single block" if w["kind"] == "hier" else "steps of the workload block"
+    sample = f"one RK3 step of each of {used} {what} ({pts} interior point-updates)"
     return {"value": pts / total, "unit": UNIT, "cores": int(cores), "kind": kind,
             "sample": f"{sample}; {total:.1f} s; OMP threads = {cores}"}
 
 
+# points of one reference step sample: a few seconds of host work on a many-core host
+REFERENCE_SAMPLE_POINTS = 1 << 21
+
+
 def run_reference(args, w, rank, world):
+    """--impl reference: W warm-up and K timed steps of the reference, each step a
+    bounded sample of the workload (units until ~2.1 M interior points; the whole
+    block for single-block workloads) advanced by one RK3 step on all host cores."""
     if rank != 0:
         return 0
     import oracle
     if not (oracle.reference_available("fast") or os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so"))):
         print(json.dumps({"impl": "reference", "unavailable": "compiled reference library not built"}))
         return 0
-    cb = reference_sample(w, seconds_target=min(120.0, 4.0 * max(1, args.steps)))
-    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world, "steps": 1,
-            "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": args.workload, "precision": "fp64", "parallelism": "host OpenMP"},
+    impl, kind, cores = reference_impl()
+    jobs = reference_jobs(w)
+
+    def one_step():
+        sec, pts = 0.0, 0
+        while pts < REFERENCE_SAMPLE_POINTS:
+            dt_s, n = reference_unit(impl, next(jobs))
+            sec += dt_s
+            pts += n
+            if w["kind"] != "hier":
+                break
+        return sec, pts
+
+    for _ in range(args.warmup):
+        one_step()
+    times, points = [], []
+    for _ in range(args.steps):
+        sec, pts = one_step()
+        times.append(sec)
+        points.append(pts)
+    value = sum(points) / sum(times)
+    what = "hierarchy blocks taken round-robin over the levels, each as a single block" if w["kind"] == "hier" \
+        else "the workload block"
+    cb = {"value": value, "unit": UNIT, "cores": int(cores), "kind": kind,
+          "sample": f"{args.steps} steps of one RK3 step of {what}, ~{int(np.mean(points))} interior points "
+                    f"per step; {sum(times):.1f} s timed; OMP threads = {cores}"}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * sum(times) / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.workload, "precision": "fp64", "parallelism": "host OpenMP",
+                       "points_per_step": int(np.mean(points))},
             "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
 
