@@ -58,6 +58,10 @@ class _BlockDesc(C.Structure):
 _LIB = None
 
 
+# granite_regrid_fn: int (*)(void* user, int level, long long step_num)
+_REGRID_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_longlong)
+
+
 def library_path() -> str:
     return _build.LIB
 
@@ -107,6 +111,10 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_set_fp64_chi_threshold.argtypes = [vp, C.c_double]
     lib.granite_ccz4_measure_fma_rate.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
     lib.granite_ccz4_get_fp64_chi_threshold.argtypes = [vp, C.POINTER(C.c_double)]
+    lib.granite_ccz4_regrid_add.argtypes = [vp, C.POINTER(_BlockDesc), C.c_int]
+    lib.granite_ccz4_hierarchy_step_regrid.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.c_int, _REGRID_FN, vp]
+    lib.granite_ccz4_level_time.argtypes = [vp, C.c_int, dp]
+    lib.granite_ccz4_tag_count.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_longlong)]
     _LIB = lib
     return lib
 
@@ -389,6 +397,43 @@ class Evolver:
             a = self.blocks[i].array if out is None else _f64(out)
             self.ctx.check(self.ctx.lib.granite_ccz4_download_block(self.ctx.h, i, _dp(a)))
 
+    def regrid_add(self, blocks):
+        """Append GridBlocks to the committed hierarchy; the device fills every cell of
+        each (ghosts included) by prolongation from the coarser level's last block
+        (granite_ccz4_regrid_add). Existing blocks keep their state and indices."""
+        blocks = list(blocks)
+        if not blocks:
+            return
+        descs = (_BlockDesc * len(blocks))(*[b.desc() for b in blocks])
+        self.ctx.check(self.ctx.lib.granite_ccz4_regrid_add(self.ctx.h, descs, len(blocks)))
+        self.blocks.extend(blocks)
+
+    def tag_count(self, level: int, var: int, threshold: float) -> int:
+        """Interior cells of ``level`` that gradientChiTagger (var 0) or
+        gradientLapseTagger (var 18) tags (amr.cpp:653-731), counted on the device."""
+        n = C.c_longlong()
+        self.ctx.check(self.ctx.lib.granite_ccz4_tag_count(self.ctx.h, level, var, float(threshold),
+                                                           C.byref(n)))
+        return n.value
+
+    def regrid(self, planner, level: int, tagger=None):
+        """AMRHierarchy::regrid(level, tagger) (amr.cpp:80-301) on the device state.
+
+        ``planner`` is a ``regrid.RegridPlanner``; ``tagger`` is None (never tags)
+        or (var, threshold) for the chi / lapse gradient tagger, consulted only
+        when no tracking sphere requires level + 1, as in the reference. Returns
+        the GridBlocks added (their host arrays stay zero until ``download``).
+        """
+        if not any(b.level == level for b in self.blocks):
+            return []
+        if not planner.spheres_require(level + 1):
+            if tagger is None or self.tag_count(level, tagger[0], tagger[1]) == 0:
+                return []
+        new = [GridBlock(bx.id, bx.level, bx.ncells, bx.lo, bx.hi)
+               for bx in planner.plan(level, self.blocks)]
+        self.regrid_add(new)
+        return new
+
     def rk3_step(self, level: int, dt: float, precision: int = PRECISION_FP64,
                  bc: int = BC_REFERENCE):
         self.ctx.check(self.ctx.lib.granite_ccz4_rk3_step(self.ctx.h, level, dt, precision, bc))
@@ -397,6 +442,36 @@ class Evolver:
                        amr_mode: int = AMR_REFERENCE):
         self.ctx.check(self.ctx.lib.granite_ccz4_hierarchy_step(self.ctx.h, dt_coarse, precision,
                                                                 amr_mode))
+
+    def hierarchy_step_regrid(self, dt_coarse: float, planner, regrid_interval: int, tagger=None,
+                              precision: int = PRECISION_FP64, amr_mode: int = AMR_REFERENCE):
+        """One coarse step of AMRHierarchy::subcycle with its in-step regrid
+        (amr.cpp:303-350): at every level step whose step number is a multiple of
+        ``regrid_interval``, ``regrid(planner, level, tagger)`` runs before the
+        step goes on, as in the reference. Returns the GridBlocks added."""
+        added, errors = [], []
+
+        def on_regrid(_user, level, _step_num):
+            try:
+                added.extend(self.regrid(planner, level, tagger))
+                return 0
+            except Exception as e:  # reported after the step returns
+                errors.append(e)
+                return -1
+
+        fn = _REGRID_FN(on_regrid)
+        rc = self.ctx.lib.granite_ccz4_hierarchy_step_regrid(self.ctx.h, dt_coarse, precision, amr_mode,
+                                                             int(regrid_interval), fn, None)
+        if errors:
+            raise errors[0]
+        self.ctx.check(rc)
+        return added
+
+    def level_time(self, level: int) -> float:
+        """Level::current_time of the reference hierarchy (amr.hpp:108-113)."""
+        t = C.c_double()
+        self.ctx.check(self.ctx.lib.granite_ccz4_level_time(self.ctx.h, level, C.byref(t)))
+        return t.value
 
     def sync(self):
         self.ctx.check(self.ctx.lib.granite_ccz4_sync(self.ctx.h))

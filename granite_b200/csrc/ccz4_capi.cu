@@ -176,6 +176,10 @@ struct Ctx {
     bool committed = false;
     std::vector<LevelLists> levels;
     std::vector<bool> level_ghosts_valid;
+    // AMRHierarchy Level::current_time per level (amr.hpp:108-113): advanced by
+    // the level's dt at every step of the level; a level a regrid creates starts
+    // at its parent's time (amr.cpp:137-143)
+    std::vector<double> level_time;
     std::map<std::tuple<int, int, int, unsigned long long, int>, Graph> graphs;
     // hierarchy transfer lists per AMR mode (built on first use), and graphs
     // of whole subcycled coarse steps keyed by (precision, mode, dt bits)
@@ -534,36 +538,19 @@ int granite_ccz4_create(const granite_ccz4_params* p, void** out) {
     return GRANITE_OK;
 }
 
+static void release_lists(Ctx* c);
+
 int granite_ccz4_destroy(void* h) {
     Ctx* c = static_cast<Ctx*>(h);
     if (!c) return GRANITE_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (auto& kv : c->graphs)
-        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     for (auto& p : c->pending) {
         cudaEventDestroy(p.a);
         cudaEventDestroy(p.b);
     }
     for (auto e : c->event_pool) cudaEventDestroy(e);
-    for (auto& L : c->levels) {
-        cudaFree(L.d_tiles);
-        cudaFree(L.d_flags);
-        cudaFree(L.d_mtiles);
-        cudaFree(L.d_ghost);
-    }
-    for (auto& kv : c->hgraphs)
-        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-    for (auto& mode : c->xfer)
-        for (auto& X : mode) {
-            free_xfer(X.prolong);
-            free_xfer(X.copy);
-            for (auto& r : X.restrict_) free_xfer(r);
-            cudaFree(X.d_facemask);
-            cudaFree(X.d_src);
-            cudaFree(X.d_src_stage);
-        }
-    cudaFree(c->d_blocks);
+    release_lists(c);
     cudaFree(c->arena);
     cudaFree(c->s_u);
     cudaFree(c->s_rhs);
@@ -574,7 +561,6 @@ int granite_ccz4_destroy(void* h) {
     cudaFree(c->s_sum);
     cudaFree(c->d_nonfinite);
     cudaFree(c->d_errflag);
-    cudaFree(c->d_tmaps);
     cudaFree(c->s_tmap);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -768,33 +754,71 @@ int granite_ccz4_arena_bytes(const void* h, size_t* bytes) {
     return GRANITE_OK;
 }
 
-int granite_ccz4_commit(void* h) {
-    Ctx* c = static_cast<Ctx*>(h);
-    if (!c) return GRANITE_ERR_INVALID;
-    if (c->committed) return fail(c, GRANITE_ERR_INVALID, "already committed");
-    if (c->descs.empty()) return fail(c, GRANITE_ERR_INVALID, "no blocks");
-    CK(cudaSetDevice(c->device), "cudaSetDevice");
-    // arena: 3 buffers per block, each 256-byte aligned
-    std::vector<size_t> off(c->descs.size());
+namespace {
+cudaError_t upload_xfer(const std::vector<XferBox>& boxes, XferList& out, cudaStream_t s);
+}
+
+// Arena layout of a block list: 3 buffers per block, each 256-byte aligned.
+static int alloc_arena(Ctx* c, const std::vector<granite_block_desc>& descs, char** arena, size_t* bytes,
+                       std::vector<DevBlock>& hb) {
+    std::vector<size_t> off(descs.size());
     size_t total = 0;
-    for (size_t i = 0; i < c->descs.size(); ++i) {
+    for (size_t i = 0; i < descs.size(); ++i) {
         off[i] = total;
-        const size_t one = ((size_t)cells_of(c->descs[i]) * NV * sizeof(double) + 255) / 256 * 256;
+        const size_t one = ((size_t)cells_of(descs[i]) * NV * sizeof(double) + 255) / 256 * 256;
         total += 3 * one;
     }
-    CK(cudaMalloc(&c->arena, total), "cudaMalloc(arena)");
-    c->arena_bytes = total;
-    int maxlev = 0;
-    c->hblocks.resize(c->descs.size());
-    for (size_t i = 0; i < c->descs.size(); ++i) {
-        DevBlock d = make_devblock(c->descs[i], c->p.ko_sigma);
-        const size_t one = ((size_t)cells_of(c->descs[i]) * NV * sizeof(double) + 255) / 256 * 256;
-        for (int sl = 0; sl < 3; ++sl) d.buf[sl] = reinterpret_cast<double*>(c->arena + off[i] + sl * one);
-        c->hblocks[i] = d;
-        maxlev = std::max(maxlev, c->descs[i].level);
+    CK(cudaMalloc(arena, total), "cudaMalloc(arena)");
+    *bytes = total;
+    hb.resize(descs.size());
+    for (size_t i = 0; i < descs.size(); ++i) {
+        DevBlock d = make_devblock(descs[i], c->p.ko_sigma);
+        const size_t one = ((size_t)cells_of(descs[i]) * NV * sizeof(double) + 255) / 256 * 256;
+        for (int sl = 0; sl < 3; ++sl) d.buf[sl] = reinterpret_cast<double*>(*arena + off[i] + sl * one);
+        hb[i] = d;
     }
-    CK(cudaMemsetAsync(c->arena, 0, total, c->stream), "memset arena");
+    return GRANITE_OK;
+}
+
+// Everything derived from the block list (not the arena): block table, tensor
+// maps, per-level work-lists, transfer lists and the cached step graphs.
+static void release_lists(Ctx* c) {
+    for (auto& kv : c->graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    for (auto& kv : c->hgraphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    c->graphs.clear();
+    c->hgraphs.clear();
+    for (auto& L : c->levels) {
+        cudaFree(L.d_tiles);
+        cudaFree(L.d_flags);
+        cudaFree(L.d_mtiles);
+        cudaFree(L.d_ghost);
+    }
+    c->levels.clear();
+    for (int m = 0; m < 2; ++m) {
+        for (auto& X : c->xfer[m]) {
+            free_xfer(X.prolong);
+            free_xfer(X.copy);
+            for (auto& r : X.restrict_) free_xfer(r);
+            cudaFree(X.d_facemask);
+            cudaFree(X.d_src);
+            cudaFree(X.d_src_stage);
+        }
+        c->xfer[m].clear();
+        c->xfer_built[m] = false;
+    }
+    cudaFree(c->d_blocks);
+    c->d_blocks = nullptr;
+    cudaFree(c->d_tmaps);
+    c->d_tmaps = nullptr;
+}
+
+// Block table, tensor maps and per-level work-lists of c->descs / c->hblocks.
+static int build_lists(Ctx* c) {
     CK(upload_vec(c->hblocks, &c->d_blocks, c->stream), "upload block table");
+    int maxlev = 0;
+    for (const auto& d : c->descs) maxlev = std::max(maxlev, d.level);
     // TMA variant: one tensor map per (block, slot); a block that cannot be
     // mapped sends its whole level to the global-load kernel
     std::vector<char> mapped(c->descs.size(), 0);
@@ -837,9 +861,119 @@ int granite_ccz4_commit(void* h) {
     }
     int maxt = 0;
     for (auto& L : c->levels) maxt = std::max(maxt, std::max(L.ntiles, L.nmtiles));
-    int r = ensure_scratch(c, 1, std::max(1, maxt));
+    return ensure_scratch(c, 1, std::max(1, maxt));
+}
+
+int granite_ccz4_commit(void* h) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (c->committed) return fail(c, GRANITE_ERR_INVALID, "already committed");
+    if (c->descs.empty()) return fail(c, GRANITE_ERR_INVALID, "no blocks");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    int r = alloc_arena(c, c->descs, &c->arena, &c->arena_bytes, c->hblocks);
     if (r) return r;
+    CK(cudaMemsetAsync(c->arena, 0, c->arena_bytes, c->stream), "memset arena");
+    if ((r = build_lists(c))) return r;
+    c->level_time.assign(c->levels.size(), 0.0);
     c->committed = true;
+    return GRANITE_OK;
+}
+
+int granite_ccz4_tag_count(void* h, int level, int var, double threshold, long long* count) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c || !count) return GRANITE_ERR_INVALID;
+    if (!c->committed) return fail(c, GRANITE_ERR_INVALID, "commit before tagging");
+    if (level < 0 || level >= (int)c->levels.size()) return fail(c, GRANITE_ERR_INVALID, "level out of range");
+    if (var != CHI && var != ALPHA) return fail(c, GRANITE_ERR_INVALID, "taggers exist for chi (0) and the lapse (18)");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    const LevelLists& L = c->levels[level];
+    unsigned long long* d = reinterpret_cast<unsigned long long*>(c->s_sum);  // 16 bytes of scratch
+    unsigned long long v = 0;
+    CK(cudaMemsetAsync(d, 0, sizeof(v), c->stream), "memset tag count");
+    CK(launch_tag_count(c->d_blocks, L.d_mtiles, L.nmtiles, var, threshold, d, c->stream), "launch tagger");
+    CK(cudaMemcpyAsync(&v, d, sizeof(v), cudaMemcpyDeviceToHost, c->stream), "read tag count");
+    CK(cudaStreamSynchronize(c->stream), "sync");
+    c->launches += 1;
+    *count = (long long)v;
+    return GRANITE_OK;
+}
+
+int granite_ccz4_regrid_add(void* h, const granite_block_desc* b, int n) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (!c->committed) return fail(c, GRANITE_ERR_INVALID, "commit before regrid");
+    if (n < 0 || (n > 0 && !b)) return fail(c, GRANITE_ERR_INVALID, "bad block list");
+    if (n == 0) return GRANITE_OK;
+    std::vector<granite_block_desc> descs = c->descs;
+    std::vector<int> count(64, 0);
+    for (const auto& d : descs) ++count[d.level];
+    for (int i = 0; i < n; ++i) {
+        int r = check_desc(c, &b[i]);
+        if (r) return r;
+        if (b[i].level < 1 || b[i].level > 31) return fail(c, GRANITE_ERR_INVALID, "regrid adds blocks on levels >= 1");
+        descs.push_back(b[i]);
+    }
+    // every new block needs a coarser level to be filled from (checked in ascending level order)
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b[x].level < b[y].level; });
+    for (int i : order) {
+        if (count[b[i].level - 1] == 0) return fail(c, GRANITE_ERR_INVALID, "regrid: no block on the coarser level");
+        ++count[b[i].level];
+    }
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    CK(drain_profile(c), "profile drain");
+    CK(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    char* arena = nullptr;
+    size_t bytes = 0;
+    std::vector<DevBlock> hb;
+    int r = alloc_arena(c, descs, &arena, &bytes, hb);
+    if (r) return r;
+    // existing blocks keep their state
+    cudaError_t e = cudaMemsetAsync(arena, 0, bytes, c->stream);
+    const size_t nold = c->descs.size();
+    for (size_t i = 0; i < nold && e == cudaSuccess; ++i)
+        e = cudaMemcpyAsync(hb[i].buf[0], c->hblocks[i].buf[0], (size_t)hb[i].stride * NV * sizeof(double),
+                            cudaMemcpyDeviceToDevice, c->stream);
+    DevBlock* d_hb = nullptr;
+    if (e == cudaSuccess) e = upload_vec(hb, &d_hb, c->stream);
+    // new blocks: trilinear prolongation of every cell (ghosts included) from the
+    // coarser level; the reference prolongates from each coarse block in list order
+    // and each writes every fine cell, so the level's last block decides
+    // (amr.cpp:291-293 with prolongate, amr.cpp:484-564)
+    // (new blocks are filled in ascending level order, so a new coarse block is
+    // filled before the finer ones that read it)
+    for (int i : order) {
+        if (e != cudaSuccess) break;
+        const int f = (int)nold + i, L = b[i].level;
+        int last = -1;
+        for (size_t j = 0; j < descs.size(); ++j)
+            if (descs[j].level == L - 1) last = (int)j;
+        XferBox x{};
+        x.dst = f;
+        x.src = last;
+        for (int d = 0; d < 3; ++d) x.n[d] = b[i].ncells[d] + 2 * NG;
+        XferList xl;
+        e = upload_xfer(std::vector<XferBox>{x}, xl, c->stream);
+        if (e == cudaSuccess) e = launch_xfer(XFER_PROLONG, d_hb, xl.d_boxes, xl.d_chunks, xl.nchunks, 0, 0, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        free_xfer(xl);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_hb);
+    if (e != cudaSuccess) {
+        cudaFree(arena);
+        return cuda_fail(c, e, "regrid");
+    }
+    release_lists(c);
+    cudaFree(c->arena);
+    c->arena = arena;
+    c->arena_bytes = bytes;
+    c->descs = std::move(descs);
+    c->hblocks = std::move(hb);
+    c->launches += n;
+    if ((r = build_lists(c))) return r;
+    for (size_t L = c->level_time.size(); L < c->levels.size(); ++L) c->level_time.push_back(c->level_time[L - 1]);
     return GRANITE_OK;
 }
 
@@ -1215,11 +1349,26 @@ int build_ghosts_mode(Ctx* c) {
             CK(upload_vec(sitems, &X[L].d_src_stage, c->stream), "upload stage ghost sources");
             X[L].nsrc_stage = (long long)sitems.size();
         }
-        // restriction into level L-1 from level L
+        // restriction into level L-1 from level L: one launch for the level, or,
+        // where fine interiors overlap (a regrid adds blocks beside the old ones),
+        // one launch per fine block in list order so that the last one holding a
+        // coarse cell's children decides it, as in the reference (amr.cpp:339-341)
         if (L == 0) continue;
-        std::vector<XferBox> res;
+        bool overlap = false;
+        for (size_t p = 0; p < blocks.size() && !overlap; ++p)
+            for (size_t q = p + 1; q < blocks.size() && !overlap; ++q) {
+                bool all = true;
+                for (int d = 0; d < 3 && all; ++d)
+                    all = !meet({G[blocks[p]][d], G[blocks[p]][d] + c->descs[blocks[p]].ncells[d]},
+                                {G[blocks[q]][d], G[blocks[q]][d] + c->descs[blocks[q]].ncells[d]})
+                               .empty();
+                overlap = all;
+            }
+        std::vector<std::vector<XferBox>> waves(overlap ? blocks.size() : 1);
         for (int cb : c->levels[L - 1].blocks)
-            for (int f : blocks) {
+            for (size_t fi = 0; fi < blocks.size(); ++fi) {
+                const int f = blocks[fi];
+                std::vector<XferBox>& res = waves[overlap ? fi : 0];
                 XferBox x{};
                 bool ok = true;
                 for (int d = 0; d < 3; ++d) {
@@ -1240,8 +1389,10 @@ int build_ghosts_mode(Ctx* c) {
                 x.src = f;
                 res.push_back(x);
             }
-        X[L - 1].restrict_.emplace_back();
-        CK(upload_xfer(res, X[L - 1].restrict_.back(), c->stream), "upload restriction boxes");
+        for (const auto& res : waves) {
+            X[L - 1].restrict_.emplace_back();
+            CK(upload_xfer(res, X[L - 1].restrict_.back(), c->stream), "upload restriction boxes");
+        }
     }
     c->xfer_built[GRANITE_AMR_GHOSTS] = true;
     return GRANITE_OK;
@@ -1395,9 +1546,28 @@ cudaError_t stage(Ctx* c, int L, int precision, int in, int out, double a1, doub
     return level_stage(c, ll, precision, a, n);
 }
 
+int ensure_xfer(Ctx* c, int mode) {
+    if (c->xfer_built[mode]) return GRANITE_OK;
+    return mode == GRANITE_AMR_GHOSTS ? build_ghosts_mode(c) : build_reference_mode(c);
+}
+
+// The regrid step of subcycle (amr.cpp:343-349): after level L's step, with
+// step_num = round(current_time / (dt + 1e-15)) a multiple of the interval,
+// the caller's regrid runs on the host (it may add blocks through
+// granite_ccz4_regrid_add, which rebuilds every list; subcycle re-reads them).
+struct RegridHook {
+    int interval;
+    granite_regrid_fn fn;
+    void* user;
+    int status;  // first non-zero status of fn or of a list rebuild
+};
+
 // AMRHierarchy::subcycle(L) with the RK3 step as evolve_func, amr.cpp:303-350.
-cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long long* n) {
+// With a hook, nothing is captured: the level times advance here and the hook
+// runs at the reference's regrid points.
+cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long long* n, RegridHook* hook = nullptr) {
     cudaError_t e;
+    if (hook && (hook->status = ensure_xfer(c, mode))) return cudaErrorInvalidValue;
     const LevelXfer& X = c->xfer[mode][L];
     if (mode == GRANITE_AMR_REFERENCE && L > 0) {  // amr.cpp:313-318 (the fill below repeats it exactly)
         if ((e = xfer(c, XFER_PROLONG, X.prolong, 0, 0))) return e;
@@ -1413,12 +1583,24 @@ cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long lon
     if ((e = fill_level(c, L, 2, false, mode, n))) return e;
     if ((e = stage(c, L, precision, 2, 0, 1.0 / 3.0, 2.0 / 3.0, (2.0 / 3.0) * dt, 1, n))) return e;
     if ((e = fill_level(c, L, 0, true, mode, n))) return e;  // amr.cpp:329
+    if (hook) c->level_time[L] += dt;                         // amr.cpp:326
     if (L + 1 < (int)c->levels.size()) {
         for (int r = 0; r < 2; ++r)
-            if ((e = subcycle(c, L + 1, dt / 2.0, precision, mode, n))) return e;  // amr.cpp:334-336, :393-397
-        for (const XferList& rl : X.restrict_) {                                   // amr.cpp:339-341
+            if ((e = subcycle(c, L + 1, dt / 2.0, precision, mode, n, hook))) return e;  // amr.cpp:334-336, :393-397
+        if (hook && (hook->status = ensure_xfer(c, mode))) return cudaErrorInvalidValue;  // a regrid rebuilt them
+        for (const XferList& rl : c->xfer[mode][L].restrict_) {                            // amr.cpp:339-341
             if ((e = xfer(c, XFER_RESTRICT, rl, 0, 0))) return e;
             ++*n;
+        }
+    }
+    if (hook && hook->interval > 0) {
+        const long long step_num = std::llround(c->level_time[L] / (dt + 1e-15));
+        if (step_num % hook->interval == 0) {
+            if ((e = cudaStreamSynchronize(c->stream))) return e;
+            if ((hook->status = hook->fn(hook->user, L, step_num))) {
+                fail(c, hook->status, "regrid callback returned " + std::to_string(hook->status));
+                return cudaErrorInvalidValue;
+            }
         }
     }
     return cudaSuccess;
@@ -1426,9 +1608,7 @@ cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long lon
 
 }  // namespace
 
-int granite_ccz4_hierarchy_step(void* h, double dt_coarse, int precision, int amr_mode) {
-    Ctx* c = static_cast<Ctx*>(h);
-    if (!c) return GRANITE_ERR_INVALID;
+static int check_hierarchy_step(Ctx* c, double dt_coarse, int precision, int amr_mode) {
     if (!c->committed) return fail(c, GRANITE_ERR_INVALID, "commit before stepping");
     int r = check_precision(c, precision);
     if (r) return r;
@@ -1438,15 +1618,29 @@ int granite_ccz4_hierarchy_step(void* h, double dt_coarse, int precision, int am
     for (auto& L : c->levels)
         if (L.blocks.empty()) return fail(c, GRANITE_ERR_INVALID, "hierarchy levels must be contiguous from 0");
     CK(cudaSetDevice(c->device), "cudaSetDevice");
-    if (!c->xfer_built[amr_mode]) {
-        r = amr_mode == GRANITE_AMR_GHOSTS ? build_ghosts_mode(c) : build_reference_mode(c);
-        if (r) return r;
-    }
+    return ensure_xfer(c, amr_mode);
+}
+
+// Level times of one coarse step without the hook: level L takes 2^L steps of
+// dt / 2^L (the same additions the hook path makes).
+static void advance_level_times(Ctx* c, double dt_coarse) {
+    double dt = dt_coarse;
+    for (size_t L = 0; L < c->level_time.size(); ++L, dt /= 2.0)
+        for (long long s = 0; s < (1LL << L); ++s) c->level_time[L] += dt;
+}
+
+int granite_ccz4_hierarchy_step(void* h, double dt_coarse, int precision, int amr_mode) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    int r = check_hierarchy_step(c, dt_coarse, precision, amr_mode);
+    if (r) return r;
+    for (size_t L = 0; L < c->level_ghosts_valid.size(); ++L) c->level_ghosts_valid[L] = false;
     if (c->profiling || !c->batched) {
         long long n = 0;
         cudaError_t e = subcycle(c, 0, dt_coarse, precision, amr_mode, &n);
         if (e != cudaSuccess) return cuda_fail(c, e, "hierarchy step");
         c->launches += n;
+        advance_level_times(c, dt_coarse);
         return GRANITE_OK;
     }
     unsigned long long dtbits;
@@ -1470,7 +1664,34 @@ int granite_ccz4_hierarchy_step(void* h, double dt_coarse, int precision, int am
     }
     CK(cudaGraphLaunch(it->second.exec, c->stream), "graph launch");
     c->launches += it->second.launches;
+    advance_level_times(c, dt_coarse);
+    return GRANITE_OK;
+}
+
+int granite_ccz4_hierarchy_step_regrid(void* h, double dt_coarse, int precision, int amr_mode, int regrid_interval,
+                                       granite_regrid_fn fn, void* user) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (regrid_interval < 0 || (regrid_interval > 0 && !fn))
+        return fail(c, GRANITE_ERR_INVALID, "regrid_interval >= 0, with a callback when > 0");
+    int r = check_hierarchy_step(c, dt_coarse, precision, amr_mode);
+    if (r) return r;
     for (size_t L = 0; L < c->level_ghosts_valid.size(); ++L) c->level_ghosts_valid[L] = false;
+    RegridHook hook{regrid_interval, fn, user, 0};
+    long long n = 0;
+    cudaError_t e = subcycle(c, 0, dt_coarse, precision, amr_mode, &n, &hook);
+    c->launches += n;
+    if (hook.status) return hook.status;  // the message is the callback's or the rebuild's
+    if (e != cudaSuccess) return cuda_fail(c, e, "hierarchy step with regrid");
+    return GRANITE_OK;
+}
+
+int granite_ccz4_level_time(void* h, int level, double* t) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c || !t) return GRANITE_ERR_INVALID;
+    if (!c->committed) return fail(c, GRANITE_ERR_INVALID, "commit first");
+    if (level < 0 || level >= (int)c->level_time.size()) return fail(c, GRANITE_ERR_INVALID, "bad level");
+    *t = c->level_time[level];
     return GRANITE_OK;
 }
 

@@ -262,6 +262,47 @@ cudaError_t launch_sum_partials(const double* partials, int n, double* out, cuda
 }
 
 // ---------------------------------------------------------------------------
+// Regrid taggers (amr.cpp:653-731): a cell is tagged when |grad f| / (|f| + 1e-30)
+// exceeds the threshold, grad f from centred differences (f[+1] - f[-1]) / (2 dx)
+// summed as squares over x, y, z, in the reference's order with separately
+// rounded operations (so the decision at the threshold is the reference's).
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void __launch_bounds__(CT_X* CT_Y)
+    tag_count_kernel(const DevBlock* __restrict__ blocks, const Tile* __restrict__ tiles, int var, double threshold,
+                     unsigned long long* count) {
+    const Tile t = tiles[blockIdx.x];
+    const DevBlock& B = blocks[t.block];
+    const int w = t.w > 0 ? t.w : CT_X;
+    const int tid = threadIdx.x + CT_X * threadIdx.y;
+    const int i = t.i0 + tid % w, j = t.j0 + tid / w, k = t.k0;
+    bool tag = false;
+    if (i < B.n[0] && j < B.n[1] && k < B.n[2]) {
+        const double* f = B.buf[0] + (long long)var * B.stride + cell_index(B, i + NG, j + NG, k + NG);
+        const long long off[3] = {1, B.tx, (long long)B.tx * B.ty};
+        double grad2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double df = __ddiv_rn(__dsub_rn(__ldg(f + off[d]), __ldg(f - off[d])), __dmul_rn(2.0, B.dx[d]));
+            grad2 = __dadd_rn(grad2, __dmul_rn(df, df));
+        }
+        tag = __ddiv_rn(__dsqrt_rn(grad2), __dadd_rn(fabs(__ldg(f)), 1e-30)) > threshold;
+    }
+    const unsigned n = __popc(__ballot_sync(0xffffffffu, tag));
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(count, (unsigned long long)n);
+}
+
+}  // namespace
+
+cudaError_t launch_tag_count(const DevBlock* blocks, const Tile* tiles, int ntiles, int var, double threshold,
+                             unsigned long long* count, cudaStream_t stream) {
+    if (ntiles <= 0) return cudaSuccess;
+    tag_count_kernel<<<ntiles, dim3(CT_X, CT_Y, 1), 0, stream>>>(blocks, tiles, var, threshold, count);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Constraint norms without any allocation (granite_ccz4_constraint_norms_noalloc)
 //
 // For callers that cannot allocate device memory themselves (see the header):

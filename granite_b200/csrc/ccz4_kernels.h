@@ -123,6 +123,11 @@ cudaError_t launch_ghost_sources(const DevBlock* blocks, const GhostSrc* items, 
 cudaError_t launch_constraints(const DevBlock* blocks, const Tile* tiles, int ntiles, int sel,
                                double* ham, double* mom, double* partials, cudaStream_t stream);
 
+// Regrid tagger (amr.cpp:653-731) over the interior cells of slot 0 of the
+// listed tiles (32x4x1 monitor shape): adds the number of tagged cells to *count.
+cudaError_t launch_tag_count(const DevBlock* blocks, const Tile* tiles, int ntiles, int var, double threshold,
+                             unsigned long long* count, cudaStream_t stream);
+
 // Deterministic fixed-order sum of n partial pairs into out[2].
 cudaError_t launch_sum_partials(const double* partials, int n, double* out, cudaStream_t stream);
 

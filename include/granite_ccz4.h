@@ -147,6 +147,26 @@ GRANITE_API int granite_ccz4_compute_rhs_device(void* ctx, const granite_block_d
 
 GRANITE_API int granite_ccz4_add_block(void* ctx, const granite_block_desc* b, int* block_index);
 GRANITE_API int granite_ccz4_commit(void* ctx);
+
+/* Replaces the block creation of AMRHierarchy::regrid (amr.cpp:80-301), which
+ * only ever adds blocks: appends n blocks (levels >= 1) to a committed
+ * hierarchy. Existing blocks keep their state and their indices; each new
+ * block gets indices num_blocks() .. in the order given and is filled in every
+ * cell (ghosts included) by trilinear prolongation from its coarser level as
+ * the reference's regrid does (amr.cpp:291-293: each coarse block in list order
+ * overwrites every fine cell, so the level's last block decides). New blocks
+ * are filled in ascending level order. The arena is reallocated (a device-side
+ * copy of the states), work-lists and tensor maps are rebuilt, cached step
+ * graphs are dropped. Which boxes to add (tracking spheres, taggers) is the
+ * caller's decision; granite_ccz4_tag_count gives the reference taggers' cell
+ * counts on the device. */
+GRANITE_API int granite_ccz4_regrid_add(void* ctx, const granite_block_desc* blocks, int n);
+/* Replaces gradientChiTagger / gradientLapseTagger (amr.cpp:653-731) as the
+ * regrid uses them: the number of interior cells of `level` (state slot 0)
+ * with |grad f| / (|f| + 1e-30) > threshold, f = chi (var 0) or the lapse
+ * (var 18), evaluated in the reference's order. Blocks until the count is on
+ * the host. */
+GRANITE_API int granite_ccz4_tag_count(void* ctx, int level, int var, double threshold, long long* count);
 GRANITE_API int granite_ccz4_num_blocks(const void* ctx);
 /* bytes of device memory held by the arena after commit */
 GRANITE_API int granite_ccz4_arena_bytes(const void* ctx, size_t* bytes);
@@ -168,6 +188,26 @@ GRANITE_API int granite_ccz4_rk3_step(void* ctx, int level, double dt, int preci
  * (main.cpp:1142-1177): level l advances by dt_coarse / 2^l, twice per parent
  * step, followed by restriction to the parent. amr_mode: GRANITE_AMR_*. */
 GRANITE_API int granite_ccz4_hierarchy_step(void* ctx, double dt_coarse, int precision, int amr_mode);
+
+/* The regrid point of AMRHierarchy::subcycle (amr.cpp:343-349): called after
+ * level `level`'s step (its restriction from the finer level included) when
+ * step_num = round(current_time / (dt + 1e-15)) is a multiple of the regrid
+ * interval. It runs on the calling thread with the stream synchronised and may
+ * call granite_ccz4_tag_count and granite_ccz4_regrid_add on the same context;
+ * a non-zero return stops the step and is returned by it. */
+typedef int (*granite_regrid_fn)(void* user, int level, long long step_num);
+
+/* granite_ccz4_hierarchy_step with the reference's in-step regrid
+ * (AMRHierarchy::subcycle with regrid_interval > 0, amr.cpp:303-350): `fn`
+ * runs at every regrid point of every level, in the reference's order, and the
+ * levels it creates join the remaining substeps of the coarse step. Not
+ * captured in a graph. regrid_interval = 0 never calls fn. */
+GRANITE_API int granite_ccz4_hierarchy_step_regrid(void* ctx, double dt_coarse, int precision, int amr_mode,
+                                                   int regrid_interval, granite_regrid_fn fn, void* user);
+
+/* Level::current_time (amr.hpp:108-113): the sum of the level's step sizes so
+ * far; a level created by a regrid starts at its parent's time. */
+GRANITE_API int granite_ccz4_level_time(void* ctx, int level, double* t);
 
 /* ---- diagnostics ----------------------------------------------------------- */
 

@@ -294,6 +294,12 @@ class Reference:
         self.lib.ref_init_brill_lindquist(*self._g(g), _p(u), C.c_int(len(m)), _p(m), _p(pos))
         return u
 
+    def tag_count(self, g: Geom, u, var: int, threshold: float) -> int:
+        """gradientChiTagger / gradientLapseTagger (amr.cpp:653-731) over the interior."""
+        self.lib.ref_tag_count.restype = C.c_longlong
+        return int(self.lib.ref_tag_count(*self._g(g), _p(np.ascontiguousarray(u, dtype=np.float64)),
+                                          C.c_int(var), C.c_double(threshold)))
+
     def bl_conformal_factor(self, masses, positions, x, y, z):
         m = np.ascontiguousarray(masses, dtype=np.float64)
         pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)

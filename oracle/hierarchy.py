@@ -2,7 +2,13 @@
 
 * ``RefHierarchy``: the compiled reference's own AMRHierarchy (tracking
   spheres, subcycle; amr.cpp:34-350) behind oracle/ref_shim.cpp, with the
-  restated spacetime RK3 step as evolve_func. Regridding is off.
+  restated spacetime RK3 step as evolve_func. Regridding inside the step is
+  off; ``regrid`` runs AMRHierarchy::regrid on demand.
+* ``tag_count``: the gradient taggers (amr.cpp:653-731) restated in numpy.
+* In-step regrid (amr.cpp:343-349) for both drivers: ``HierarchyOracle`` keeps
+  each level's current_time and calls ``regrid_hook(self, level)`` at the
+  reference's regrid points (``add_blocks`` prolongates the new blocks);
+  ``RefHierarchy(..., regrid_interval=k)`` runs the reference's own.
 * ``HierarchyOracle``: a restatement of the same Berger-Oliger step over the
   oracle's C pieces, in two modes:
     - "reference": amr.cpp literally (prolongation from every coarse block into
@@ -21,6 +27,7 @@
 from __future__ import annotations
 
 import ctypes as C
+import math
 
 import numpy as np
 
@@ -30,7 +37,7 @@ NG = 4
 
 
 class RefHierarchy:
-    def __init__(self, ref: Reference, n, lo, hi, spheres, max_levels=15):
+    def __init__(self, ref: Reference, n, lo, hi, spheres, max_levels=15, regrid_interval=0):
         self.ref = ref
         lib = ref.lib
         lib.ref_hier_create.restype = C.c_void_p
@@ -45,8 +52,16 @@ class RefHierarchy:
         cen = np.ascontiguousarray([s[0] for s in spheres], dtype=np.float64).reshape(-1, 3)
         rad = np.ascontiguousarray([s[1] for s in spheres], dtype=np.float64)
         mlv = (C.c_int * len(spheres))(*[int(s[2]) for s in spheres])
+        lib.ref_hier_update_spheres.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
+        lib.ref_hier_regrid.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double]
+        lib.ref_hier_set_tagger.argtypes = [C.c_void_p, C.c_int, C.c_double]
         self.h = lib.ref_hier_create((C.c_int * 3)(*n), (C.c_double * 3)(*lo), (C.c_double * 3)(*hi),
-                                     C.c_int(max_levels), C.c_int(len(spheres)), _p(cen), _p(rad), mlv)
+                                     C.c_int(max_levels), C.c_int(len(spheres)), _p(cen), _p(rad), mlv,
+                                     C.c_int(regrid_interval))
+        self._read_layout()
+
+    def _read_layout(self):
+        lib = self.ref.lib
         self.geoms, self.levels = [], []
         for i in range(lib.ref_hier_num_blocks(self.h)):
             lv = C.c_int()
@@ -57,6 +72,18 @@ class RefHierarchy:
             self.geoms.append(Geom(tuple(nn), tuple(blo), tuple(bhi)))
             self.levels.append(lv.value)
 
+    def update_spheres(self, centers):
+        """AMRHierarchy::updateTrackingSpheres (amr.cpp:632-636)."""
+        c = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 3)
+        self.ref.lib.ref_hier_update_spheres(self.h, C.c_int(len(c)), _p(c))
+
+    def regrid(self, level: int, var: int = -1, threshold: float = 0.0):
+        """AMRHierarchy::regrid (amr.cpp:80-301) with the chi (var 0) or lapse (var 18)
+        gradient tagger, or one that never tags; the block list is re-read (level
+        order, then creation order)."""
+        self.ref.lib.ref_hier_regrid(self.h, C.c_int(level), C.c_int(var), C.c_double(threshold))
+        self._read_layout()
+
     def get(self, i):
         u = self.geoms[i].zeros()
         self.ref.lib.ref_hier_get(self.h, i, _p(u))
@@ -66,15 +93,41 @@ class RefHierarchy:
         u = np.ascontiguousarray(u, dtype=np.float64)
         self.ref.lib.ref_hier_set(self.h, i, _p(u))
 
+    def set_tagger(self, var: int, threshold: float):
+        """The tagger subcycle's regrids use (var 0 chi, 18 lapse, other: none)."""
+        self.ref.lib.ref_hier_set_tagger(self.h, C.c_int(var), C.c_double(threshold))
+
     def step(self, p: Params, dt: float, nsteps: int = 1):
         p6 = p.as6()
         self.ref.lib.ref_hier_step(self.h, _p(p6), C.c_double(dt), C.c_int(nsteps))
+        self._read_layout()
 
     def __del__(self):
         try:
             self.ref.lib.ref_hier_destroy(self.h)
         except Exception:
             pass
+
+
+def tag_count(g: Geom, u, var: int, threshold: float) -> int:
+    """Interior cells of one block tagged by gradientChiTagger (var 0) or
+    gradientLapseTagger (var 18), amr.cpp:653-731: |grad f| / (|f| + 1e-30) >
+    threshold with grad f from centred differences (f[+1] - f[-1]) / (2 dx),
+    squares summed x, y, z from 0.0 (separately rounded, no contraction)."""
+    a = np.asarray(u, dtype=np.float64)[var]
+    nx, ny, nz = g.n
+    s = slice(NG, NG + nz), slice(NG, NG + ny), slice(NG, NG + nx)
+
+    def shifted(axis, o):
+        sl = list(s)
+        sl[2 - axis] = slice(NG + o, NG + o + g.n[axis])
+        return a[tuple(sl)]
+
+    grad2 = np.zeros((nz, ny, nx))
+    for d in range(3):
+        df = (shifted(d, 1) - shifted(d, -1)) / (2.0 * g.dx[d])
+        grad2 = grad2 + df * df
+    return int(np.count_nonzero(np.sqrt(grad2) / (np.abs(a[s]) + 1e-30) > threshold))
 
 
 def _centres(g: Geom):
@@ -104,6 +157,36 @@ class HierarchyOracle:
         self.s1 = [g.zeros() for g in self.geoms]
         self.s2 = [g.zeros() for g in self.geoms]
         self.rhs = [g.zeros() for g in self.geoms]
+        self._ghost_plan = None
+        # in-step regrid (amr.cpp:343-349): Level::current_time per level and the
+        # hook called as hook(self, level) at the regrid points
+        self.time = [0.0] * self.nlev
+        self.regrid_interval = 0
+        self.regrid_hook = None
+
+    def add_blocks(self, geoms, levels):
+        """New blocks after the existing ones, each prolongated in all its cells
+        from every block of the coarser level in list order (the regrid's
+        amr.cpp:291-293 with prolongate, amr.cpp:484-564); a new level starts
+        at its parent's time (amr.cpp:137-143)."""
+        lib = self.o.lib
+        for g, L in zip(geoms, levels):
+            assert 1 <= L <= self.nlev
+            i = len(self.geoms)
+            self.geoms.append(g)
+            self.levels.append(L)
+            if L == self.nlev:
+                self.nlev += 1
+                self.by_level.append([])
+                self.time.append(self.time[L - 1])
+            u = g.zeros()
+            for c in self.by_level[L - 1]:
+                lib.orc_prolongate(C.byref(_cg(self.geoms[c])), _p(self.u[c]), C.byref(_cg(g)), _p(u), C.c_int(0))
+            self.by_level[L].append(i)
+            self.u.append(u)
+            self.s1.append(g.zeros())
+            self.s2.append(g.zeros())
+            self.rhs.append(g.zeros())
         self._ghost_plan = None
 
     # -- reference mode ----------------------------------------------------
@@ -231,6 +314,8 @@ class HierarchyOracle:
 
     def _subcycle(self, L, dt, p, mode):
         lib = self.o.lib
+        if mode == "ghosts" and self._ghost_plan is None:
+            self._plan()
         if mode == "reference":
             if L > 0:
                 for f in self.by_level[L]:
@@ -241,6 +326,7 @@ class HierarchyOracle:
         else:
             self._ghost_fill(L, self.u, level_fill=True)
         self._evolve(L, dt, p, mode)
+        self.time[L] += dt
         if mode == "reference":
             self._ref_fill(L, self.u)
         else:
@@ -248,6 +334,8 @@ class HierarchyOracle:
         if L + 1 < self.nlev:
             for _ in range(2):
                 self._subcycle(L + 1, dt / 2.0, p, mode)
+            if mode == "ghosts" and self._ghost_plan is None:
+                self._plan()
             if mode == "reference":
                 for f in self.by_level[L + 1]:
                     for c in self.by_level[L]:
@@ -255,6 +343,13 @@ class HierarchyOracle:
                                          C.byref(_cg(self.geoms[c])), _p(self.u[c]))
             else:
                 self._ghost_restrict(L)
+        if self.regrid_interval > 0 and self.regrid_hook is not None:
+            q = self.time[L] / (dt + 1e-15)
+            step_num = math.trunc(q)
+            if abs(q - step_num) >= 0.5:  # std::round: halves away from zero
+                step_num += 1 if q > 0 else -1
+            if step_num % self.regrid_interval == 0:
+                self.regrid_hook(self, L)
 
     def step(self, p: Params, dt_coarse: float, mode: str = "reference", nsteps: int = 1):
         if mode == "ghosts" and self._ghost_plan is None:

@@ -321,18 +321,32 @@ void ref_rk3_steps(const double* p6, const int* n, int ng, const double* lo, con
 // spheres (amr.cpp:34-301), stepped by AMRHierarchy::subcycle (amr.cpp:303-350)
 // with the spacetime part of TimeIntegrator::sspRK3Step as evolve_func
 // (main.cpp:86-690, the restated lambdas of ccz4_oracle.c around the reference
-// computeRHSVacuum). Regridding is off (regrid_interval = 0).
+// computeRHSVacuum). Regridding inside subcycle follows the regrid_interval
+// given at creation (0 = off); ref_hier_regrid runs AMRHierarchy::regrid on
+// demand.
 // ---------------------------------------------------------------------------
 struct RefHier {
     std::unique_ptr<amr::AMRHierarchy> h;
     std::vector<GridBlock*> blocks;  // level order, then creation order
+    int tag_var = -1;                // tagger of the in-step regrid (see tagger_of)
+    double tag_threshold = 0.0;
 };
 
+namespace {
+void relist(RefHier* r) {
+    r->blocks.clear();
+    for (int L = 0; L < r->h->numLevels(); ++L)
+        for (GridBlock* b : r->h->getLevel(L)) r->blocks.push_back(b);
+}
+} // namespace
+
+// regrid_interval > 0 turns on the regrid inside subcycle (amr.cpp:343-349),
+// with the tagger of ref_hier_set_tagger (none by default).
 void* ref_hier_create(const int* n, const double* lo, const double* hi, int max_levels, int nspheres,
-                      const double* centers, const double* radii, const int* min_levels) {
+                      const double* centers, const double* radii, const int* min_levels, int regrid_interval) {
     amr::AMRParams ap;
     ap.max_levels = max_levels;
-    ap.regrid_interval = 0;
+    ap.regrid_interval = regrid_interval;
     SimulationParams sp;
     for (int d = 0; d < 3; ++d) {
         sp.ncells[d] = n[d];
@@ -347,8 +361,7 @@ void* ref_hier_create(const int* n, const double* lo, const double* hi, int max_
     std::cout.setstate(std::ios_base::failbit);
     r->h->initialize([](const GridBlock&, int, int, int) { return false; });
     std::cout.clear();
-    for (int L = 0; L < r->h->numLevels(); ++L)
-        for (GridBlock* b : r->h->getLevel(L)) r->blocks.push_back(b);
+    relist(r);
     return r;
 }
 
@@ -374,6 +387,18 @@ void ref_hier_set(void* hp, int i, const double* u) {
     std::memcpy(b->flatBuffer(), u, nbytes(*b));
 }
 
+namespace {
+amr::TaggingFunction tagger_of(int var, double threshold);
+} // namespace
+
+void ref_hier_set_tagger(void* hp, int var, double threshold) {
+    RefHier* r = static_cast<RefHier*>(hp);
+    r->tag_var = var;
+    r->tag_threshold = threshold;
+}
+
+// nsteps coarse steps of AMRHierarchy::subcycle(0) (regrids included when the
+// interval is set); the block list is re-read afterwards.
 void ref_hier_step(void* hp, const double* p6, double dt_coarse, int nsteps) {
     RefHier* r = static_cast<RefHier*>(hp);
     spacetime::CCZ4Evolution ev(params(p6));
@@ -411,10 +436,54 @@ void ref_hier_step(void* hp, const double* p6, double dt_coarse, int nsteps) {
         }
     };
     r->h->setLevelDt(0, dt_coarse);
+    const amr::TaggingFunction tagger = tagger_of(r->tag_var, r->tag_threshold);
     std::cout.setstate(std::ios_base::failbit);
-    for (int s = 0; s < nsteps; ++s)
-        r->h->subcycle(0, evolve, [](const GridBlock&, int, int, int) { return false; });
+    for (int s = 0; s < nsteps; ++s) r->h->subcycle(0, evolve, tagger);
     std::cout.clear();
+    relist(r);
+}
+
+// AMRHierarchy::updateTrackingSpheres (amr.cpp:632-636): new centres of the
+// first n tracking spheres.
+void ref_hier_update_spheres(void* hp, int n, const double* centers) {
+    std::vector<std::array<Real, DIM>> c(n);
+    for (int s = 0; s < n; ++s) c[s] = {centers[3 * s], centers[3 * s + 1], centers[3 * s + 2]};
+    static_cast<RefHier*>(hp)->h->updateTrackingSpheres(c);
+}
+
+namespace {
+amr::TaggingFunction tagger_of(int var, double threshold) {
+    if (var == static_cast<int>(SpacetimeVar::CHI)) return amr::gradientChiTagger(threshold);
+    if (var == static_cast<int>(SpacetimeVar::LAPSE)) return amr::gradientLapseTagger(threshold);
+    return [](const GridBlock&, int, int, int) { return false; };
+}
+} // namespace
+
+// AMRHierarchy::regrid(level, tagger) (amr.cpp:80-301) with gradientChiTagger
+// (var 0), gradientLapseTagger (var 18) or a tagger that never tags (any other
+// var). The block list is rebuilt (level order, then creation order); returns
+// its length.
+int ref_hier_regrid(void* hp, int level, int var, double threshold) {
+    RefHier* r = static_cast<RefHier*>(hp);
+    std::cout.setstate(std::ios_base::failbit);  // regrid prints one line per new block
+    r->h->regrid(level, tagger_of(var, threshold));
+    std::cout.clear();
+    relist(r);
+    return (int)r->blocks.size();
+}
+
+// gradientChiTagger / gradientLapseTagger (amr.cpp:653-731) over the interior
+// cells of one block: the number of tagged cells.
+long long ref_tag_count(const int* n, int ng, const double* lo, const double* hi, const double* u, int var,
+                        double threshold) {
+    auto b = block(geo(n, ng, lo, hi));
+    std::memcpy(b->flatBuffer(), u, nbytes(*b));
+    const amr::TaggingFunction t = tagger_of(var, threshold);
+    long long count = 0;
+    for (int k = b->istart(2); k < b->iend(2); ++k)
+        for (int j = b->istart(1); j < b->iend(1); ++j)
+            for (int i = b->istart(0); i < b->iend(0); ++i) count += t(*b, i, j, k) ? 1 : 0;
+    return count;
 }
 
 void ref_hier_destroy(void* hp) { delete static_cast<RefHier*>(hp); }
