@@ -112,6 +112,11 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_measure_fma_rate.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
     lib.granite_ccz4_get_fp64_chi_threshold.argtypes = [vp, C.POINTER(C.c_double)]
     lib.granite_ccz4_regrid_add.argtypes = [vp, C.POINTER(_BlockDesc), C.c_int]
+    lib.granite_ccz4_matter_sources_host.argtypes = [vp, C.POINTER(_BlockDesc), dp, dp, dp, dp, dp]
+    lib.granite_ccz4_matter_sources_device.argtypes = [vp, C.POINTER(_BlockDesc), vp, vp, vp, vp, vp, vp]
+    lib.granite_ccz4_enable_matter.argtypes = [vp, C.c_int]
+    lib.granite_ccz4_upload_primitives.argtypes = [vp, C.c_int, dp]
+    lib.granite_ccz4_set_primitives_device.argtypes = [vp, C.c_int, vp]
     lib.granite_ccz4_hierarchy_step_regrid.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.c_int, _REGRID_FN, vp]
     lib.granite_ccz4_level_time.argtypes = [vp, C.c_int, dp]
     lib.granite_ccz4_tag_count.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_longlong)]
@@ -334,6 +339,35 @@ class CCZ4Evolution:
         return ham, mom
 
 
+NUM_PRIMITIVE_VARS = 11  # PrimitiveVar (types.hpp:149-162)
+
+
+class MatterSources:
+    """GRMHDEvolution::computeMatterSources (grmhd.hpp:333-338, grmhd.cpp:1034-1103)
+    on the GPU: the ADM matter sources of the CCZ4 RHS from a primitive
+    GridBlock (11 fields in PrimitiveVar order). Only this coupling of the
+    GRMHD module is provided; its own evolution is not."""
+
+    def __init__(self):
+        self.ctx = _Context(CCZ4Params())
+
+    def computeMatterSources(self, spacetime_grid: GridBlock, prim_grid: GridBlock, rho_src, Si, Sij,
+                             S_trace):
+        """Fills the interior cells of rho_src[N], Si[N,3], Sij[N,6], S_trace[N]
+        (float64 C-contiguous arrays, N = totalSize; other cells keep their values)."""
+        if prim_grid.num_vars != NUM_PRIMITIVE_VARS or prim_grid.ncells != spacetime_grid.ncells:
+            raise ValueError("prim_grid: 11 primitive fields on the spacetime grid's cells")
+        N = spacetime_grid.totalSize()
+        arrs = [_f64(a) for a in (rho_src, Si, Sij, S_trace)]
+        if [a.size for a in arrs] != [N, 3 * N, 6 * N, N]:
+            raise ValueError("matter arrays must hold N, 3N, 6N and N values")
+        self.ctx.check(self.ctx.lib.granite_ccz4_matter_sources_host(
+            self.ctx.h, C.byref(spacetime_grid.desc()), _dp(prim_grid.array), *[_dp(a) for a in arrs]))
+
+    def close(self):
+        self.ctx.close()
+
+
 # ---------------------------------------------------------------------------
 # Resident hierarchy + RK3 driver (main.cpp TimeIntegrator, amr.cpp subcycle)
 # ---------------------------------------------------------------------------
@@ -368,6 +402,17 @@ class Evolver:
         v = C.c_int()
         self.ctx.check(self.ctx.lib.granite_ccz4_get_kernel_variant(self.ctx.h, C.byref(v)))
         return v.value
+
+    def enable_matter(self, on: bool = True):
+        """Before commit: every block gets matter sources (zero = vacuum) that the
+        RHS of every step reads (the non-vacuum applyRHS, main.cpp:296-302)."""
+        self.ctx.check(self.ctx.lib.granite_ccz4_enable_matter(self.ctx.h, int(bool(on))))
+
+    def upload_primitives(self, idx: int, prim):
+        """Block idx's matter sources from its primitives (11 x totalSize float64,
+        PrimitiveVar order) by computeMatterSources on the device; they hold
+        until the next upload."""
+        self.ctx.check(self.ctx.lib.granite_ccz4_upload_primitives(self.ctx.h, idx, _dp(_f64(prim))))
 
     def add_block(self, b: GridBlock) -> int:
         idx = C.c_int()

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <climits>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -146,6 +147,9 @@ struct Ctx {
     int device = 0;
     int variant = VARIANT_TMA;     // stage-kernel variant (granite_ccz4_set_kernel_variant)
     bool batched = true;           // one launch per level and stage + CUDA graphs (else per block, eager)
+    bool matter = false;           // resident matter sources (granite_ccz4_enable_matter)
+    double* d_matter = nullptr;    // rho[N] | Si[N][3] | Sij[N][6] | S[N], N = matter_cells (all blocks)
+    long long matter_cells = 0;
     double fp64_chi = 0.0;         // MIXED: tiles with a point of chi below this run the FP64 algebra
     cudaStream_t stream = nullptr;
     std::string err;
@@ -299,6 +303,13 @@ StageArgs base_args(const Ctx* c) {
     a.nonfinite = c->d_nonfinite;
     a.tmaps = c->d_tmaps;
     a.errflag = c->d_errflag;
+    if (c->d_matter) {  // resident matter: the context-wide arrays, block b at cell offset moff
+        const long long N = c->matter_cells;
+        a.rho = c->d_matter;
+        a.Si = c->d_matter + N;
+        a.Sij = c->d_matter + 4 * N;
+        a.S = c->d_matter + 10 * N;
+    }
     return a;
 }
 
@@ -312,7 +323,7 @@ int ensure_scratch(Ctx* c, size_t cells, int ntiles) {
         c->s_cells = 0;
         CK(cudaMalloc(&c->s_u, cells * NV * sizeof(double)), "cudaMalloc(scratch u)");
         CK(cudaMalloc(&c->s_rhs, cells * NV * sizeof(double)), "cudaMalloc(scratch rhs)");
-        CK(cudaMalloc(&c->s_mat, cells * 11 * sizeof(double)), "cudaMalloc(scratch matter)");
+        CK(cudaMalloc(&c->s_mat, cells * NPRIM * sizeof(double)), "cudaMalloc(scratch matter)");
         c->s_cells = cells;
     }
     if (ntiles > c->s_tiles_cap) {
@@ -555,6 +566,7 @@ int granite_ccz4_destroy(void* h) {
     cudaFree(c->s_u);
     cudaFree(c->s_rhs);
     cudaFree(c->s_mat);
+    cudaFree(c->d_matter);
     cudaFree(c->s_desc);
     cudaFree(c->s_tiles);
     cudaFree(c->s_partials);
@@ -642,6 +654,49 @@ int granite_ccz4_compute_rhs_device(void* h, const granite_block_desc* b, const 
     a.tmaps = c->s_tmap;  // block 0, slot 0
     CK(launch_stage(variant, precision, EPI_STORE, c->s_desc, c->s_tiles, nt, a, s), "launch RHS");
     c->launches += 1;
+    return GRANITE_OK;
+}
+
+int granite_ccz4_matter_sources_device(void* h, const granite_block_desc* b, const double* prim_dev, double* rho_dev,
+                                      double* Si_dev, double* Sij_dev, double* S_dev, void* stream) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    int r = check_desc(c, b);
+    if (r) return r;
+    if (!prim_dev || !rho_dev || !Si_dev || !Sij_dev || !S_dev) return fail(c, GRANITE_ERR_INVALID, "null buffer");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    const MatterOut o{rho_dev, Si_dev, Sij_dev, S_dev, 3, 1, 6, 1};
+    CK(launch_matter_sources(make_devblock(*b, c->p.ko_sigma), prim_dev, o,
+                             stream ? static_cast<cudaStream_t>(stream) : c->stream),
+       "launch matter sources");
+    c->launches += 1;
+    return GRANITE_OK;
+}
+
+int granite_ccz4_matter_sources_host(void* h, const granite_block_desc* b, const double* prim, double* rho,
+                                    double* Si, double* Sij, double* S) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    int r = check_desc(c, b);
+    if (r) return r;
+    if (!prim || !rho || !Si || !Sij || !S) return fail(c, GRANITE_ERR_INVALID, "null host buffer");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    const size_t N = (size_t)cells_of(*b);
+    if ((r = ensure_scratch(c, N, 1))) return r;
+    cudaStream_t s = c->stream;
+    double* m = c->s_mat;  // rho | Si (3N) | Sij (6N) | S: the caller's arrays, in/out
+    CK(cudaMemcpyAsync(c->s_u, prim, N * NPRIM * sizeof(double), cudaMemcpyHostToDevice, s), "H2D prim");
+    CK(cudaMemcpyAsync(m, rho, N * sizeof(double), cudaMemcpyHostToDevice, s), "H2D rho");
+    CK(cudaMemcpyAsync(m + N, Si, 3 * N * sizeof(double), cudaMemcpyHostToDevice, s), "H2D Si");
+    CK(cudaMemcpyAsync(m + 4 * N, Sij, 6 * N * sizeof(double), cudaMemcpyHostToDevice, s), "H2D Sij");
+    CK(cudaMemcpyAsync(m + 10 * N, S, N * sizeof(double), cudaMemcpyHostToDevice, s), "H2D S");
+    r = granite_ccz4_matter_sources_device(c, b, c->s_u, m, m + N, m + 4 * N, m + 10 * N, s);
+    if (r) return r;
+    CK(cudaMemcpyAsync(rho, m, N * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H rho");
+    CK(cudaMemcpyAsync(Si, m + N, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H Si");
+    CK(cudaMemcpyAsync(Sij, m + 4 * N, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H Sij");
+    CK(cudaMemcpyAsync(S, m + 10 * N, N * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H S");
+    CK(cudaStreamSynchronize(s), "sync");
     return GRANITE_OK;
 }
 
@@ -759,6 +814,7 @@ cudaError_t upload_xfer(const std::vector<XferBox>& boxes, XferList& out, cudaSt
 }
 
 // Arena layout of a block list: 3 buffers per block, each 256-byte aligned.
+// Block i's cells start at cell offset moff in the matter arrays (block order).
 static int alloc_arena(Ctx* c, const std::vector<granite_block_desc>& descs, char** arena, size_t* bytes,
                        std::vector<DevBlock>& hb) {
     std::vector<size_t> off(descs.size());
@@ -771,13 +827,45 @@ static int alloc_arena(Ctx* c, const std::vector<granite_block_desc>& descs, cha
     CK(cudaMalloc(arena, total), "cudaMalloc(arena)");
     *bytes = total;
     hb.resize(descs.size());
+    long long moff = 0;
     for (size_t i = 0; i < descs.size(); ++i) {
         DevBlock d = make_devblock(descs[i], c->p.ko_sigma);
         const size_t one = ((size_t)cells_of(descs[i]) * NV * sizeof(double) + 255) / 256 * 256;
         for (int sl = 0; sl < 3; ++sl) d.buf[sl] = reinterpret_cast<double*>(*arena + off[i] + sl * one);
+        d.moff = c->matter ? (int)moff : 0;  // the total is checked against INT_MAX when matter is on
+        moff += cells_of(descs[i]);
         hb[i] = d;
     }
     return GRANITE_OK;
+}
+
+// Resident matter arrays for n cells (zero = vacuum); the first `keep` cells of
+// each of the four arrays are copied from the current ones.
+static int realloc_matter(Ctx* c, long long n, long long keep) {
+    if (n > INT_MAX) return fail(c, GRANITE_ERR_UNSUPPORTED, "resident matter: more than 2^31 cells in all blocks");
+    double* m = nullptr;
+    CK(cudaMalloc(&m, (size_t)n * NPRIM * sizeof(double)), "cudaMalloc(matter)");
+    cudaError_t e = cudaMemsetAsync(m, 0, (size_t)n * NPRIM * sizeof(double), c->stream);
+    const long long N = c->matter_cells;
+    const int width[4] = {1, 3, 6, 1}, at[4] = {0, 1, 4, 10};  // rho, Si, Sij, S
+    for (int q = 0; q < 4 && e == cudaSuccess && keep > 0; ++q)
+        e = cudaMemcpyAsync(m + at[q] * n, c->d_matter + at[q] * N, (size_t)keep * width[q] * sizeof(double),
+                            cudaMemcpyDeviceToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        cudaFree(m);
+        return cuda_fail(c, e, "matter arrays");
+    }
+    cudaFree(c->d_matter);
+    c->d_matter = m;
+    c->matter_cells = n;
+    return GRANITE_OK;
+}
+
+static long long total_cells(const std::vector<granite_block_desc>& descs) {
+    long long n = 0;
+    for (const auto& d : descs) n += cells_of(d);
+    return n;
 }
 
 // Everything derived from the block list (not the arena): block table, tensor
@@ -873,10 +961,49 @@ int granite_ccz4_commit(void* h) {
     int r = alloc_arena(c, c->descs, &c->arena, &c->arena_bytes, c->hblocks);
     if (r) return r;
     CK(cudaMemsetAsync(c->arena, 0, c->arena_bytes, c->stream), "memset arena");
+    if (c->matter && (r = realloc_matter(c, total_cells(c->descs), 0))) return r;
     if ((r = build_lists(c))) return r;
     c->level_time.assign(c->levels.size(), 0.0);
     c->committed = true;
     return GRANITE_OK;
+}
+
+int granite_ccz4_enable_matter(void* h, int on) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (c->committed) return fail(c, GRANITE_ERR_INVALID, "enable matter before commit");
+    c->matter = on != 0;
+    return GRANITE_OK;
+}
+
+int granite_ccz4_set_primitives_device(void* h, int i, const double* prim_dev) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (!c->committed || !c->matter) return fail(c, GRANITE_ERR_INVALID, "enable matter and commit first");
+    if (i < 0 || i >= (int)c->descs.size()) return fail(c, GRANITE_ERR_INVALID, "block index out of range");
+    if (!prim_dev) return fail(c, GRANITE_ERR_INVALID, "null buffer");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    const DevBlock& d = c->hblocks[i];
+    double* m = c->d_matter;
+    const long long N = c->matter_cells, o0 = d.moff;
+    const MatterOut o{m + o0, m + N + 3 * o0, m + 4 * N + 6 * o0, m + 10 * N + o0, 3, 1, 6, 1};
+    CK(launch_matter_sources(d, prim_dev, o, c->stream), "launch matter sources");
+    c->launches += 1;
+    return GRANITE_OK;
+}
+
+int granite_ccz4_upload_primitives(void* h, int i, const double* prim) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (!c->committed || !c->matter) return fail(c, GRANITE_ERR_INVALID, "enable matter and commit first");
+    if (i < 0 || i >= (int)c->descs.size()) return fail(c, GRANITE_ERR_INVALID, "block index out of range");
+    if (!prim) return fail(c, GRANITE_ERR_INVALID, "null host buffer");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    const size_t N = (size_t)c->hblocks[i].stride;
+    int r = ensure_scratch(c, N, 1);
+    if (r) return r;
+    CK(cudaMemcpyAsync(c->s_u, prim, N * NPRIM * sizeof(double), cudaMemcpyHostToDevice, c->stream), "H2D prim");
+    return granite_ccz4_set_primitives_device(c, i, c->s_u);
 }
 
 int granite_ccz4_tag_count(void* h, int level, int var, double threshold, long long* count) {
@@ -964,6 +1091,12 @@ int granite_ccz4_regrid_add(void* h, const granite_block_desc* b, int n) {
     if (e != cudaSuccess) {
         cudaFree(arena);
         return cuda_fail(c, e, "regrid");
+    }
+    if (c->d_matter) {  // old blocks keep their sources (same offsets), new blocks start in vacuum
+        if ((r = realloc_matter(c, total_cells(descs), c->matter_cells))) {
+            cudaFree(arena);
+            return r;
+        }
     }
     release_lists(c);
     cudaFree(c->arena);

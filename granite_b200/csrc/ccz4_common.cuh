@@ -35,7 +35,7 @@ struct DevBlock {
     double kocf[3];      // sigma/(64 dx)  KO (ccz4.cpp:886-887)
     double kow[3][4];    // kocf[d] * {1, -6, 15, -20}: the KO weights of ccz4.cpp:921
     int level;
-    int pad_;
+    int moff;            // resident matter: cell offset of the block in the context's matter arrays
 };
 
 // One unit of the batched work-list: a tile of interior points of a block.
@@ -56,7 +56,9 @@ struct StageArgs {
     double chi_c, chi_w, kappa1, kappa2, eta;
     // standalone RHS output (EPI_STORE): rhs base per block is given by rhs_ptr
     double* rhs;     // single-block RHS destination (EPI_STORE only)
-    const double* rho; const double* Si; const double* Sij; const double* S;  // matter (nullable)
+    // matter sources (nullable): rho[N], Si[N][3], Sij[N][6], S[N] over the cells of
+    // all blocks, block b's cell c at N-index B.moff + c
+    const double* rho; const double* Si; const double* Sij; const double* S;
     unsigned long long* nonfinite;  // floor hits on non-finite chi/alpha (nullable)
     const void* tmaps;     // TMA variant: CUtensorMap of (block b, slot s) at tmaps[3 b + s]
     unsigned int* errflag; // TMA variant: set to 1 when a bounded mbarrier wait gives up (nullable)

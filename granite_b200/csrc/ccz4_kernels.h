@@ -128,6 +128,20 @@ cudaError_t launch_constraints(const DevBlock* blocks, const Tile* tiles, int nt
 cudaError_t launch_tag_count(const DevBlock* blocks, const Tile* tiles, int ntiles, int var, double threshold,
                              unsigned long long* count, cudaStream_t stream);
 
+// Matter sources of the CCZ4 RHS from GRMHD primitives (grmhd.cpp:1034-1103)
+// at the interior cells of one block. prim: NPRIM fields of B.stride cells.
+// Outputs: rho[c], S[c], Si[c * si_cell + a * si_comp], Sij[c * sij_cell + q * sij_comp]
+// (the reference's AoS arrays: si_cell 3, si_comp 1, sij_cell 6, sij_comp 1).
+constexpr int NPRIM = 11;
+struct MatterOut {
+    double* rho;
+    double* Si;
+    double* Sij;
+    double* S;
+    long long si_cell, si_comp, sij_cell, sij_comp;
+};
+cudaError_t launch_matter_sources(const DevBlock& B, const double* prim, const MatterOut& out, cudaStream_t stream);
+
 // Deterministic fixed-order sum of n partial pairs into out[2].
 cudaError_t launch_sum_partials(const double* partials, int n, double* out, cudaStream_t stream);
 

@@ -520,12 +520,13 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     // matter sources (ccz4.cpp:651,664,682,764), zero in vacuum
     P rho = (P)0, Str = (P)0, Si[3] = {(P)0, (P)0, (P)0}, Sij[6] = {(P)0, (P)0, (P)0, (P)0, (P)0, (P)0};
     if (A.rho) {
-        rho = (P)__ldg(A.rho + c);
-        Str = (P)__ldg(A.S + c);
+        const long long cm = c + B.moff;
+        rho = (P)__ldg(A.rho + cm);
+        Str = (P)__ldg(A.S + cm);
 #pragma unroll
-        for (int a = 0; a < 3; ++a) Si[a] = (P)__ldg(A.Si + 3 * c + a);
+        for (int a = 0; a < 3; ++a) Si[a] = (P)__ldg(A.Si + 3 * cm + a);
 #pragma unroll
-        for (int a = 0; a < 6; ++a) Sij[a] = (P)__ldg(A.Sij + 6 * c + a);
+        for (int a = 0; a < 6; ++a) Sij[a] = (P)__ldg(A.Sij + 6 * cm + a);
     }
     const P PI = (P)PI_D;
 

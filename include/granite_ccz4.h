@@ -139,6 +139,19 @@ GRANITE_API int granite_ccz4_compute_rhs_device(void* ctx, const granite_block_d
                                     const double* Sij_dev, const double* S_dev, int precision,
                                     void* stream);
 
+/* Replaces: GRMHDEvolution::computeMatterSources, grmhd.hpp:333-338,
+ * grmhd.cpp:1034-1103 (the matter sources main.cpp:300 hands to computeRHS).
+ * prim[11][N]: the primitive GridBlock's flatBuffer() (PrimitiveVar order rho,
+ * v^x, v^y, v^z, p, B^x, B^y, B^z, eps, T, Ye; types.hpp:149-162); rho[N],
+ * Si[N][3], Sij[N][6], S[N]: written at interior cells, equal to the
+ * reference's bit for bit; other cells keep their values. */
+GRANITE_API int granite_ccz4_matter_sources_host(void* ctx, const granite_block_desc* b, const double* prim,
+                                                 double* rho, double* Si, double* Sij, double* S);
+/* Same on device memory, enqueued on `stream` (NULL = the context stream). */
+GRANITE_API int granite_ccz4_matter_sources_device(void* ctx, const granite_block_desc* b, const double* prim_dev,
+                                                   double* rho_dev, double* Si_dev, double* Sij_dev,
+                                                   double* S_dev, void* stream);
+
 /* ---- resident blocks ----------------------------------------------------- */
 /* The hierarchy lives in one device arena per context: add every block, then
  * commit (allocates state + 2 stage buffers per block and builds the per-level
@@ -147,6 +160,18 @@ GRANITE_API int granite_ccz4_compute_rhs_device(void* ctx, const granite_block_d
 
 GRANITE_API int granite_ccz4_add_block(void* ctx, const granite_block_desc* b, int* block_index);
 GRANITE_API int granite_ccz4_commit(void* ctx);
+
+/* Resident matter coupling (the non-vacuum applyRHS of main.cpp:296-302):
+ * before commit, granite_ccz4_enable_matter(ctx, 1) gives every block 11
+ * matter-source fields (rho, S_i, S_ij, S; zero = vacuum), which every RHS of
+ * rk3_step / hierarchy_step reads. granite_ccz4_upload_primitives (host
+ * prim[11][N]) or _set_primitives_device (device, stream-ordered on the
+ * context stream) recompute a block's sources from its primitives with
+ * computeMatterSources; they stay fixed until the next call. Blocks a regrid
+ * adds start in vacuum. */
+GRANITE_API int granite_ccz4_enable_matter(void* ctx, int on);
+GRANITE_API int granite_ccz4_upload_primitives(void* ctx, int block_index, const double* prim);
+GRANITE_API int granite_ccz4_set_primitives_device(void* ctx, int block_index, const double* prim_dev);
 
 /* Replaces the block creation of AMRHierarchy::regrid (amr.cpp:80-301), which
  * only ever adds blocks: appends n blocks (levels >= 1) to a committed

@@ -152,6 +152,16 @@ class Oracle:
         self.lib.orc_constraints(C.byref(_cg(g)), _p(u), _p(ham), _p(mom))
         return ham, mom
 
+    def matter_sources(self, g: Geom, prim, out=None):
+        """GRMHDEvolution::computeMatterSources (grmhd.cpp:1034-1103): (rho, Si, Sij, S)
+        shaped (nz, ny, nx[, 3 | 6]) incl. ghosts; only interior cells are written
+        (``out`` supplies the initial arrays, zeros by default)."""
+        rho, Si, Sij, S = out if out is not None else matter_zeros(g)
+        rho, Si, Sij, S = (np.array(a, dtype=np.float64, copy=True) for a in (rho, Si, Sij, S))
+        prim = np.ascontiguousarray(prim, dtype=np.float64)
+        self.lib.orc_matter_sources(C.byref(_cg(g)), _p(prim), _p(rho), _p(Si), _p(Sij), _p(S))
+        return rho, Si, Sij, S
+
     def constraint_sums(self, g: Geom, u):
         h2, m2, n = C.c_double(), C.c_double(), C.c_long()
         self.lib.orc_constraint_sums(C.byref(_cg(g)), _p(u), C.byref(h2), C.byref(m2),
@@ -167,13 +177,16 @@ class Oracle:
         fn(C.byref(_cg(g)), _p(u))
         return u
 
-    def rk3_steps(self, p: Params, g: Geom, u, dt: float, nsteps: int, bc: int = BC_SOMMERFELD):
+    def rk3_steps(self, p: Params, g: Geom, u, dt: float, nsteps: int, bc: int = BC_SOMMERFELD,
+                  matter=None):
+        """nsteps RK3 steps; ``matter`` = (rho, Si, Sij, S) held fixed, or None (vacuum)."""
         u = np.array(u, dtype=np.float64, copy=True)
         stage = g.zeros()
         rhs = g.zeros()
+        m = [None] * 4 if matter is None else [np.ascontiguousarray(a, dtype=np.float64) for a in matter]
         for _ in range(nsteps):
-            self.lib.orc_rk3_step(C.byref(_cp(p)), C.byref(_cg(g)), _p(u), _p(stage), _p(rhs),
-                                  C.c_double(dt), C.c_int(bc))
+            self.lib.orc_rk3_step_matter(C.byref(_cp(p)), C.byref(_cg(g)), _p(u), _p(stage), _p(rhs),
+                                         C.c_double(dt), C.c_int(bc), *[_p(a) for a in m])
         return u
 
     def init_flat(self, g: Geom):
@@ -276,6 +289,14 @@ class Reference:
         self.lib.ref_constraints(*self._g(g), _p(u), _p(ham), _p(mom))
         return ham, mom
 
+    def matter_sources(self, g: Geom, prim, out=None):
+        """The compiled GRMHDEvolution::computeMatterSources (grmhd.cpp:1034-1103)."""
+        rho, Si, Sij, S = out if out is not None else matter_zeros(g)
+        rho, Si, Sij, S = (np.array(a, dtype=np.float64, copy=True) for a in (rho, Si, Sij, S))
+        prim = np.ascontiguousarray(prim, dtype=np.float64)
+        self.lib.ref_matter_sources(*self._g(g), _p(prim), _p(rho), _p(Si), _p(Sij), _p(S))
+        return rho, Si, Sij, S
+
     def init_flat(self, g: Geom):
         u = g.zeros()
         self.lib.ref_init_flat(*self._g(g), _p(u))
@@ -338,6 +359,41 @@ class Reference:
 # ---------------------------------------------------------------------------
 # Seeded workloads shared by tests and bench (same draws on every backend)
 # ---------------------------------------------------------------------------
+
+NPRIM = 11  # PrimitiveVar::NUM_VARS (types.hpp:149-162)
+
+
+def matter_zeros(g: Geom):
+    cells = g.shape[1:]
+    return (np.zeros(cells), np.zeros(cells + (3,)), np.zeros(cells + (6,)), np.zeros(cells))
+
+
+def seeded_primitives(g: Geom, seed: int, superluminal: float = 0.0):
+    """Primitives (PrimitiveVar order) of a magnetised fluid on every cell, from
+    the integer hash of hash_noise (identical on every host): rho in [1e-3, 1]
+    with ~1 % exact zeros, |v_a| < 0.5 (a fraction ``superluminal`` of cells with
+    v^x in [0.9, 1.2], where the W clamp of computeMatterSources acts), p in
+    [1e-4, 0.1], B in [-0.2, 0.2], eps in [0.01, 1], T and Ye arbitrary."""
+    cells = g.shape[1:]
+
+    def h(s):
+        return hash_noise(cells, seed * 16 + s) + 0.5  # [0, 1)
+
+    p = np.empty((NPRIM,) + cells)
+    p[0] = 1e-3 + (1.0 - 1e-3) * h(1)
+    p[0][h(2) < 0.01] = 0.0
+    for a in range(3):
+        p[1 + a] = h(3 + a) - 0.5
+    fast = h(6) < superluminal
+    p[1][fast] = 0.9 + 0.3 * h(7)[fast]
+    p[4] = 1e-4 + 0.1 * h(8)
+    for a in range(3):
+        p[5 + a] = 0.4 * (h(9 + a) - 0.5)
+    p[8] = 0.01 + h(12)
+    p[9] = 10.0 * h(13)
+    p[10] = 0.05 + 0.45 * h(14)
+    return p
+
 
 def add_noise(u, amplitude: float, seed: int):
     """Uniform(-a, a) noise on every field and cell, numpy PCG64 stream."""

@@ -802,18 +802,26 @@ static void level_fill(const orc_geom* g, double* u, int bc) {
  * TimeIntegrator::sspRK3Step's spacetime part (main.cpp:673-689). */
 void orc_rk3_step(const orc_params* p, const orc_geom* g, double* u, double* stage,
                   double* rhs, double dt, int bc) {
+    orc_rk3_step_matter(p, g, u, stage, rhs, dt, bc, NULL, NULL, NULL, NULL);
+}
+
+/* The same step with matter sources held fixed over its three RHS evaluations
+ * (main.cpp:296-302 with the primitives unchanged between stages). */
+void orc_rk3_step_matter(const orc_params* p, const orc_geom* g, double* u, double* stage, double* rhs,
+                         double dt, int bc, const double* rho, const double* Si, const double* Sij,
+                         const double* S) {
     level_fill(g, u, bc);
-    orc_rhs(p, g, u, rhs, NULL, NULL, NULL, NULL);
+    orc_rhs(p, g, u, rhs, rho, Si, Sij, S);
     combine(g, stage, u, 1.0, u, 0.0, rhs, 1.0, dt);
     orc_floors(g, stage);
     outer_bc(g, stage, bc);
 
-    orc_rhs(p, g, stage, rhs, NULL, NULL, NULL, NULL);
+    orc_rhs(p, g, stage, rhs, rho, Si, Sij, S);
     combine(g, stage, u, 0.75, stage, 0.25, rhs, 0.25, dt);
     orc_floors(g, stage);
     outer_bc(g, stage, bc);
 
-    orc_rhs(p, g, stage, rhs, NULL, NULL, NULL, NULL);
+    orc_rhs(p, g, stage, rhs, rho, Si, Sij, S);
     combine(g, u, u, 1.0 / 3.0, stage, 2.0 / 3.0, rhs, 2.0 / 3.0, dt);
     orc_floors(g, u);
     orc_algebraic(g, u);
@@ -1103,5 +1111,54 @@ void orc_prolongate_masked(const orc_geom* cg, const double* uc, const orc_geom*
                         w011 * CV(ci[0], cn[1], cn[2]) + w111 * CV(cn[0], cn[1], cn[2]);
 #undef CV
                 }
+            }
+}
+
+/* GRMHDEvolution::computeMatterSources, grmhd.cpp:1034-1103, at interior
+ * cells: the ADM matter sources of a magnetised perfect fluid from the
+ * primitives (PrimitiveVar order: rho, v^x, v^y, v^z, p, B^x, B^y, B^z, eps,
+ * T, Ye; types.hpp:149-162). h = 1 + eps + p / (rho + 1e-30) (grmhd.hpp:55);
+ * W = 1 / sqrt(max(1 - v^2, 1e-10)) with std::max's NaN behaviour;
+ * b^2 = B^2 / W^2 + (B.v)^2; b_i = B_i / W^2 + (B.v) v_i;
+ * rho_ADM = rho h W^2 - p + b^2 / 2; S_i = (rho h W^2 + b^2) v_i - (B.v) b_i;
+ * S_ij = (rho h W^2 + b^2) v_i v_j + (p + b^2/2) delta_ij - b_i b_j - B_i B_j / W^2;
+ * S = S_xx + S_yy + S_zz. Cells outside the interior keep their values. */
+void orc_matter_sources(const orc_geom* g, const double* prim, double* rho, double* Si, double* Sij,
+                        double* S) {
+    const int ng = g->ng, tx = tx_(g), ty = ty_(g);
+    const long stride = orc_stride(g);
+    for (int k = ng; k < ng + g->n[2]; ++k)
+        for (int j = ng; j < ng + g->n[1]; ++j)
+            for (int i = ng; i < ng + g->n[0]; ++i) {
+                const long c = i + (long)tx * (j + (long)ty * k);
+                const double rho_p = prim[c], vx = prim[stride + c], vy = prim[2 * stride + c],
+                             vz = prim[3 * stride + c], press = prim[4 * stride + c];
+                const double Bx = prim[5 * stride + c], By = prim[6 * stride + c], Bz = prim[7 * stride + c];
+                const double eps = prim[8 * stride + c];
+                const double h = 1.0 + eps + press / (rho_p + 1e-30);
+                const double v2 = vx * vx + vy * vy + vz * vz;
+                const double one_m = 1.0 - v2;
+                const double W = 1.0 / sqrt(one_m < 1.0e-10 ? 1.0e-10 : one_m);
+                const double W2 = W * W;
+                const double Bv = Bx * vx + By * vy + Bz * vz;
+                const double B2 = Bx * Bx + By * By + Bz * Bz;
+                const double b2 = B2 / W2 + Bv * Bv;
+                const double rhoHW2 = rho_p * h * W2;
+                rho[c] = rhoHW2 - press + 0.5 * b2;
+                const double vel[3] = {vx, vy, vz};
+                const double bco[3] = {Bx / W2 + Bv * vx, By / W2 + Bv * vy, Bz / W2 + Bv * vz};
+                const double Bco[3] = {Bx, By, Bz};
+                for (int a = 0; a < 3; ++a) Si[3 * c + a] = (rhoHW2 + b2) * vel[a] - Bv * bco[a];
+                double tr = 0.0;
+                for (int a = 0; a < 3; ++a)
+                    for (int b = a; b < 3; ++b) {
+                        const double delta = a == b ? 1.0 : 0.0;
+                        const int s = a == 0 ? b : (a == 1 ? 2 + b : 5);  /* symIdx, types.hpp:52-54 */
+                        const double v = (rhoHW2 + b2) * vel[a] * vel[b] + (press + 0.5 * b2) * delta -
+                            bco[a] * bco[b] - Bco[a] * Bco[b] / W2;
+                        Sij[6 * c + s] = v;
+                        if (a == b) tr += v;
+                    }
+                S[c] = tr;
             }
 }

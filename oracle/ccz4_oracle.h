@@ -64,6 +64,10 @@ void orc_algebraic(const orc_geom* g, double* u);
  * u: state (in/out); stage, rhs: scratch of the same size. bc: ORC_BC_*. */
 void orc_rk3_step(const orc_params* p, const orc_geom* g, double* u, double* stage,
                   double* rhs, double dt, int bc);
+/* orc_rk3_step with matter sources (layout as orc_rhs) in all three stages. */
+void orc_rk3_step_matter(const orc_params* p, const orc_geom* g, double* u, double* stage, double* rhs,
+                         double dt, int bc, const double* rho, const double* Si, const double* Sij,
+                         const double* S);
 
 /* initial data over all cells */
 void orc_init_flat(const orc_geom* g, double* u);
@@ -88,6 +92,13 @@ void orc_prolongate_masked(const orc_geom* cg, const double* uc, const orc_geom*
 /* sum over interior points of H^2 and |M|^2 of one block (for RMS norms) */
 void orc_constraint_sums(const orc_geom* g, const double* u, double* h2, double* m2,
                          long* npts);
+
+/* GRMHD matter sources of the CCZ4 RHS (grmhd.cpp:1034-1103): prim[11][N] in
+ * PrimitiveVar order; rho[N], Si[N][3], Sij[N][6], S[N] written at interior
+ * cells only. */
+#define ORC_NPRIM 11
+void orc_matter_sources(const orc_geom* g, const double* prim, double* rho, double* Si, double* Sij,
+                        double* S);
 
 /* OpenMP thread count used by the parallel loops (0 = leave default) */
 void orc_set_threads(int n);

@@ -1,8 +1,9 @@
 // ref_shim.cpp -- C ABI over the compiled GRANITE reference (test infrastructure).
 //
 // oracle/Makefile compiles this file together with the unmodified reference
-// sources src/spacetime/ccz4.cpp, src/core/grid.cpp, src/amr/amr.cpp and
-// src/initial_data/initial_data.cpp into oracle/_ref/libgranite_ref_*.so.
+// sources src/spacetime/ccz4.cpp, src/core/grid.cpp, src/amr/amr.cpp,
+// src/initial_data/initial_data.cpp and src/grmhd/{grmhd,hlld,tabulated_eos}.cpp
+// into oracle/_ref/libgranite_ref_*.so.
 // The shim only copies flat buffers in and out of reference GridBlocks and
 // calls the reference's own operators; it adds no arithmetic of its own except
 // in ref_rk3_steps, whose main.cpp lambdas (combine, floors, algebraic
@@ -12,6 +13,7 @@
 // computeRHSVacuum and AMRHierarchy::fillGhostZones.
 #include "granite/amr/amr.hpp"
 #include "granite/core/grid.hpp"
+#include "granite/grmhd/grmhd.hpp"
 #include "granite/initial_data/initial_data.hpp"
 #include "granite/spacetime/ccz4.hpp"
 
@@ -150,6 +152,36 @@ void ref_constraints(const int* n, int ng, const double* lo, const double* hi, c
     for (size_t c = 0; c < h.size(); ++c) {
         ham[c] = h[c];
         for (int a = 0; a < 3; ++a) mom[3 * c + a] = m[c][a];
+    }
+}
+
+// GRMHDEvolution::computeMatterSources (grmhd.cpp:1034-1103): prim[11][N]
+// (PrimitiveVar order, types.hpp:149-162) in; rho[N], Si[N][3], Sij[N][6],
+// S[N] in/out (interior written, the rest keeps the caller's values). The
+// ideal-gas EOS is a placeholder: the routine only calls the non-virtual
+// EquationOfState::enthalpy (grmhd.hpp:55).
+void ref_matter_sources(const int* n, int ng, const double* lo, const double* hi, const double* prim,
+                        double* rho, double* Si, double* Sij, double* S) {
+    Geo g = geo(n, ng, lo, hi);
+    auto st = block(g);
+    auto pr = std::make_unique<GridBlock>(1, 0, g.n, g.lo, g.hi, g.ng, NUM_PRIMITIVE_VARS);
+    std::memcpy(pr->flatBuffer(), prim, sizeof(Real) * pr->totalSize() * NUM_PRIMITIVE_VARS);
+    const size_t N = st->totalSize();
+    std::vector<Real> r(rho, rho + N), s(S, S + N);
+    std::vector<std::array<Real, DIM>> si(N);
+    std::vector<std::array<Real, SYM_TENSOR_COMPS>> sij(N);
+    for (size_t c = 0; c < N; ++c) {
+        for (int a = 0; a < 3; ++a) si[c][a] = Si[3 * c + a];
+        for (int a = 0; a < 6; ++a) sij[c][a] = Sij[6 * c + a];
+    }
+    grmhd::GRMHDParams gp;
+    grmhd::GRMHDEvolution ev(gp, std::make_shared<grmhd::IdealGasEOS>());
+    ev.computeMatterSources(*st, *pr, r, si, sij, s);
+    for (size_t c = 0; c < N; ++c) {
+        rho[c] = r[c];
+        S[c] = s[c];
+        for (int a = 0; a < 3; ++a) Si[3 * c + a] = si[c][a];
+        for (int a = 0; a < 6; ++a) Sij[6 * c + a] = sij[c][a];
     }
 }
 

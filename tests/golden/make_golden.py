@@ -5,8 +5,8 @@ Run where the reference tree is present (it builds oracle/_ref from it):
     python tests/golden/make_golden.py
 
 Inputs are not stored: they are rebuilt from oracle.seeded_state /
-oracle.seeded_matter (IEEE + and * plus an integer hash, so identical on any
-host). Outputs of the reference (strict IEEE build) are stored, interior cells
+oracle.seeded_matter / oracle.seeded_primitives (IEEE + and * plus an integer
+hash, so identical on any host). Outputs of the reference (strict IEEE build) are stored, interior cells
 only, float64. Each case records its geometry and parameters.
 """
 from __future__ import annotations
@@ -86,6 +86,12 @@ def main():
     cases["prolong"] = (G_F, dict(u=ref.prolongate(G_C, uc, 0, G_F, uf, 1)[:4], seed_c=31, seed_f=32))
     cases["restrict"] = (G_C, dict(u=ref.restrict(G_F, uf, 1, G_C, uc, 0)[G_C.interior()], seed_c=31,
                                   seed_f=32))
+
+    prim = oracle.seeded_primitives(G_RAND, 41, superluminal=0.05)
+    rho, Si, Sij, S = ref.matter_sources(G_RAND, prim)
+    it = G_RAND.interior()[1:]
+    cases["matter_sources"] = (G_RAND, dict(rho=rho[it], Si=Si[it], Sij=Sij[it], S=S[it], seed=41,
+                                            superluminal=0.05))
 
     for name, (g, data) in cases.items():
         path = os.path.join(OUT, f"{name}.npz")

@@ -36,7 +36,7 @@ def test_golden_files_present():
     names = {os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLD, "*.npz"))}
     for n in ["rhs_random", "rhs_matter", "rhs_random_noko", "constraints_random", "ko_random",
               "rhs_bl", "constraints_bl", "rk3_bl_3steps", "init_bl", "init_gauge_wave",
-              "rk3_gauge_wave_periodic_4steps", "prolong", "restrict"]:
+              "rk3_gauge_wave_periodic_4steps", "prolong", "restrict", "matter_sources"]:
         assert n in names, n
 
 
@@ -54,6 +54,32 @@ def test_oracle_rhs_matter_golden(oracle_lib):
     m = oracle.seeded_matter(g, int(z["matter_seed"]))
     out = oracle_lib.rhs(Params(), g, u, *m)
     assert np.array_equal(out[g.interior()], z["rhs"])
+
+
+def test_oracle_matter_sources_golden(oracle_lib):
+    """GRMHDEvolution::computeMatterSources (grmhd.cpp:1034-1103), with cells of
+    v^2 >= 1 (the W clamp) and of zero density among them."""
+    g, z = load("matter_sources")
+    prim = oracle.seeded_primitives(g, int(z["seed"]), superluminal=float(z["superluminal"]))
+    assert (prim[1] ** 2 + prim[2] ** 2 + prim[3] ** 2 >= 1.0).any() and (prim[0] == 0.0).any()
+    out = oracle_lib.matter_sources(g, prim)
+    it = g.interior()[1:]
+    for a, name in zip(out, ("rho", "Si", "Sij", "S")):
+        assert np.array_equal(a[it], z[name]), name
+        rest = np.ones(a.shape[:3], dtype=bool)
+        rest[it] = False
+        assert not a[rest].any(), f"{name}: a cell outside the interior was written"
+
+
+@pytest.mark.skipif(not oracle.reference_available("strict"), reason="reference library not built")
+@pytest.mark.parametrize("seed,superluminal", [(3, 0.0), (4, 0.3)])
+def test_oracle_matter_sources_vs_reference(oracle_lib, seed, superluminal):
+    ref = oracle.Reference("strict")
+    g = Geom((9, 7, 5), (-1.0, 0.0, 2.0), (0.8, 1.4, 3.0))
+    prim = oracle.seeded_primitives(g, seed, superluminal)
+    init = tuple(oracle.hash_noise(a.shape, 90 + k) for k, a in enumerate(oracle.matter_zeros(g)))
+    for a, b in zip(oracle_lib.matter_sources(g, prim, init), ref.matter_sources(g, prim, init)):
+        assert np.array_equal(a, b)
 
 
 def test_oracle_constraints_golden(oracle_lib):
