@@ -112,6 +112,10 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_measure_fma_rate.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
     lib.granite_ccz4_get_fp64_chi_threshold.argtypes = [vp, C.POINTER(C.c_double)]
     lib.granite_ccz4_regrid_add.argtypes = [vp, C.POINTER(_BlockDesc), C.c_int]
+    lib.granite_ccz4_checkpoint_write.argtypes = [vp, C.c_char_p, C.c_int, C.c_double]
+    lib.granite_ccz4_checkpoint_read.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int), dp]
+    lib.granite_ccz4_checkpoint_header.argtypes = [C.c_char_p, C.POINTER(C.c_int), dp, C.POINTER(C.c_int),
+                                                   C.POINTER(_BlockDesc), C.c_int, C.POINTER(C.c_int)]
     lib.granite_ccz4_matter_sources_host.argtypes = [vp, C.POINTER(_BlockDesc), dp, dp, dp, dp, dp]
     lib.granite_ccz4_matter_sources_device.argtypes = [vp, C.POINTER(_BlockDesc), vp, vp, vp, vp, vp, vp]
     lib.granite_ccz4_enable_matter.argtypes = [vp, C.c_int]
@@ -372,6 +376,25 @@ class MatterSources:
 # Resident hierarchy + RK3 driver (main.cpp TimeIntegrator, amr.cpp subcycle)
 # ---------------------------------------------------------------------------
 
+def checkpoint_header(path: str) -> dict:
+    """Step, time, has_matter and the GridBlocks (geometry only, in order) of a
+    checkpoint written by Evolver.checkpoint_write."""
+    lib = load_library()
+    n, step, mat = C.c_int(), C.c_int(), C.c_int()
+    t = C.c_double()
+    rc = lib.granite_ccz4_checkpoint_header(os.fsencode(path), C.byref(step), C.byref(t), C.byref(mat), None, 0,
+                                            C.byref(n))
+    if rc != GRANITE_OK:
+        raise GraniteError(rc, f"cannot read checkpoint header of {path}")
+    descs = (_BlockDesc * max(n.value, 1))()
+    rc = lib.granite_ccz4_checkpoint_header(os.fsencode(path), None, None, None, descs, n.value, C.byref(n))
+    if rc != GRANITE_OK:
+        raise GraniteError(rc, f"cannot read checkpoint header of {path}")
+    blocks = [GridBlock(d.id, d.level, tuple(d.ncells), tuple(d.lo), tuple(d.hi), d.nghost)
+              for d in descs[:n.value]]
+    return dict(step=step.value, time=t.value, has_matter=bool(mat.value), blocks=blocks)
+
+
 class Evolver:
     """Device-resident blocks advanced by the fused RK3 step.
 
@@ -511,6 +534,34 @@ class Evolver:
             raise errors[0]
         self.ctx.check(rc)
         return added
+
+    def checkpoint_write(self, path: str, step: int = 0, time: float = 0.0):
+        """The resident state (every block's state, level times, matter sources) to
+        ``path``, with the data model of HDF5Writer::writeCheckpoint (hdf5_io.cpp:166-233)."""
+        self.ctx.check(self.ctx.lib.granite_ccz4_checkpoint_write(self.ctx.h, os.fsencode(path), int(step),
+                                                                  float(time)))
+
+    def checkpoint_read(self, path: str):
+        """Restore a checkpoint of this hierarchy (same blocks in the same order);
+        returns (step, time)."""
+        step, t = C.c_int(), C.c_double()
+        self.ctx.check(self.ctx.lib.granite_ccz4_checkpoint_read(self.ctx.h, os.fsencode(path), C.byref(step),
+                                                                 C.byref(t)))
+        return step.value, t.value
+
+    @classmethod
+    def from_checkpoint(cls, path: str, params: CCZ4Params | None = None, variant: int | None = None):
+        """A committed Evolver holding the checkpoint's blocks and state; returns
+        (evolver, step, time). The blocks' host arrays stay zero until download()."""
+        hdr = checkpoint_header(path)
+        ev = cls(params, variant)
+        if hdr["has_matter"]:
+            ev.enable_matter()
+        for b in hdr["blocks"]:
+            ev.add_block(b)
+        ev.commit()
+        step, t = ev.checkpoint_read(path)
+        return ev, step, t
 
     def level_time(self, level: int) -> float:
         """Level::current_time of the reference hierarchy (amr.hpp:108-113)."""

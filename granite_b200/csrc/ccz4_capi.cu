@@ -1858,4 +1858,192 @@ int granite_ccz4_constraint_norms(void* h, int level, double* h_l2, double* m_l2
     return GRANITE_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Checkpoint / restart of the resident state
+//
+// The data model of HDF5Writer::writeCheckpoint (hdf5_io.cpp:166-233): root
+// attributes time, step, num_blocks, then per block b the totalSize() values of
+// every field v ("block_b/var_v"), in block order and field order. The
+// container is a flat little-endian file (the HDF5 library is not linked):
+//   "GRNB200\0", u32 version, u32 data offset,
+//   i32 step, i32 num_blocks, i32 num_vars, i32 num_levels, i32 has_matter, i32 0,
+//   f64 time, f64 level_time[num_levels], granite_block_desc blocks[num_blocks],
+//   zero padding to the data offset (a multiple of 4096),
+//   block_b/var_v for every b, v (f64), then, with matter, rho[N], Si[N][3],
+//   Sij[N][6], S[N] (N = the cells of all blocks).
+// Unlike the reference's reader (hdf5_io.cpp:392-467, which rebuilds every block
+// with the level-0 geometry), the block geometry is stored, so a hierarchy
+// resumes as it was.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr char CK_MAGIC[8] = {'G', 'R', 'N', 'B', '2', '0', '0', '\0'};
+constexpr uint32_t CK_VERSION = 1;
+constexpr size_t CK_CHUNK = size_t(64) << 20;  // pinned staging per transfer
+
+struct CkHeader {
+    char magic[8];
+    uint32_t version, data_offset;
+    int32_t step, num_blocks, num_vars, num_levels, has_matter, zero;
+    double time;
+};
+static_assert(sizeof(CkHeader) == 48, "checkpoint header layout");
+static_assert(sizeof(granite_block_desc) == 72, "block descriptor layout");
+
+struct File {
+    FILE* f = nullptr;
+    ~File() {
+        if (f) std::fclose(f);
+    }
+};
+
+int read_header(Ctx* c, FILE* f, CkHeader& h, std::vector<double>& lt, std::vector<granite_block_desc>& d) {
+    if (std::fread(&h, sizeof(h), 1, f) != 1 || std::memcmp(h.magic, CK_MAGIC, 8) != 0)
+        return fail(c, GRANITE_ERR_INVALID, "not a granite_b200 checkpoint");
+    if (h.version != CK_VERSION) return fail(c, GRANITE_ERR_UNSUPPORTED, "checkpoint version");
+    if (h.num_vars != NV || h.num_blocks < 0 || h.num_levels < 0 || h.num_levels > 64)
+        return fail(c, GRANITE_ERR_INVALID, "checkpoint header");
+    lt.resize(h.num_levels);
+    d.resize(h.num_blocks);
+    if ((h.num_levels && std::fread(lt.data(), sizeof(double), lt.size(), f) != lt.size()) ||
+        (h.num_blocks && std::fread(d.data(), sizeof(granite_block_desc), d.size(), f) != d.size()))
+        return fail(c, GRANITE_ERR_INVALID, "truncated checkpoint header");
+    return GRANITE_OK;
+}
+
+// Device <-> file through one pinned staging buffer, CK_CHUNK bytes at a time.
+int stream_out(Ctx* c, FILE* f, const char* dev, size_t bytes, char* pin) {
+    for (size_t o = 0; o < bytes; o += CK_CHUNK) {
+        const size_t n = std::min(CK_CHUNK, bytes - o);
+        CK(cudaMemcpyAsync(pin, dev + o, n, cudaMemcpyDeviceToHost, c->stream), "D2H checkpoint");
+        CK(cudaStreamSynchronize(c->stream), "sync");
+        if (std::fwrite(pin, 1, n, f) != n) return fail(c, GRANITE_ERR_INVALID, "checkpoint write failed");
+    }
+    return GRANITE_OK;
+}
+
+int stream_in(Ctx* c, FILE* f, char* dev, size_t bytes, char* pin) {
+    for (size_t o = 0; o < bytes; o += CK_CHUNK) {
+        const size_t n = std::min(CK_CHUNK, bytes - o);
+        if (std::fread(pin, 1, n, f) != n) return fail(c, GRANITE_ERR_INVALID, "truncated checkpoint data");
+        CK(cudaMemcpyAsync(dev + o, pin, n, cudaMemcpyHostToDevice, c->stream), "H2D checkpoint");
+        CK(cudaStreamSynchronize(c->stream), "sync");
+    }
+    return GRANITE_OK;
+}
+
+struct Pinned {
+    char* p = nullptr;
+    ~Pinned() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+}  // namespace
+
+int granite_ccz4_checkpoint_header(const char* path, int* step, double* time, int* has_matter,
+                                   granite_block_desc* blocks, int cap, int* num_blocks) {
+    if (!path || !num_blocks) return GRANITE_ERR_INVALID;
+    File f;
+    if (!(f.f = std::fopen(path, "rb"))) return GRANITE_ERR_INVALID;
+    CkHeader h;
+    std::vector<double> lt;
+    std::vector<granite_block_desc> d;
+    int r = read_header(nullptr, f.f, h, lt, d);
+    if (r) return r;
+    *num_blocks = h.num_blocks;
+    if (step) *step = h.step;
+    if (time) *time = h.time;
+    if (has_matter) *has_matter = h.has_matter;
+    if (blocks) {
+        if (cap < h.num_blocks) return GRANITE_ERR_TOO_LARGE;
+        std::copy(d.begin(), d.end(), blocks);
+    }
+    return GRANITE_OK;
+}
+
+int granite_ccz4_checkpoint_write(void* hc, const char* path, int step, double time) {
+    Ctx* c = static_cast<Ctx*>(hc);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (!c->committed) return fail(c, GRANITE_ERR_INVALID, "commit first");
+    if (!path) return fail(c, GRANITE_ERR_INVALID, "null path");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(c->stream), "sync");
+    CkHeader h{};
+    std::memcpy(h.magic, CK_MAGIC, 8);
+    h.version = CK_VERSION;
+    h.step = step;
+    h.num_blocks = (int)c->descs.size();
+    h.num_vars = NV;
+    h.num_levels = (int)c->level_time.size();
+    h.has_matter = c->d_matter ? 1 : 0;
+    h.time = time;
+    const size_t head = sizeof(h) + c->level_time.size() * sizeof(double) + c->descs.size() * sizeof(granite_block_desc);
+    h.data_offset = (uint32_t)((head + 4095) / 4096 * 4096);
+    if ((head + 4095) / 4096 * 4096 > UINT32_MAX) return fail(c, GRANITE_ERR_TOO_LARGE, "checkpoint header");
+    File f;
+    if (!(f.f = std::fopen(path, "wb"))) return fail(c, GRANITE_ERR_INVALID, std::string("cannot create ") + path);
+    std::vector<char> pad(h.data_offset - head, 0);
+    if (std::fwrite(&h, sizeof(h), 1, f.f) != 1 ||
+        (!c->level_time.empty() &&
+         std::fwrite(c->level_time.data(), sizeof(double), c->level_time.size(), f.f) != c->level_time.size()) ||
+        std::fwrite(c->descs.data(), sizeof(granite_block_desc), c->descs.size(), f.f) != c->descs.size() ||
+        (!pad.empty() && std::fwrite(pad.data(), 1, pad.size(), f.f) != pad.size()))
+        return fail(c, GRANITE_ERR_INVALID, "checkpoint write failed");
+    Pinned pin;
+    CK(cudaMallocHost(&pin.p, CK_CHUNK), "cudaMallocHost(checkpoint staging)");
+    int r;
+    for (size_t i = 0; i < c->descs.size(); ++i)  // block_b/var_v: slot 0 is field-major already
+        if ((r = stream_out(c, f.f, reinterpret_cast<const char*>(c->hblocks[i].buf[0]),
+                            (size_t)c->hblocks[i].stride * NV * sizeof(double), pin.p)))
+            return r;
+    if (c->d_matter &&
+        (r = stream_out(c, f.f, reinterpret_cast<const char*>(c->d_matter),
+                        (size_t)c->matter_cells * NPRIM * sizeof(double), pin.p)))
+        return r;
+    if (std::fflush(f.f) != 0) return fail(c, GRANITE_ERR_INVALID, "checkpoint write failed");
+    return GRANITE_OK;
+}
+
+int granite_ccz4_checkpoint_read(void* hc, const char* path, int* step, double* time) {
+    Ctx* c = static_cast<Ctx*>(hc);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (!c->committed) return fail(c, GRANITE_ERR_INVALID, "add the checkpoint's blocks and commit first");
+    if (!path) return fail(c, GRANITE_ERR_INVALID, "null path");
+    File f;
+    if (!(f.f = std::fopen(path, "rb"))) return fail(c, GRANITE_ERR_INVALID, std::string("cannot open ") + path);
+    CkHeader h;
+    std::vector<double> lt;
+    std::vector<granite_block_desc> d;
+    int r = read_header(c, f.f, h, lt, d);
+    if (r) return r;
+    if (d.size() != c->descs.size()) return fail(c, GRANITE_ERR_INVALID, "checkpoint: block count differs");
+    for (size_t i = 0; i < d.size(); ++i) {
+        const granite_block_desc &a = d[i], &b = c->descs[i];
+        bool same = a.nghost == b.nghost && a.level == b.level;
+        for (int k = 0; k < 3; ++k) same = same && a.ncells[k] == b.ncells[k] && a.lo[k] == b.lo[k] && a.hi[k] == b.hi[k];
+        if (!same) return fail(c, GRANITE_ERR_INVALID, "checkpoint: block " + std::to_string(i) + " geometry differs");
+    }
+    if ((h.has_matter != 0) != (c->d_matter != nullptr))
+        return fail(c, GRANITE_ERR_INVALID, "checkpoint: matter sources present in one of file and context only");
+    if (lt.size() != c->level_time.size()) return fail(c, GRANITE_ERR_INVALID, "checkpoint: level count differs");
+    if (std::fseek(f.f, (long)h.data_offset, SEEK_SET) != 0) return fail(c, GRANITE_ERR_INVALID, "checkpoint seek");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(c->stream), "sync");
+    Pinned pin;
+    CK(cudaMallocHost(&pin.p, CK_CHUNK), "cudaMallocHost(checkpoint staging)");
+    for (size_t i = 0; i < c->descs.size(); ++i)
+        if ((r = stream_in(c, f.f, reinterpret_cast<char*>(c->hblocks[i].buf[0]),
+                           (size_t)c->hblocks[i].stride * NV * sizeof(double), pin.p)))
+            return r;
+    if (c->d_matter && (r = stream_in(c, f.f, reinterpret_cast<char*>(c->d_matter),
+                                      (size_t)c->matter_cells * NPRIM * sizeof(double), pin.p)))
+        return r;
+    c->level_time = lt;
+    for (size_t L = 0; L < c->level_ghosts_valid.size(); ++L) c->level_ghosts_valid[L] = false;
+    if (step) *step = h.step;
+    if (time) *time = h.time;
+    return GRANITE_OK;
+}
+
 }  // extern "C"

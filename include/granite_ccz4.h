@@ -230,6 +230,23 @@ typedef int (*granite_regrid_fn)(void* user, int level, long long step_num);
 GRANITE_API int granite_ccz4_hierarchy_step_regrid(void* ctx, double dt_coarse, int precision, int amr_mode,
                                                    int regrid_interval, granite_regrid_fn fn, void* user);
 
+/* ---- checkpoint / restart --------------------------------------------------
+ * Replaces HDF5Writer::writeCheckpoint / HDF5Reader::readCheckpoint
+ * (hdf5_io.cpp:166-233, 392-467) for the resident state, with their data model
+ * (time, step, num_blocks; per block b every field v as "block_b/var_v", the
+ * block's totalSize() values) in a flat container (the HDF5 library is not
+ * linked) that also stores each block's geometry, the level times and the
+ * resident matter sources, so a hierarchy resumes exactly where it stopped.
+ * Restart: read the header (blocks may be NULL to get num_blocks first), add
+ * those blocks in that order, enable matter if has_matter, commit, then
+ * granite_ccz4_checkpoint_read. A bad or mismatching file returns
+ * GRANITE_ERR_INVALID and leaves the state unspecified only if the data part
+ * is truncated. Blocks until the file is written / the state is on the GPU. */
+GRANITE_API int granite_ccz4_checkpoint_write(void* ctx, const char* path, int step, double time);
+GRANITE_API int granite_ccz4_checkpoint_header(const char* path, int* step, double* time, int* has_matter,
+                                               granite_block_desc* blocks, int cap, int* num_blocks);
+GRANITE_API int granite_ccz4_checkpoint_read(void* ctx, const char* path, int* step, double* time);
+
 /* Level::current_time (amr.hpp:108-113): the sum of the level's step sizes so
  * far; a level created by a regrid starts at its parent's time. */
 GRANITE_API int granite_ccz4_level_time(void* ctx, int level, double* t);
