@@ -112,6 +112,12 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_measure_fma_rate.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
     lib.granite_ccz4_get_fp64_chi_threshold.argtypes = [vp, C.POINTER(C.c_double)]
     lib.granite_ccz4_regrid_add.argtypes = [vp, C.POINTER(_BlockDesc), C.c_int]
+    ip = C.POINTER(C.c_int)
+    lib.granite_ccz4_psi4_modes.argtypes = [vp, C.c_int, dp, C.c_int, C.c_int, C.c_int, C.c_int, dp, ip]
+    lib.granite_ccz4_psi4_modes_host.argtypes = [vp, C.POINTER(_BlockDesc), dp, dp, C.c_int, C.c_int, C.c_int,
+                                                 C.c_int, dp, ip]
+    lib.granite_ccz4_psi4_modes_device.argtypes = [vp, C.POINTER(_BlockDesc), vp, dp, C.c_int, C.c_int, C.c_int,
+                                                   C.c_int, dp, ip]
     lib.granite_ccz4_checkpoint_write.argtypes = [vp, C.c_char_p, C.c_int, C.c_double]
     lib.granite_ccz4_checkpoint_read.argtypes = [vp, C.c_char_p, C.POINTER(C.c_int), dp]
     lib.granite_ccz4_checkpoint_header.argtypes = [C.c_char_p, C.POINTER(C.c_int), dp, C.POINTER(C.c_int),

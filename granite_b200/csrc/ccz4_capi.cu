@@ -149,6 +149,8 @@ struct Ctx {
     bool batched = true;           // one launch per level and stage + CUDA graphs (else per block, eager)
     bool matter = false;           // resident matter sources (granite_ccz4_enable_matter)
     double* d_matter = nullptr;    // rho[N] | Si[N][3] | Sij[N][6] | S[N], N = matter_cells (all blocks)
+    char* s_diag = nullptr;        // diagnostics scratch (Psi4 sphere points, radii, modes, counts)
+    size_t s_diag_bytes = 0;
     long long matter_cells = 0;
     double fp64_chi = 0.0;         // MIXED: tiles with a point of chi below this run the FP64 algebra
     cudaStream_t stream = nullptr;
@@ -567,6 +569,7 @@ int granite_ccz4_destroy(void* h) {
     cudaFree(c->s_rhs);
     cudaFree(c->s_mat);
     cudaFree(c->d_matter);
+    cudaFree(c->s_diag);
     cudaFree(c->s_desc);
     cudaFree(c->s_tiles);
     cudaFree(c->s_partials);
@@ -2044,6 +2047,86 @@ int granite_ccz4_checkpoint_read(void* hc, const char* path, int* step, double* 
     if (step) *step = h.step;
     if (time) *time = h.time;
     return GRANITE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Psi4 extraction (Psi4Extractor::extract, postprocess.cpp:245-314)
+// ---------------------------------------------------------------------------
+namespace {
+
+int psi4_run(Ctx* c, const DevBlock& B, const double* u, const double hi[3], const double* radii, int nr, int n_theta,
+             int n_phi, int l_max, double* modes, int* npoints) {
+    if (!radii || !modes || nr <= 0 || n_theta <= 0 || n_phi <= 0 || l_max < 2 || l_max > 16)
+        return fail(c, GRANITE_ERR_INVALID, "psi4: radii, nr > 0, n_theta, n_phi > 0, 2 <= l_max <= 16");
+    const long long npts = (long long)nr * n_theta * n_phi;
+    if (npts > (1LL << 28)) return fail(c, GRANITE_ERR_TOO_LARGE, "psi4: more than 2^28 sphere points");
+    const int nm = (l_max + 1) * (l_max + 1) - 4;
+    const size_t b_r = ((size_t)nr * sizeof(double) + 255) / 256 * 256,
+                 b_modes = ((size_t)nr * nm * sizeof(double2) + 255) / 256 * 256,
+                 b_cnt = ((size_t)nr * sizeof(unsigned int) + 255) / 256 * 256, b_pts = (size_t)npts * sizeof(double2);
+    const size_t need = b_r + b_modes + b_cnt + b_pts;
+    if (need > c->s_diag_bytes) {
+        cudaFree(c->s_diag);
+        c->s_diag = nullptr;
+        c->s_diag_bytes = 0;
+        CK(cudaMalloc(&c->s_diag, need), "cudaMalloc(psi4 scratch)");
+        c->s_diag_bytes = need;
+    }
+    double* d_r = reinterpret_cast<double*>(c->s_diag);
+    double2* d_modes = reinterpret_cast<double2*>(c->s_diag + b_r);
+    unsigned int* d_cnt = reinterpret_cast<unsigned int*>(c->s_diag + b_r + b_modes);
+    double2* d_pts = reinterpret_cast<double2*>(c->s_diag + b_r + b_modes + b_cnt);
+    CK(cudaMemcpyAsync(d_r, radii, (size_t)nr * sizeof(double), cudaMemcpyHostToDevice, c->stream), "H2D radii");
+    CK(launch_psi4_modes(B, u, hi, d_r, nr, n_theta, n_phi, l_max, d_pts, d_modes, d_cnt, c->stream), "launch psi4");
+    CK(cudaMemcpyAsync(modes, d_modes, (size_t)nr * nm * sizeof(double2), cudaMemcpyDeviceToHost, c->stream),
+       "D2H modes");
+    std::vector<unsigned int> cnt(nr);
+    CK(cudaMemcpyAsync(cnt.data(), d_cnt, (size_t)nr * sizeof(unsigned int), cudaMemcpyDeviceToHost, c->stream),
+       "D2H counts");
+    CK(cudaStreamSynchronize(c->stream), "sync");
+    if (npoints)
+        for (int r = 0; r < nr; ++r) npoints[r] = (int)cnt[r];
+    c->launches += 2;
+    return GRANITE_OK;
+}
+
+}  // namespace
+
+int granite_ccz4_psi4_modes(void* h, int block_index, const double* radii, int nr, int n_theta, int n_phi, int l_max,
+                            double* modes, int* npoints) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (!c->committed) return fail(c, GRANITE_ERR_INVALID, "commit first");
+    if (block_index < 0 || block_index >= (int)c->descs.size()) return fail(c, GRANITE_ERR_INVALID, "bad block");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    const DevBlock& B = c->hblocks[block_index];
+    return psi4_run(c, B, B.buf[0], c->descs[block_index].hi, radii, nr, n_theta, n_phi, l_max, modes, npoints);
+}
+
+int granite_ccz4_psi4_modes_device(void* h, const granite_block_desc* b, const double* u_dev, const double* radii,
+                                   int nr, int n_theta, int n_phi, int l_max, double* modes, int* npoints) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    int r = check_desc(c, b);
+    if (r) return r;
+    if (!u_dev) return fail(c, GRANITE_ERR_INVALID, "null device buffer");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    return psi4_run(c, make_devblock(*b, c->p.ko_sigma), u_dev, b->hi, radii, nr, n_theta, n_phi, l_max, modes,
+                    npoints);
+}
+
+int granite_ccz4_psi4_modes_host(void* h, const granite_block_desc* b, const double* u, const double* radii, int nr,
+                                 int n_theta, int n_phi, int l_max, double* modes, int* npoints) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    int r = check_desc(c, b);
+    if (r) return r;
+    if (!u) return fail(c, GRANITE_ERR_INVALID, "null host buffer");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    const size_t N = (size_t)cells_of(*b);
+    if ((r = ensure_scratch(c, N, 1))) return r;
+    CK(cudaMemcpyAsync(c->s_u, u, N * NV * sizeof(double), cudaMemcpyHostToDevice, c->stream), "H2D u");
+    return granite_ccz4_psi4_modes_device(c, b, c->s_u, radii, nr, n_theta, n_phi, l_max, modes, npoints);
 }
 
 }  // extern "C"

@@ -142,6 +142,14 @@ struct MatterOut {
 };
 cudaError_t launch_matter_sources(const DevBlock& B, const double* prim, const MatterOut& out, cudaStream_t stream);
 
+// Psi4Extractor::extract (postprocess.cpp:245-314) on one block: modes[r * nm + q]
+// (q over l = 2..l_max, m = -l..l; nm = (l_max + 1)^2 - 4) at the nr radii (device
+// array); psi4_scratch holds nr * n_theta * n_phi values; inside_count[r] gets the
+// number of sphere points of radius r inside the block. hi: the block's upper corner.
+cudaError_t launch_psi4_modes(const DevBlock& B, const double* u, const double hi[3], const double* radii, int nr,
+                              int n_theta, int n_phi, int l_max, double2* psi4_scratch, double2* modes,
+                              unsigned int* inside_count, cudaStream_t stream);
+
 // Deterministic fixed-order sum of n partial pairs into out[2].
 cudaError_t launch_sum_partials(const double* partials, int n, double* out, cudaStream_t stream);
 

@@ -230,6 +230,27 @@ typedef int (*granite_regrid_fn)(void* user, int level, long long step_num);
 GRANITE_API int granite_ccz4_hierarchy_step_regrid(void* ctx, double dt_coarse, int precision, int amr_mode,
                                                    int regrid_interval, granite_regrid_fn fn, void* user);
 
+/* ---- gravitational-wave extraction ------------------------------------------
+ * Replaces Psi4Extractor::extract + getMode (postprocess.hpp:34-77,
+ * postprocess.cpp:245-326) on one block: modes[r][q][re, im] for the nr
+ * extraction radii (host array) and q over l = 2..l_max, m = -l..l
+ * ((l_max + 1)^2 - 4 modes), the sphere sampled at n_theta x n_phi points as
+ * GWExtractionParams describes, points within one cell of the block's faces
+ * skipped. Equal to the reference to rounding (sin, cos, pow are CUDA's; the
+ * sums run in a fixed tree order). The resident form reads state slot 0 of
+ * block_index, the device / host forms a caller's field-major block.
+ * npoints[r] (nullable) gets the number of sphere points of radius r inside
+ * the block: 0 means the reference records no mode for that radius. Blocks
+ * until the modes are on the host. 2 <= l_max <= 16. */
+GRANITE_API int granite_ccz4_psi4_modes(void* ctx, int block_index, const double* radii, int nr, int n_theta,
+                                        int n_phi, int l_max, double* modes, int* npoints);
+GRANITE_API int granite_ccz4_psi4_modes_device(void* ctx, const granite_block_desc* b, const double* u_dev,
+                                               const double* radii, int nr, int n_theta, int n_phi, int l_max,
+                                               double* modes, int* npoints);
+GRANITE_API int granite_ccz4_psi4_modes_host(void* ctx, const granite_block_desc* b, const double* u,
+                                             const double* radii, int nr, int n_theta, int n_phi, int l_max,
+                                             double* modes, int* npoints);
+
 /* ---- checkpoint / restart --------------------------------------------------
  * Replaces HDF5Writer::writeCheckpoint / HDF5Reader::readCheckpoint
  * (hdf5_io.cpp:166-233, 392-467) for the resident state, with their data model

@@ -162,6 +162,20 @@ class Oracle:
         self.lib.orc_matter_sources(C.byref(_cg(g)), _p(prim), _p(rho), _p(Si), _p(Sij), _p(S))
         return rho, Si, Sij, S
 
+    def psi4_modes(self, g: Geom, u, radii, n_theta: int, n_phi: int, l_max: int, counts: bool = False):
+        """Psi4Extractor::extract on one block (postprocess.cpp:245-314): complex
+        modes [len(radii), (l_max + 1)^2 - 4], l = 2..l_max, m = -l..l (and the
+        sphere points inside the block per radius when ``counts``)."""
+        nm = (l_max + 1) ** 2 - 4
+        out = np.zeros((len(radii), nm, 2))
+        r = np.ascontiguousarray(radii, dtype=np.float64)
+        hi = np.ascontiguousarray(g.hi, dtype=np.float64)
+        npts = (C.c_int * len(r))()
+        self.lib.orc_psi4_modes(C.byref(_cg(g)), _p(hi), _p(np.ascontiguousarray(u, dtype=np.float64)), _p(r),
+                                C.c_int(len(r)), C.c_int(n_theta), C.c_int(n_phi), C.c_int(l_max), _p(out), npts)
+        modes = out[..., 0] + 1j * out[..., 1]
+        return (modes, list(npts)) if counts else modes
+
     def constraint_sums(self, g: Geom, u):
         h2, m2, n = C.c_double(), C.c_double(), C.c_long()
         self.lib.orc_constraint_sums(C.byref(_cg(g)), _p(u), C.byref(h2), C.byref(m2),
@@ -296,6 +310,15 @@ class Reference:
         prim = np.ascontiguousarray(prim, dtype=np.float64)
         self.lib.ref_matter_sources(*self._g(g), _p(prim), _p(rho), _p(Si), _p(Sij), _p(S))
         return rho, Si, Sij, S
+
+    def psi4_modes(self, g: Geom, u, radii, n_theta: int, n_phi: int, l_max: int):
+        """The compiled Psi4Extractor::extract + getMode (postprocess.cpp:245-326)."""
+        nm = (l_max + 1) ** 2 - 4
+        out = np.zeros((len(radii), nm, 2))
+        r = np.ascontiguousarray(radii, dtype=np.float64)
+        self.lib.ref_psi4_modes(*self._g(g), _p(np.ascontiguousarray(u, dtype=np.float64)), _p(r), C.c_int(len(r)),
+                                C.c_int(n_theta), C.c_int(n_phi), C.c_int(l_max), _p(out))
+        return out[..., 0] + 1j * out[..., 1]
 
     def init_flat(self, g: Geom):
         u = g.zeros()

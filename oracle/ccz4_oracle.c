@@ -1162,3 +1162,149 @@ void orc_matter_sources(const orc_geom* g, const double* prim, double* rho, doub
                 S[c] = tr;
             }
 }
+
+/* ---------------------------------------------------------------------------
+ * Psi4 extraction, postprocess.cpp:61-99 (interp), :106-162 (spin-weight -2
+ * harmonics), :167-235 (Psi4 at a point), :245-314 (Psi4Extractor::extract).
+ * std::complex arithmetic is written out as GCC evaluates it for finite
+ * values: complex x complex = (ac - bd, ad + bc), complex x real and
+ * complex / real component-wise.
+ * ------------------------------------------------------------------------- */
+typedef struct { double re, im; } orc_cplx;
+
+static orc_cplx cmul(orc_cplx a, orc_cplx b) {
+    orc_cplx r = {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+    return r;
+}
+static orc_cplx cscale(orc_cplx a, double s) {
+    orc_cplx r = {a.re * s, a.im * s};
+    return r;
+}
+static orc_cplx cadd(orc_cplx a, orc_cplx b) {
+    orc_cplx r = {a.re + b.re, a.im + b.im};
+    return r;
+}
+
+static double pp_interp(const orc_geom* g, const double* u, int var, double px, double py, double pz) {
+    const int ng = g->ng, tx = tx_(g), ty = ty_(g), tz = tz_(g);
+    const long stride = orc_stride(g);
+    const double ix = (px - g->lo[0]) / g->dx[0] + ng - 0.5;
+    const double iy = (py - g->lo[1]) / g->dx[1] + ng - 0.5;
+    const double iz = (pz - g->lo[2]) / g->dx[2] + ng - 0.5;
+    const int nx = tx - 1, ny = ty - 1, nz = tz - 1;
+#define CLAMP(v, lo, hi) ((v) < (lo) ? (lo) : ((v) > (hi) ? (hi) : (v)))
+    const int i0 = CLAMP((int)floor(ix), 0, nx - 1), j0 = CLAMP((int)floor(iy), 0, ny - 1),
+              k0 = CLAMP((int)floor(iz), 0, nz - 1);
+#undef CLAMP
+    const int i1 = i0 + 1 < nx ? i0 + 1 : nx, j1 = j0 + 1 < ny ? j0 + 1 : ny, k1 = k0 + 1 < nz ? k0 + 1 : nz;
+    const double wx = ix - floor(ix), wy = iy - floor(iy), wz = iz - floor(iz);
+    const double* f = u + (long)var * stride;
+#define D(i, j, k) f[((i) < nx ? (i) : nx) + (long)tx * (((j) < ny ? (j) : ny) + (long)ty * ((k) < nz ? (k) : nz))]
+    return (1 - wz) * ((1 - wy) * ((1 - wx) * D(i0, j0, k0) + wx * D(i1, j0, k0)) +
+                       wy * ((1 - wx) * D(i0, j1, k0) + wx * D(i1, j1, k0))) +
+        wz * ((1 - wy) * ((1 - wx) * D(i0, j0, k1) + wx * D(i1, j0, k1)) +
+              wy * ((1 - wx) * D(i0, j1, k1) + wx * D(i1, j1, k1)));
+#undef D
+}
+
+#define ORC_PI 3.14159265358979323846
+
+/* -2 Y_lm: l = 2 all m, l = 3 m = +-3; zero otherwise (postprocess.cpp:106-162) */
+static orc_cplx sw_ylm(int l, int m, double theta, double phi) {
+    const double c2th = cos(theta / 2.0), s2th = sin(theta / 2.0);
+    orc_cplx e = {cos(m * phi), sin(m * phi)}, z = {0.0, 0.0};
+    if (l == 2) {
+        if (m == 2) return cscale(e, sqrt(5.0 / (4.0 * ORC_PI)) * pow(c2th, 4));
+        if (m == 1) return cscale(e, sqrt(5.0 / ORC_PI) * pow(c2th, 3) * s2th);
+        if (m == 0) {
+            orc_cplx r = {sqrt(15.0 / (2.0 * ORC_PI)) * pow(c2th, 2) * pow(s2th, 2), 0.0};
+            return r;
+        }
+        if (m == -1) return cscale(e, sqrt(5.0 / ORC_PI) * c2th * pow(s2th, 3));
+        if (m == -2) return cscale(e, sqrt(5.0 / (4.0 * ORC_PI)) * pow(s2th, 4));
+    }
+    if (l == 3) {
+        const double N33 = sqrt(21.0 / (2.0 * ORC_PI));
+        if (m == 3) return cscale(e, -N33 / 4.0 * pow(c2th, 5) * s2th / 2.0);
+        if (m == -3) return cscale(e, N33 / 4.0 * c2th * pow(s2th, 5) / 2.0);
+    }
+    return z;
+}
+
+static orc_cplx psi4_at(const orc_geom* g, const double* u, double px, double py, double pz, double nx, double ny,
+                        double nz) {
+    orc_cplx zero = {0.0, 0.0};
+    const double chi = pp_interp(g, u, CHI, px, py, pz);
+    if (chi < 1.0e-12) return zero;
+    const double rho = sqrt(nx * nx + ny * ny);
+    double tx, ty, tz, phx, phy, phz;
+    if (rho > 1.0e-10) {
+        tx = nx * nz / rho;
+        ty = ny * nz / rho;
+        tz = -rho;
+        phx = -ny / rho;
+        phy = nx / rho;
+        phz = 0.0;
+    } else {
+        tx = 1.0, ty = 0.0, tz = 0.0, phx = 0.0, phy = 1.0, phz = 0.0;
+    }
+    const double sqrt2 = sqrt(2.0);
+    const orc_cplx mx = {tx / sqrt2, -phx / sqrt2}, my = {ty / sqrt2, -phy / sqrt2}, mz = {tz / sqrt2, -phz / sqrt2};
+    const double fac = 1.0 / chi;
+    const double Bxx = pp_interp(g, u, AXX, px, py, pz) * fac, Bxy = pp_interp(g, u, AXY, px, py, pz) * fac,
+                 Bxz = pp_interp(g, u, AXZ, px, py, pz) * fac, Byy = pp_interp(g, u, AYY, px, py, pz) * fac,
+                 Byz = pp_interp(g, u, AYZ, px, py, pz) * fac, Bzz = pp_interp(g, u, AZZ, px, py, pz) * fac;
+    orc_cplx p = cmul(cscale(mx, Bxx), mx);
+    p = cadd(p, cmul(cscale(my, Byy), my));
+    p = cadd(p, cmul(cscale(mz, Bzz), mz));
+    p = cadd(p, cmul(cscale(mx, 2.0 * Bxy), my));
+    p = cadd(p, cmul(cscale(mx, 2.0 * Bxz), mz));
+    p = cadd(p, cmul(cscale(my, 2.0 * Byz), mz));
+    p.re = -p.re;
+    p.im = -p.im;
+    return p;
+}
+
+void orc_psi4_modes(const orc_geom* g, const double* hi, const double* u, const double* radii, int nr, int n_theta,
+                    int n_phi, int l_max, double* modes, int* npoints) {
+    const int nm = (l_max + 1) * (l_max + 1) - 4;
+    const double dth = ORC_PI / n_theta, dph = 2.0 * ORC_PI / n_phi;
+    for (int r = 0; r < nr; ++r) {
+        const double r_ext = radii[r];
+        double* out = modes + (long)r * nm * 2;
+        int* seen = (int*)calloc((size_t)nm, sizeof(int));
+        int inside = 0;
+        for (int q = 0; q < 2 * nm; ++q) out[q] = 0.0;
+        for (int it = 0; it < n_theta; ++it) {
+            const double theta = (it + 0.5) * dth, sth = sin(theta), cth = cos(theta);
+            for (int jp = 0; jp < n_phi; ++jp) {
+                const double phi = jp * dph, sph = sin(phi), cph = cos(phi);
+                const double px = r_ext * sth * cph, py = r_ext * sth * sph, pz = r_ext * cth;
+                const double nx = sth * cph, ny = sth * sph, nz = cth;
+                /* lowerCorner() + dx <= p <= upperCorner() - dx (postprocess.cpp:273-278) */
+                if (!(px >= g->lo[0] + g->dx[0] && px <= hi[0] - g->dx[0] && py >= g->lo[1] + g->dx[1] &&
+                      py <= hi[1] - g->dx[1] && pz >= g->lo[2] + g->dx[2] && pz <= hi[2] - g->dx[2]))
+                    continue;
+                ++inside;
+                const orc_cplx psi4 = psi4_at(g, u, px, py, pz, nx, ny, nz);
+                int q = 0;
+                for (int l = 2; l <= l_max; ++l)
+                    for (int m = -l; m <= l; ++m, ++q) {
+                        orc_cplx y = sw_ylm(l, m, theta, phi);
+                        y.im = -y.im;
+                        const orc_cplx c = cscale(cscale(cscale(cscale(cmul(psi4, y), sth), dth), dph), r_ext);
+                        if (seen[q]) {
+                            out[2 * q] += c.re;
+                            out[2 * q + 1] += c.im;
+                        } else {
+                            out[2 * q] = c.re;
+                            out[2 * q + 1] = c.im;
+                            seen[q] = 1;
+                        }
+                    }
+            }
+        }
+        if (npoints) npoints[r] = inside;
+        free(seen);
+    }
+}

@@ -100,6 +100,13 @@ void orc_constraint_sums(const orc_geom* g, const double* u, double* h2, double*
 void orc_matter_sources(const orc_geom* g, const double* prim, double* rho, double* Si, double* Sij,
                         double* S);
 
+/* Psi4Extractor::extract (postprocess.cpp:245-314) on one block at one time:
+ * modes[r][q][re, im] for extraction radius r and q over l = 2..l_max,
+ * m = -l..l; hi = the block's upper corner; npoints[r] (nullable) = the sphere
+ * points of radius r inside the block. */
+void orc_psi4_modes(const orc_geom* g, const double* hi, const double* u, const double* radii, int nr, int n_theta,
+                    int n_phi, int l_max, double* modes, int* npoints);
+
 /* OpenMP thread count used by the parallel loops (0 = leave default) */
 void orc_set_threads(int n);
 

@@ -2,8 +2,8 @@
 //
 // oracle/Makefile compiles this file together with the unmodified reference
 // sources src/spacetime/ccz4.cpp, src/core/grid.cpp, src/amr/amr.cpp,
-// src/initial_data/initial_data.cpp and src/grmhd/{grmhd,hlld,tabulated_eos}.cpp
-// into oracle/_ref/libgranite_ref_*.so.
+// src/initial_data/initial_data.cpp, src/grmhd/{grmhd,hlld,tabulated_eos}.cpp and
+// src/postprocess/postprocess.cpp into oracle/_ref/libgranite_ref_*.so.
 // The shim only copies flat buffers in and out of reference GridBlocks and
 // calls the reference's own operators; it adds no arithmetic of its own except
 // in ref_rk3_steps, whose main.cpp lambdas (combine, floors, algebraic
@@ -14,6 +14,7 @@
 #include "granite/amr/amr.hpp"
 #include "granite/core/grid.hpp"
 #include "granite/grmhd/grmhd.hpp"
+#include "granite/postprocess/postprocess.hpp"
 #include "granite/initial_data/initial_data.hpp"
 #include "granite/spacetime/ccz4.hpp"
 
@@ -183,6 +184,29 @@ void ref_matter_sources(const int* n, int ng, const double* lo, const double* hi
         for (int a = 0; a < 3; ++a) Si[3 * c + a] = si[c][a];
         for (int a = 0; a < 6; ++a) Sij[6 * c + a] = sij[c][a];
     }
+}
+
+// Psi4Extractor::extract at time 0 then getMode (postprocess.cpp:245-326):
+// modes[r][q][re, im], q over l = 2..l_max, m = -l..l.
+void ref_psi4_modes(const int* n, int ng, const double* lo, const double* hi, const double* u, const double* radii,
+                    int nr, int n_theta, int n_phi, int l_max, double* modes) {
+    auto b = block(geo(n, ng, lo, hi));
+    std::memcpy(b->flatBuffer(), u, nbytes(*b));
+    postprocess::GWExtractionParams gp;
+    gp.extraction_radii.assign(radii, radii + nr);
+    gp.l_max = l_max;
+    gp.n_theta = n_theta;
+    gp.n_phi = n_phi;
+    postprocess::Psi4Extractor ex(gp);
+    ex.extract(*b, 0.0);
+    int q = 0;
+    for (int r = 0; r < nr; ++r)
+        for (int l = 2; l <= l_max; ++l)
+            for (int m = -l; m <= l; ++m, ++q) {
+                const std::complex<Real> v = ex.getMode(l, m, radii[r]);
+                modes[2 * q] = v.real();
+                modes[2 * q + 1] = v.imag();
+            }
 }
 
 // setFlatSpacetime / setGaugeWaveData (ccz4.cpp:1165-1221) on a zeroed block.

@@ -93,6 +93,12 @@ def main():
     cases["matter_sources"] = (G_RAND, dict(rho=rho[it], Si=Si[it], Sij=Sij[it], S=S[it], seed=41,
                                             superluminal=0.05))
 
+    gp = Geom((24, 20, 22), (-12.0, -10.0, -11.0), (12.0, 10.0, 11.0))
+    up = oracle.seeded_state(gp, 51)
+    radii = np.array([3.0, 6.5, 9.7, 10.5, 20.0])
+    modes = ref.psi4_modes(gp, up, radii, 16, 32, 4)
+    cases["psi4_modes"] = (gp, dict(modes=modes, radii=radii, seed=51, n_theta=16, n_phi=32, l_max=4))
+
     for name, (g, data) in cases.items():
         path = os.path.join(OUT, f"{name}.npz")
         np.savez_compressed(path, **geom_dict(g), **data)

@@ -36,7 +36,7 @@ def test_golden_files_present():
     names = {os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLD, "*.npz"))}
     for n in ["rhs_random", "rhs_matter", "rhs_random_noko", "constraints_random", "ko_random",
               "rhs_bl", "constraints_bl", "rk3_bl_3steps", "init_bl", "init_gauge_wave",
-              "rk3_gauge_wave_periodic_4steps", "prolong", "restrict", "matter_sources"]:
+              "rk3_gauge_wave_periodic_4steps", "prolong", "restrict", "matter_sources", "psi4_modes"]:
         assert n in names, n
 
 
@@ -80,6 +80,29 @@ def test_oracle_matter_sources_vs_reference(oracle_lib, seed, superluminal):
     init = tuple(oracle.hash_noise(a.shape, 90 + k) for k, a in enumerate(oracle.matter_zeros(g)))
     for a, b in zip(oracle_lib.matter_sources(g, prim, init), ref.matter_sources(g, prim, init)):
         assert np.array_equal(a, b)
+
+
+def test_oracle_psi4_golden(oracle_lib):
+    """Psi4Extractor::extract + getMode (postprocess.cpp:245-326) on a seeded block,
+    radii fully inside, partly inside and outside it."""
+    g, z = load("psi4_modes")
+    u = oracle.seeded_state(g, int(z["seed"]))
+    got, npts = oracle_lib.psi4_modes(g, u, z["radii"], int(z["n_theta"]), int(z["n_phi"]), int(z["l_max"]),
+                                      counts=True)
+    assert np.array_equal(got, z["modes"])
+    full = int(z["n_theta"]) * int(z["n_phi"])
+    assert npts[0] == full and 0 < npts[3] < full and npts[-1] == 0
+
+
+@pytest.mark.skipif(not oracle.reference_available("strict"), reason="reference library not built")
+@pytest.mark.parametrize("l_max,nth,nph", [(2, 8, 12), (5, 21, 17)])
+def test_oracle_psi4_vs_reference(oracle_lib, l_max, nth, nph):
+    ref = oracle.Reference("strict")
+    g = Geom((20, 18, 16), (-5.0, -4.5, -4.0), (5.0, 4.5, 4.0))
+    u = oracle.seeded_state(g, 8)
+    radii = [1.0, 2.5, 4.2]
+    assert np.array_equal(oracle_lib.psi4_modes(g, u, radii, nth, nph, l_max),
+                          ref.psi4_modes(g, u, radii, nth, nph, l_max))
 
 
 def test_oracle_constraints_golden(oracle_lib):
