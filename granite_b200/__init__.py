@@ -50,6 +50,17 @@ class _Params(C.Structure):
                 ("chi_blend_width", C.c_double), ("fd_order", C.c_int), ("device", C.c_int)]
 
 
+class _HorizonParams(C.Structure):
+    _fields_ = [("max_iterations", C.c_int), ("tolerance", C.c_double), ("angular_resolution", C.c_int),
+                ("initial_guess_radius", C.c_double)]
+
+
+class _Horizon(C.Structure):
+    _fields_ = [("found", C.c_int), ("iterations", C.c_int), ("id", C.c_int), ("centroid", C.c_double * 3),
+                ("area", C.c_double), ("irreducible_mass", C.c_double), ("spin", C.c_double),
+                ("circumference_equatorial", C.c_double), ("circumference_polar", C.c_double)]
+
+
 class _BlockDesc(C.Structure):
     _fields_ = [("ncells", C.c_int * 3), ("nghost", C.c_int), ("lo", C.c_double * 3),
                 ("hi", C.c_double * 3), ("level", C.c_int), ("id", C.c_int)]
@@ -113,6 +124,12 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_get_fp64_chi_threshold.argtypes = [vp, C.POINTER(C.c_double)]
     lib.granite_ccz4_regrid_add.argtypes = [vp, C.POINTER(_BlockDesc), C.c_int]
     ip = C.POINTER(C.c_int)
+    hp = C.POINTER(_HorizonParams)
+    lib.granite_ccz4_default_horizon_params.argtypes = [hp]
+    lib.granite_ccz4_default_horizon_params.restype = None
+    lib.granite_ccz4_find_horizon.argtypes = [vp, C.c_int, hp, dp, C.POINTER(_Horizon), dp]
+    lib.granite_ccz4_find_horizon_host.argtypes = [vp, C.POINTER(_BlockDesc), dp, hp, dp, C.POINTER(_Horizon), dp]
+    lib.granite_ccz4_find_all_horizons.argtypes = [vp, C.c_int, hp, C.POINTER(_Horizon), C.c_int, ip]
     lib.granite_ccz4_psi4_modes.argtypes = [vp, C.c_int, dp, C.c_int, C.c_int, C.c_int, C.c_int, dp, ip]
     lib.granite_ccz4_psi4_modes_host.argtypes = [vp, C.POINTER(_BlockDesc), dp, dp, C.c_int, C.c_int, C.c_int,
                                                  C.c_int, dp, ip]

@@ -2129,4 +2129,219 @@ int granite_ccz4_psi4_modes_host(void* h, const granite_block_desc* b, const dou
     return granite_ccz4_psi4_modes_device(c, b, c->s_u, radii, nr, n_theta, n_phi, l_max, modes, npoints);
 }
 
+// ---------------------------------------------------------------------------
+// Apparent horizons (ApparentHorizonFinder, horizon_finder.cpp:310-507)
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr double HZ_PI = 3.14159265358979323846;  // constants::PI
+constexpr int HZ_CHUNK = 16;                      // flow iterations per launch
+constexpr unsigned int HZ_MAX_CANDIDATES = 65536;
+
+// the next 256-byte aligned piece of `bytes` bytes of a scratch area
+char* carve(char*& p, size_t bytes) {
+    char* r = p;
+    p += (bytes + 255) / 256 * 256;
+    return r;
+}
+
+int diag_scratch(Ctx* c, size_t need) {
+    if (need > c->s_diag_bytes) {
+        cudaFree(c->s_diag);
+        c->s_diag = nullptr;
+        c->s_diag_bytes = 0;
+        CK(cudaMalloc(&c->s_diag, need), "cudaMalloc(diagnostics scratch)");
+        c->s_diag_bytes = need;
+    }
+    return GRANITE_OK;
+}
+
+int horizon_run(Ctx* c, const DevBlock& B, const double* u, const granite_horizon_params* p, const double* center,
+                granite_horizon* out, double* radii_out) {
+    if (!p || !center || !out) return fail(c, GRANITE_ERR_INVALID, "horizon: null argument");
+    if (p->angular_resolution <= 0 || p->angular_resolution > 2048 || p->max_iterations < 0)
+        return fail(c, GRANITE_ERR_INVALID, "horizon: 0 < angular_resolution <= 2048, max_iterations >= 0");
+    const int nth = p->angular_resolution, nph = 2 * nth, N = nth * nph;
+    HorizonArgs a;
+    for (int d = 0; d < 3; ++d) a.center[d] = center[d];
+    const double h_grid = B.dx[0];
+    a.flow_step = 0.05 * h_grid;
+    a.rmin = 1.0e-6 * h_grid;
+    a.dth = HZ_PI / nth;
+    a.dph = 2.0 * HZ_PI / nph;
+    a.nth = nth;
+    a.nph = nph;
+    // angular tables from the host libm, as buildAngularGrid + std::sin / std::cos
+    std::vector<double> tab(2 * nth + 2 * nph);
+    for (int i = 0; i < nth; ++i) {
+        const double th = HZ_PI * (i + 0.5) / nth;
+        tab[i] = std::sin(th);
+        tab[nth + i] = std::cos(th);
+    }
+    for (int j = 0; j < nph; ++j) {
+        const double ph = 2.0 * HZ_PI * j / nph;
+        tab[2 * nth + j] = std::sin(ph);
+        tab[2 * nth + nph + j] = std::cos(ph);
+    }
+    const size_t need = 4 * 256 + (tab.size() + (size_t)N + (size_t)HZ_CHUNK * N + 3 * (size_t)N + HZ_CHUNK) * 8;
+    int r = diag_scratch(c, need);
+    if (r) return r;
+    char* q = c->s_diag;
+    double* d_tab = reinterpret_cast<double*>(carve(q, tab.size() * 8));
+    double* d_h = reinterpret_cast<double*>(carve(q, (size_t)N * 8));
+    double* d_hist = reinterpret_cast<double*>(carve(q, (size_t)HZ_CHUNK * N * 8));
+    double* d_terms = reinterpret_cast<double*>(carve(q, 3 * (size_t)N * 8));
+    unsigned long long* d_itmax = reinterpret_cast<unsigned long long*>(carve(q, HZ_CHUNK * 8));
+    std::vector<double> h(N, p->initial_guess_radius);
+    CK(cudaMemcpyAsync(d_tab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, c->stream), "H2D tables");
+    CK(cudaMemcpyAsync(d_h, h.data(), (size_t)N * 8, cudaMemcpyHostToDevice, c->stream), "H2D radii");
+    int converged = -1, done = 0;
+    while (done < p->max_iterations && converged < 0) {
+        const int it = std::min(HZ_CHUNK, p->max_iterations - done);
+        CK(launch_horizon_flow(B, u, a, d_tab, d_h, it, d_hist, d_itmax, c->stream), "launch horizon flow");
+        unsigned long long mx[HZ_CHUNK];
+        CK(cudaMemcpyAsync(mx, d_itmax, it * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream),
+           "D2H flow maxima");
+        CK(cudaStreamSynchronize(c->stream), "sync");
+        c->launches += 1;
+        for (int k = 0; k < it && converged < 0; ++k) {
+            double v;
+            std::memcpy(&v, &mx[k], 8);
+            if (v < p->tolerance) {  // the radii of this iteration are the result
+                converged = done + k + 1;
+                CK(cudaMemcpyAsync(d_h, d_hist + (size_t)k * N, (size_t)N * 8, cudaMemcpyDeviceToDevice, c->stream),
+                   "converged radii");
+            }
+        }
+        done += it;
+    }
+    *out = granite_horizon{};
+    out->iterations = converged > 0 ? converged : done;
+    for (int d = 0; d < 3; ++d) out->centroid[d] = center[d];
+    CK(cudaMemcpyAsync(h.data(), d_h, (size_t)N * 8, cudaMemcpyDeviceToHost, c->stream), "D2H radii");
+    CK(cudaStreamSynchronize(c->stream), "sync");
+    if (radii_out) std::copy(h.begin(), h.end(), radii_out);
+    if (converged < 0) {
+        for (int d = 0; d < 3; ++d) out->centroid[d] = 0.0;
+        return GRANITE_OK;
+    }
+    std::vector<double> terms(3 * (size_t)N);
+    CK(launch_horizon_surface(B, u, a, d_tab, d_h, d_terms, c->stream), "launch horizon surface");
+    CK(cudaMemcpyAsync(terms.data(), d_terms, terms.size() * 8, cudaMemcpyDeviceToHost, c->stream), "D2H terms");
+    CK(cudaStreamSynchronize(c->stream), "sync");
+    c->launches += 1;
+    double area = 0.0, jz = 0.0;  // sums in the reference's point order
+    for (int k = 0; k < N; ++k)
+        if (terms[3 * k + 2] != 0.0) {
+            area += terms[3 * k];
+            jz += terms[3 * k + 1];
+        }
+    out->found = 1;
+    out->area = area;
+    out->irreducible_mass = std::sqrt(area / (16.0 * HZ_PI));
+    double ceq = 0.0, cpol = 0.0;
+    for (int j = 0; j < nph; ++j) ceq += h[(size_t)(nth / 2) * nph + j] * a.dph;
+    for (int i = 0; i < nth; ++i) cpol += h[(size_t)i * nph] * a.dth;
+    out->circumference_equatorial = ceq;
+    out->circumference_polar = 2.0 * cpol;
+    const double m = out->irreducible_mass;
+    const double spin = m > 1.0e-12 ? jz / (m * m) : 0.0;
+    out->spin = std::clamp(spin, -1.0, 1.0);
+    return GRANITE_OK;
+}
+
+}  // namespace
+
+void granite_ccz4_default_horizon_params(granite_horizon_params* p) {
+    if (!p) return;
+    p->max_iterations = 200;
+    p->tolerance = 1.0e-10;
+    p->angular_resolution = 50;
+    p->initial_guess_radius = 1.0;
+}
+
+int granite_ccz4_find_horizon(void* h, int block_index, const granite_horizon_params* p, const double* center,
+                              granite_horizon* out, double* radii) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (!c->committed) return fail(c, GRANITE_ERR_INVALID, "commit first");
+    if (block_index < 0 || block_index >= (int)c->descs.size()) return fail(c, GRANITE_ERR_INVALID, "bad block");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    const DevBlock& B = c->hblocks[block_index];
+    return horizon_run(c, B, B.buf[0], p, center, out, radii);
+}
+
+int granite_ccz4_find_horizon_host(void* h, const granite_block_desc* b, const double* u,
+                                   const granite_horizon_params* p, const double* center, granite_horizon* out,
+                                   double* radii) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    int r = check_desc(c, b);
+    if (r) return r;
+    if (!u) return fail(c, GRANITE_ERR_INVALID, "null host buffer");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    const size_t N = (size_t)cells_of(*b);
+    if ((r = ensure_scratch(c, N, 1))) return r;
+    CK(cudaMemcpyAsync(c->s_u, u, N * NV * sizeof(double), cudaMemcpyHostToDevice, c->stream), "H2D u");
+    DevBlock B = make_devblock(*b, c->p.ko_sigma);
+    B.buf[0] = c->s_u;
+    return horizon_run(c, B, c->s_u, p, center, out, radii);
+}
+
+int granite_ccz4_find_all_horizons(void* h, int block_index, const granite_horizon_params* p, granite_horizon* out,
+                                   int cap, int* n) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (!c->committed) return fail(c, GRANITE_ERR_INVALID, "commit first");
+    if (block_index < 0 || block_index >= (int)c->descs.size()) return fail(c, GRANITE_ERR_INVALID, "bad block");
+    if (!p || !n || cap < 0 || (cap > 0 && !out)) return fail(c, GRANITE_ERR_INVALID, "horizon: null argument");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    const DevBlock& B = c->hblocks[block_index];
+    const granite_block_desc& d = c->descs[block_index];
+    // candidate scan: indices, then count, in a scratch of their own (the flow reuses the diagnostics scratch)
+    long long* d_idx = nullptr;
+    CK(cudaMalloc(&d_idx, HZ_MAX_CANDIDATES * sizeof(long long) + 256), "cudaMalloc(candidates)");
+    unsigned int* d_cnt = reinterpret_cast<unsigned int*>(d_idx + HZ_MAX_CANDIDATES);
+    cudaError_t e = launch_lapse_minima(B, B.buf[0], d_idx, d_cnt, HZ_MAX_CANDIDATES, c->stream);
+    unsigned int cnt = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    std::vector<long long> idx(std::min(cnt, HZ_MAX_CANDIDATES));
+    if (e == cudaSuccess && !idx.empty())
+        e = cudaMemcpy(idx.data(), d_idx, idx.size() * sizeof(long long), cudaMemcpyDeviceToHost);
+    cudaFree(d_idx);
+    if (e != cudaSuccess) return cuda_fail(c, e, "lapse minima");
+    if (cnt > HZ_MAX_CANDIDATES) return fail(c, GRANITE_ERR_TOO_LARGE, "horizon: more than 65536 lapse minima");
+    c->launches += 1;
+    std::sort(idx.begin(), idx.end());  // the reference's k, j, i scan order
+    const double min_sep = 2.0 * p->initial_guess_radius;
+    std::vector<std::array<double, 3>> uniq;
+    for (long long ci : idx) {
+        const int i = (int)(ci % B.tx), j = (int)((ci / B.tx) % B.ty), k = (int)(ci / ((long long)B.tx * B.ty));
+        const std::array<double, 3> x = {xref(d, 0, i), xref(d, 1, j), xref(d, 2, k)};
+        bool dup = false;
+        for (const auto& w : uniq) {
+            const double d2 = (x[0] - w[0]) * (x[0] - w[0]) + (x[1] - w[1]) * (x[1] - w[1]) +
+                (x[2] - w[2]) * (x[2] - w[2]);
+            if (d2 < min_sep * min_sep) {
+                dup = true;
+                break;
+            }
+        }
+        if (!dup) uniq.push_back(x);
+    }
+    int found = 0;
+    for (const auto& ctr : uniq) {
+        granite_horizon hz;
+        int r = horizon_run(c, B, B.buf[0], p, ctr.data(), &hz, nullptr);
+        if (r) return r;
+        if (!hz.found) continue;
+        hz.id = found;
+        if (found < cap) out[found] = hz;
+        ++found;
+    }
+    *n = found;
+    return GRANITE_OK;
+}
+
 }  // extern "C"

@@ -150,6 +150,28 @@ cudaError_t launch_psi4_modes(const DevBlock& B, const double* u, const double h
                               int n_theta, int n_phi, int l_max, double2* psi4_scratch, double2* modes,
                               unsigned int* inside_count, cudaStream_t stream);
 
+// Apparent-horizon flow (horizon_finder.cpp:310-449) on one block. tab holds
+// sin(theta_i), cos(theta_i) (nth each), sin(phi_j), cos(phi_j) (nph each),
+// evaluated by the host's libm.
+struct HorizonArgs {
+    double center[3];
+    double flow_step, rmin;  // 0.05 dx and 1e-6 dx
+    double dth, dph;         // pi / nth, 2 pi / nph
+    int nth, nph;
+};
+// iters flow iterations of every surface point from the radii h (updated in
+// place): radii after iteration k at hist[k * N + p], max |Theta| of iteration k
+// as the bits of a non-negative double in itmax[k] (zeroed here).
+cudaError_t launch_horizon_flow(const DevBlock& B, const double* u, const HorizonArgs& a, const double* tab,
+                                double* h, int iters, double* hist, unsigned long long* itmax, cudaStream_t stream);
+// terms[3 p ..] = area term, J_z term, 1 (0 where chi < 1e-12) of surface point p.
+cudaError_t launch_horizon_surface(const DevBlock& B, const double* u, const HorizonArgs& a, const double* tab,
+                                   const double* h, double* terms, cudaStream_t stream);
+// findAllHorizons' candidate cells (lapse minima below 0.5), up to cap cell indices
+// in arbitrary order; *count = all found.
+cudaError_t launch_lapse_minima(const DevBlock& B, const double* u, long long* out, unsigned int* count,
+                                unsigned int cap, cudaStream_t stream);
+
 // Deterministic fixed-order sum of n partial pairs into out[2].
 cudaError_t launch_sum_partials(const double* partials, int n, double* out, cudaStream_t stream);
 

@@ -251,6 +251,47 @@ GRANITE_API int granite_ccz4_psi4_modes_host(void* ctx, const granite_block_desc
                                              const double* radii, int nr, int n_theta, int n_phi, int l_max,
                                              double* modes, int* npoints);
 
+/* ---- apparent horizons ------------------------------------------------------
+ * HorizonParams and the HorizonData fields the finder fills
+ * (horizon_finder.hpp:17-41); spin_axis is always z there, surface points are
+ * center + radii[i][j] * (sin t_i cos p_j, sin t_i sin p_j, cos t_i) with
+ * t_i = pi (i + 1/2) / n, p_j = 2 pi j / (2 n), n = angular_resolution. */
+typedef struct {
+    int max_iterations;          /* 200 */
+    double tolerance;            /* 1e-10 */
+    int angular_resolution;      /* 50 theta points; 2x as many phi points */
+    double initial_guess_radius; /* 1.0 */
+} granite_horizon_params;
+
+typedef struct {
+    int found;      /* 1: the flow converged (otherwise the other fields are 0) */
+    int iterations; /* flow iterations run */
+    int id;
+    double centroid[3];
+    double area, irreducible_mass, spin;
+    double circumference_equatorial, circumference_polar;
+} granite_horizon;
+
+GRANITE_API void granite_ccz4_default_horizon_params(granite_horizon_params* p);
+/* Replaces ApparentHorizonFinder::findHorizon (horizon_finder.cpp:310-449) on
+ * resident block block_index: the expansion flow from a sphere of the initial
+ * radius about center, on the GPU, equal to the reference bit for bit (the
+ * surface integrals are summed on the host in its order). radii (nullable,
+ * n x 2n) receives the final surface, also when the flow did not converge. */
+GRANITE_API int granite_ccz4_find_horizon(void* ctx, int block_index, const granite_horizon_params* p,
+                                          const double* center, granite_horizon* out, double* radii);
+/* The same on a caller's host block (copied to the GPU first). */
+GRANITE_API int granite_ccz4_find_horizon_host(void* ctx, const granite_block_desc* b, const double* u,
+                                               const granite_horizon_params* p, const double* center,
+                                               granite_horizon* out, double* radii);
+/* Replaces findAllHorizons (horizon_finder.cpp:452-507): candidate centres at
+ * lapse minima below 0.5 (scan on the GPU, cells two in from the faces, in the
+ * reference's order, at most 65536), those within 2 initial radii of an
+ * earlier one dropped, then findHorizon from each; found horizons get ids
+ * 0, 1, ... in order. Writes min(found, cap) to out, *n = found. */
+GRANITE_API int granite_ccz4_find_all_horizons(void* ctx, int block_index, const granite_horizon_params* p,
+                                               granite_horizon* out, int cap, int* n);
+
 /* ---- checkpoint / restart --------------------------------------------------
  * Replaces HDF5Writer::writeCheckpoint / HDF5Reader::readCheckpoint
  * (hdf5_io.cpp:166-233, 392-467) for the resident state, with their data model

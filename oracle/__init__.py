@@ -176,6 +176,22 @@ class Oracle:
         modes = out[..., 0] + 1j * out[..., 1]
         return (modes, list(npts)) if counts else modes
 
+    def find_horizon(self, g: Geom, u, center, max_iterations=200, tol=1e-10, ang_res=50, init_r=1.0):
+        """findHorizon's flow and surface integrals (horizon_finder.cpp:310-449):
+        (iterations or -1, h[ang_res, 2 ang_res], [area, M_irr, spin, C_eq, C_pol])."""
+        h = np.full((ang_res, 2 * ang_res), float(init_r))
+        res = np.zeros(5)
+        self.lib.orc_find_horizon.restype = C.c_int
+        it = self.lib.orc_find_horizon(C.byref(_cg(g)), _p(np.ascontiguousarray(u, dtype=np.float64)),
+                                       _p(np.ascontiguousarray(center, dtype=np.float64)), C.c_int(max_iterations),
+                                       C.c_double(tol), C.c_int(ang_res), _p(h), _p(res))
+        return it, h, res
+
+    def horizon_expansion(self, g: Geom, u, p, n):
+        self.lib.orc_horizon_expansion.restype = C.c_double
+        return self.lib.orc_horizon_expansion(C.byref(_cg(g)), _p(np.ascontiguousarray(u, dtype=np.float64)),
+                                              *[C.c_double(x) for x in (*p, *n)])
+
     def constraint_sums(self, g: Geom, u):
         h2, m2, n = C.c_double(), C.c_double(), C.c_long()
         self.lib.orc_constraint_sums(C.byref(_cg(g)), _p(u), C.byref(h2), C.byref(m2),
@@ -319,6 +335,24 @@ class Reference:
         self.lib.ref_psi4_modes(*self._g(g), _p(np.ascontiguousarray(u, dtype=np.float64)), _p(r), C.c_int(len(r)),
                                 C.c_int(n_theta), C.c_int(n_phi), C.c_int(l_max), _p(out))
         return out[..., 0] + 1j * out[..., 1]
+
+    def find_horizon(self, g: Geom, u, center, max_iterations=200, tol=1e-10, ang_res=50, init_r=1.0):
+        """The compiled ApparentHorizonFinder::findHorizon: (found, [area, M_irr, spin,
+        C_eq, C_pol], surface points [ang_res * 2 ang_res, 3])."""
+        res = np.zeros(5)
+        surf = np.zeros((ang_res * 2 * ang_res, 3))
+        found = self.lib.ref_find_horizon(*self._g(g), _p(np.ascontiguousarray(u, dtype=np.float64)),
+                                          _p(np.ascontiguousarray(center, dtype=np.float64)), C.c_int(max_iterations),
+                                          C.c_double(tol), C.c_int(ang_res), C.c_double(init_r), _p(res), _p(surf))
+        return bool(found), res, surf
+
+    def find_all_horizons(self, g: Geom, u, max_iterations=200, tol=1e-10, ang_res=50, init_r=1.0, cap=16):
+        """The compiled findAllHorizons: rows (cx, cy, cz, area, M_irr, spin)."""
+        out = np.zeros((cap, 6))
+        n = self.lib.ref_find_all_horizons(*self._g(g), _p(np.ascontiguousarray(u, dtype=np.float64)),
+                                           C.c_int(max_iterations), C.c_double(tol), C.c_int(ang_res),
+                                           C.c_double(init_r), _p(out), C.c_int(cap))
+        return out[:min(n, cap)]
 
     def init_flat(self, g: Geom):
         u = g.zeros()

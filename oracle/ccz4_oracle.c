@@ -1308,3 +1308,151 @@ void orc_psi4_modes(const orc_geom* g, const double* hi, const double* u, const 
         free(seen);
     }
 }
+
+/* ---------------------------------------------------------------------------
+ * Apparent-horizon flow, horizon_finder.cpp:55-98 (interpolate, indices
+ * clamped per access), :114-281 (computeExpansion), :292-300 (angular grid),
+ * :310-449 (findHorizon), :452-507 (findAllHorizons scan).
+ * ------------------------------------------------------------------------- */
+static double hz_interp(const orc_geom* g, const double* u, int var, double px, double py, double pz) {
+    const int ng = g->ng, tx = tx_(g), ty = ty_(g), tz = tz_(g);
+    const double ix = (px - g->lo[0]) / g->dx[0] + ng - 0.5;
+    const double iy = (py - g->lo[1]) / g->dx[1] + ng - 0.5;
+    const double iz = (pz - g->lo[2]) / g->dx[2] + ng - 0.5;
+    const int i0 = (int)floor(ix), j0 = (int)floor(iy), k0 = (int)floor(iz);
+    const int nx = tx - 1, ny = ty - 1, nz = tz - 1;
+    const int i1 = i0 + 1 < nx ? i0 + 1 : nx, j1 = j0 + 1 < ny ? j0 + 1 : ny, k1 = k0 + 1 < nz ? k0 + 1 : nz;
+    const double wx = ix - floor(ix), wy = iy - floor(iy), wz = iz - floor(iz);
+    const double* f = u + (long)var * orc_stride(g);
+#define CL(v, n) ((v) < (n) ? ((v) > 0 ? (v) : 0) : ((n) > 0 ? (n) : 0))
+#define D(i, j, k) f[CL(i, nx) + (long)tx * (CL(j, ny) + (long)ty * CL(k, nz))]
+    return (1 - wz) * ((1 - wy) * ((1 - wx) * D(i0, j0, k0) + wx * D(i1, j0, k0)) +
+                       wy * ((1 - wx) * D(i0, j1, k0) + wx * D(i1, j1, k0))) +
+        wz * ((1 - wy) * ((1 - wx) * D(i0, j0, k1) + wx * D(i1, j0, k1)) +
+              wy * ((1 - wx) * D(i0, j1, k1) + wx * D(i1, j1, k1)));
+#undef D
+#undef CL
+}
+
+/* component dir of the unit normal s^i at a displaced point (the scomp lambda) */
+static double hz_scomp(const orc_geom* g, const double* u, double px, double py, double pz, double snx, double sny,
+                       double snz, int dir, double delta) {
+    const double ppx = px + (dir == 0 ? delta : 0.0), ppy = py + (dir == 1 ? delta : 0.0),
+                 ppz = pz + (dir == 2 ? delta : 0.0);
+    const double chi = hz_interp(g, u, CHI, ppx, ppy, ppz);
+    if (chi < 1.0e-12) return 0.0;
+    const double gxx = hz_interp(g, u, GXX, ppx, ppy, ppz), gxy = hz_interp(g, u, GXY, ppx, ppy, ppz),
+                 gxz = hz_interp(g, u, GXZ, ppx, ppy, ppz), gyy = hz_interp(g, u, GYY, ppx, ppy, ppz),
+                 gyz = hz_interp(g, u, GYZ, ppx, ppy, ppz), gzz = hz_interp(g, u, GZZ, ppx, ppy, ppz);
+    const double det = gxx * (gyy * gzz - gyz * gyz) - gxy * (gxy * gzz - gyz * gxz) + gxz * (gxy * gyz - gyy * gxz);
+    if (fabs(det) < 1.0e-14) return 0.0;
+    const double idet = 1.0 / det;
+    const double igxx = (gyy * gzz - gyz * gyz) * idet, igxy = (gxz * gyz - gxy * gzz) * idet,
+                 igxz = (gxy * gyz - gxz * gyy) * idet, igyy = (gxx * gzz - gxz * gxz) * idet,
+                 igyz = (gxy * gxz - gxx * gyz) * idet, igzz = (gxx * gyy - gxy * gxy) * idet;
+    const double hxx = gxx / chi, hxy = gxy / chi, hxz = gxz / chi, hyy = gyy / chi, hyz = gyz / chi, hzz = gzz / chi;
+    const double sx = hxx * snx + hxy * sny + hxz * snz, sy = hxy * snx + hyy * sny + hyz * snz,
+                 sz = hxz * snx + hyz * sny + hzz * snz;
+    const double n2 = snx * sx + sny * sy + snz * sz;
+    if (n2 < 1.0e-14) return 0.0;
+    const double nm = sqrt(n2);
+    const double ixx = chi * igxx, ixy = chi * igxy, ixz = chi * igxz, iyy = chi * igyy, iyz = chi * igyz,
+                 izz = chi * igzz;
+    if (dir == 0) return (ixx * sx + ixy * sy + ixz * sz) / nm;
+    if (dir == 1) return (ixy * sx + iyy * sy + iyz * sz) / nm;
+    return (ixz * sx + iyz * sy + izz * sz) / nm;
+}
+
+double orc_horizon_expansion(const orc_geom* g, const double* u, double px, double py, double pz, double snx,
+                             double sny, double snz) {
+    const double chi = hz_interp(g, u, CHI, px, py, pz);
+    const double gxx = hz_interp(g, u, GXX, px, py, pz), gxy = hz_interp(g, u, GXY, px, py, pz),
+                 gxz = hz_interp(g, u, GXZ, px, py, pz), gyy = hz_interp(g, u, GYY, px, py, pz),
+                 gyz = hz_interp(g, u, GYZ, px, py, pz), gzz = hz_interp(g, u, GZZ, px, py, pz);
+    const double Axx = hz_interp(g, u, AXX, px, py, pz), Axy = hz_interp(g, u, AXY, px, py, pz),
+                 Axz = hz_interp(g, u, AXZ, px, py, pz), Ayy = hz_interp(g, u, AYY, px, py, pz),
+                 Ayz = hz_interp(g, u, AYZ, px, py, pz), Azz = hz_interp(g, u, AZZ, px, py, pz);
+    const double K = hz_interp(g, u, KTR, px, py, pz);
+    if (chi < 1.0e-12) return 0.0;
+    const double hxx = gxx / chi, hxy = gxy / chi, hxz = gxz / chi, hyy = gyy / chi, hyz = gyz / chi, hzz = gzz / chi;
+    const double det = gxx * (gyy * gzz - gyz * gyz) - gxy * (gxy * gzz - gyz * gxz) + gxz * (gxy * gyz - gyy * gxz);
+    if (fabs(det) < 1.0e-14) return 0.0;
+    const double sx = hxx * snx + hxy * sny + hxz * snz, sy = hxy * snx + hyy * sny + hyz * snz,
+                 sz = hxz * snx + hyz * sny + hzz * snz;
+    const double norm2 = snx * sx + sny * sy + snz * sz;
+    if (norm2 < 1.0e-14) return 0.0;
+    const double norm = sqrt(norm2);
+    const double ux = snx / norm, uy = sny / norm, uz = snz / norm;
+    const double Kxx = (Axx + gxx * K / 3.0) / chi, Kxy = (Axy + gxy * K / 3.0) / chi, Kxz = (Axz + gxz * K / 3.0) / chi,
+                 Kyy = (Ayy + gyy * K / 3.0) / chi, Kyz = (Ayz + gyz * K / 3.0) / chi, Kzz = (Azz + gzz * K / 3.0) / chi;
+    const double Kss = Kxx * ux * ux + Kyy * uy * uy + Kzz * uz * uz +
+        2.0 * (Kxy * ux * uy + Kxz * ux * uz + Kyz * uy * uz);
+    const double eps = g->dx[0];
+#define SC(d, e) hz_scomp(g, u, px, py, pz, snx, sny, snz, d, e)
+    const double div_s = (SC(0, eps) - SC(0, -eps)) / (2.0 * eps) + (SC(1, eps) - SC(1, -eps)) / (2.0 * eps) +
+        (SC(2, eps) - SC(2, -eps)) / (2.0 * eps);
+#undef SC
+    return div_s + K - Kss;
+}
+
+/* findHorizon's flow and surface integrals. h[Nth * 2 Nth] in/out (start:
+ * the initial radius everywhere); returns the number of iterations run when
+ * converged (max |Theta| < tol at that iteration), -1 otherwise. res[0..4] =
+ * area, irreducible mass, spin (clamped), equatorial and polar circumference. */
+int orc_find_horizon(const orc_geom* g, const double* u, const double* center, int max_iterations, double tol,
+                     int ang_res, double* h, double* res) {
+    const int Nth = ang_res, Nph = 2 * ang_res;
+    const double h_grid = g->dx[0], flow_step = 0.05 * h_grid;
+    int converged = -1;
+    for (int iter = 0; iter < max_iterations; ++iter) {
+        double max_theta = 0.0;
+        for (int i = 0; i < Nth; ++i) {
+            const double th = ORC_PI * (i + 0.5) / Nth, sth = sin(th), cth = cos(th);
+            for (int j = 0; j < Nph; ++j) {
+                const double ph = 2.0 * ORC_PI * j / Nph, sph = sin(ph), cph = cos(ph);
+                const double r = h[i * Nph + j];
+                const double px = center[0] + r * sth * cph, py = center[1] + r * sth * sph, pz = center[2] + r * cth;
+                const double Theta = orc_horizon_expansion(g, u, px, py, pz, sth * cph, sth * sph, cth);
+                h[i * Nph + j] -= flow_step * Theta;
+                const double lo = 1.0e-6 * h_grid;
+                h[i * Nph + j] = h[i * Nph + j] < lo ? lo : h[i * Nph + j];
+                const double a = fabs(Theta);
+                max_theta = max_theta < a ? a : max_theta;
+            }
+        }
+        if (max_theta < tol) {
+            converged = iter + 1;
+            break;
+        }
+    }
+    if (converged < 0) return -1;
+    const double dth = ORC_PI / Nth, dph = 2.0 * ORC_PI / Nph;
+    double area = 0.0, jz = 0.0;
+    for (int i = 0; i < Nth; ++i) {
+        const double th = ORC_PI * (i + 0.5) / Nth, sth = sin(th), cth = cos(th);
+        for (int j = 0; j < Nph; ++j) {
+            const double ph = 2.0 * ORC_PI * j / Nph, sph = sin(ph), cph = cos(ph);
+            const double r = h[i * Nph + j];
+            const double px = center[0] + r * sth * cph, py = center[1] + r * sth * sph, pz = center[2] + r * cth;
+            const double chi = hz_interp(g, u, CHI, px, py, pz);
+            if (chi < 1.0e-12) continue;
+            const double gxx = hz_interp(g, u, GXX, px, py, pz), gyy = hz_interp(g, u, GYY, px, py, pz),
+                         gzz = hz_interp(g, u, GZZ, px, py, pz);
+            const double sqrt_g = sqrt(fabs(gxx * gyy * gzz)) / (chi * sqrt(chi));
+            area += sqrt_g * r * r * sth * dth * dph;
+            jz += (-sph * px + cph * py) * sqrt_g * r * sth * dth * dph;
+        }
+    }
+    const double mirr = sqrt(area / (16.0 * ORC_PI));
+    double ceq = 0.0, cpol = 0.0;
+    for (int j = 0; j < Nph; ++j) ceq += h[(Nth / 2) * Nph + j] * dph;
+    for (int i = 0; i < Nth; ++i) cpol += h[i * Nph] * dth;
+    double a = mirr > 1.0e-12 ? jz / (mirr * mirr) : 0.0;
+    a = a < -1.0 ? -1.0 : (a > 1.0 ? 1.0 : a);
+    res[0] = area;
+    res[1] = mirr;
+    res[2] = a;
+    res[3] = ceq;
+    res[4] = 2.0 * cpol;
+    return converged;
+}

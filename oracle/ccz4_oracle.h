@@ -107,6 +107,16 @@ void orc_matter_sources(const orc_geom* g, const double* prim, double* rho, doub
 void orc_psi4_modes(const orc_geom* g, const double* hi, const double* u, const double* radii, int nr, int n_theta,
                     int n_phi, int l_max, double* modes, int* npoints);
 
+/* Apparent-horizon flow (horizon_finder.cpp): the null expansion at a point
+ * for the coordinate normal sn (computeExpansion, :114-281), and findHorizon
+ * (:310-449): h[ang_res * 2 ang_res] in (initial radius) / out; returns the
+ * iterations run when converged, else -1; res = area, irreducible mass, spin,
+ * equatorial and polar circumference. */
+double orc_horizon_expansion(const orc_geom* g, const double* u, double px, double py, double pz, double snx,
+                             double sny, double snz);
+int orc_find_horizon(const orc_geom* g, const double* u, const double* center, int max_iterations, double tol,
+                     int ang_res, double* h, double* res);
+
 /* OpenMP thread count used by the parallel loops (0 = leave default) */
 void orc_set_threads(int n);
 

@@ -2,8 +2,9 @@
 //
 // oracle/Makefile compiles this file together with the unmodified reference
 // sources src/spacetime/ccz4.cpp, src/core/grid.cpp, src/amr/amr.cpp,
-// src/initial_data/initial_data.cpp, src/grmhd/{grmhd,hlld,tabulated_eos}.cpp and
-// src/postprocess/postprocess.cpp into oracle/_ref/libgranite_ref_*.so.
+// src/initial_data/initial_data.cpp, src/grmhd/{grmhd,hlld,tabulated_eos}.cpp,
+// src/postprocess/postprocess.cpp and src/horizon/horizon_finder.cpp into
+// oracle/_ref/libgranite_ref_*.so.
 // The shim only copies flat buffers in and out of reference GridBlocks and
 // calls the reference's own operators; it adds no arithmetic of its own except
 // in ref_rk3_steps, whose main.cpp lambdas (combine, floors, algebraic
@@ -14,6 +15,7 @@
 #include "granite/amr/amr.hpp"
 #include "granite/core/grid.hpp"
 #include "granite/grmhd/grmhd.hpp"
+#include "granite/horizon/horizon_finder.hpp"
 #include "granite/postprocess/postprocess.hpp"
 #include "granite/initial_data/initial_data.hpp"
 #include "granite/spacetime/ccz4.hpp"
@@ -207,6 +209,54 @@ void ref_psi4_modes(const int* n, int ng, const double* lo, const double* hi, co
                 modes[2 * q] = v.real();
                 modes[2 * q + 1] = v.imag();
             }
+}
+
+// ApparentHorizonFinder::findHorizon (horizon_finder.cpp:310-449). Returns 1 and
+// res = area, irreducible mass, spin, equatorial / polar circumference and
+// surface[N][3] when found, 0 otherwise.
+int ref_find_horizon(const int* n, int ng, const double* lo, const double* hi, const double* u,
+                     const double* center, int max_iterations, double tol, int ang_res, double init_r, double* res,
+                     double* surface) {
+    auto b = block(geo(n, ng, lo, hi));
+    std::memcpy(b->flatBuffer(), u, nbytes(*b));
+    horizon::HorizonParams hp;
+    hp.max_iterations = max_iterations;
+    hp.tolerance = tol;
+    hp.angular_resolution = ang_res;
+    hp.initial_guess_radius = init_r;
+    horizon::ApparentHorizonFinder f(hp);
+    auto r = f.findHorizon(*b, {center[0], center[1], center[2]});
+    if (!r) return 0;
+    res[0] = r->area;
+    res[1] = r->irreducible_mass;
+    res[2] = r->spin;
+    res[3] = r->circumference_equatorial;
+    res[4] = r->circumference_polar;
+    for (size_t q = 0; q < r->surface_points.size(); ++q)
+        for (int d = 0; d < 3; ++d) surface[3 * q + d] = r->surface_points[q][d];
+    return 1;
+}
+
+// findAllHorizons (horizon_finder.cpp:452-507): up to cap horizons; per horizon
+// out[6 h ..] = centroid x, y, z, area, irreducible mass, spin. Returns the count.
+int ref_find_all_horizons(const int* n, int ng, const double* lo, const double* hi, const double* u,
+                          int max_iterations, double tol, int ang_res, double init_r, double* out, int cap) {
+    auto b = block(geo(n, ng, lo, hi));
+    std::memcpy(b->flatBuffer(), u, nbytes(*b));
+    horizon::HorizonParams hp;
+    hp.max_iterations = max_iterations;
+    hp.tolerance = tol;
+    hp.angular_resolution = ang_res;
+    hp.initial_guess_radius = init_r;
+    horizon::ApparentHorizonFinder f(hp);
+    const auto all = f.findAllHorizons(*b);
+    for (size_t q = 0; q < all.size() && (int)q < cap; ++q) {
+        for (int d = 0; d < 3; ++d) out[6 * q + d] = all[q].centroid[d];
+        out[6 * q + 3] = all[q].area;
+        out[6 * q + 4] = all[q].irreducible_mass;
+        out[6 * q + 5] = all[q].spin;
+    }
+    return (int)all.size();
 }
 
 // setFlatSpacetime / setGaugeWaveData (ccz4.cpp:1165-1221) on a zeroed block.

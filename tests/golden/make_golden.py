@@ -99,6 +99,18 @@ def main():
     modes = ref.psi4_modes(gp, up, radii, 16, 32, 4)
     cases["psi4_modes"] = (gp, dict(modes=modes, radii=radii, seed=51, n_theta=16, n_phi=32, l_max=4))
 
+    gh = Geom((32, 32, 32), (-1.6, -1.6, -1.6), (1.6, 1.6, 1.6))
+    uh = ref.init_brill_lindquist(gh, [1.0], [[0.0, 0.0, 0.0]]) + 1e-9 * oracle.hash_noise(gh.shape, 61)
+    found, res, surf = ref.find_horizon(gh, uh, (0.0, 0.0, 0.0), 3000, 1e-2, 8, 1.0)
+    assert found
+    cases["horizon_flow"] = (gh, dict(res=res, surface=surf, seed=61, max_iterations=3000, tolerance=1e-2,
+                                      angular_resolution=8, initial_guess_radius=1.0))
+    ga = Geom((33, 33, 33), (-1.65, -1.65, -1.65), (1.65, 1.65, 1.65))
+    ua = ref.init_brill_lindquist(ga, [1.0], [[0.0, 0.0, 0.0]])
+    rows = ref.find_all_horizons(ga, ua, 1500, 1e-2, 8, 1.0)
+    cases["horizon_all"] = (ga, dict(rows=rows, max_iterations=1500, tolerance=1e-2, angular_resolution=8,
+                                     initial_guess_radius=1.0))
+
     for name, (g, data) in cases.items():
         path = os.path.join(OUT, f"{name}.npz")
         np.savez_compressed(path, **geom_dict(g), **data)

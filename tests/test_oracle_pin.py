@@ -36,7 +36,8 @@ def test_golden_files_present():
     names = {os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLD, "*.npz"))}
     for n in ["rhs_random", "rhs_matter", "rhs_random_noko", "constraints_random", "ko_random",
               "rhs_bl", "constraints_bl", "rk3_bl_3steps", "init_bl", "init_gauge_wave",
-              "rk3_gauge_wave_periodic_4steps", "prolong", "restrict", "matter_sources", "psi4_modes"]:
+              "rk3_gauge_wave_periodic_4steps", "prolong", "restrict", "matter_sources", "psi4_modes",
+              "horizon_flow", "horizon_all"]:
         assert n in names, n
 
 
@@ -103,6 +104,32 @@ def test_oracle_psi4_vs_reference(oracle_lib, l_max, nth, nph):
     radii = [1.0, 2.5, 4.2]
     assert np.array_equal(oracle_lib.psi4_modes(g, u, radii, nth, nph, l_max),
                           ref.psi4_modes(g, u, radii, nth, nph, l_max))
+
+
+def test_oracle_horizon_golden(oracle_lib):
+    """findHorizon (horizon_finder.cpp:310-449): the flow, its converged iteration
+    and the surface integrals, bit for bit."""
+    g, z = load("horizon_flow")
+    u = oracle_lib.init_brill_lindquist(g, [1.0], [[0.0, 0.0, 0.0]]) + 1e-9 * oracle.hash_noise(g.shape, int(z["seed"]))
+    it, h, res = oracle_lib.find_horizon(g, u, (0.0, 0.0, 0.0), int(z["max_iterations"]), float(z["tolerance"]),
+                                         int(z["angular_resolution"]), float(z["initial_guess_radius"]))
+    assert it > 0 and np.array_equal(res, z["res"])
+    from granite_b200.horizon import surface_points
+    assert np.array_equal(np.array(surface_points((0.0, 0.0, 0.0), h)), z["surface"])
+
+
+@pytest.mark.skipif(not oracle.reference_available("strict"), reason="reference library not built")
+def test_oracle_horizon_vs_reference(oracle_lib):
+    ref = oracle.Reference("strict")
+    g = Geom((24, 20, 22), (-1.2, -1.0, -1.1), (1.2, 1.0, 1.1))
+    u = ref.init_brill_lindquist(g, [0.8], [[0.0, 0.0, 0.0]]) + 1e-7 * oracle.hash_noise(g.shape, 3)
+    for center, tol in [((0.0, 0.0, 0.0), 1e-2), ((0.02, -0.01, 0.03), 1e-2), ((0.0, 0.0, 0.0), 1e-12)]:
+        it, h, res = oracle_lib.find_horizon(g, u, center, 800, tol, 6, 0.9)
+        found, rres, surf = ref.find_horizon(g, u, center, 800, tol, 6, 0.9)
+        assert found == (it > 0) and np.array_equal(res, rres)
+        if found:
+            from granite_b200.horizon import surface_points
+            assert np.array_equal(np.array(surface_points(center, h)), surf)
 
 
 def test_oracle_constraints_golden(oracle_lib):
