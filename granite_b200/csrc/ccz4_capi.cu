@@ -1701,11 +1701,18 @@ struct RegridHook {
 // AMRHierarchy::subcycle(L) with the RK3 step as evolve_func, amr.cpp:303-350.
 // With a hook, nothing is captured: the level times advance here and the hook
 // runs at the reference's regrid points.
-cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long long* n, RegridHook* hook = nullptr) {
+// skip_prefill: the level's state and every cell its fill reads are what the
+// fill at the end of its previous step saw (the second substep of the finest
+// level in GRANITE_AMR_GHOSTS: nothing restricts into it, its parent does not
+// change between the two substeps), so the fill before this step would write
+// the values already there.
+cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long long* n, RegridHook* hook = nullptr,
+                     bool skip_prefill = false) {
     cudaError_t e;
     if (hook && (hook->status = ensure_xfer(c, mode))) return cudaErrorInvalidValue;
     const LevelXfer& X = c->xfer[mode][L];
-    if (mode == GRANITE_AMR_REFERENCE && L > 0) {  // amr.cpp:313-318 (the fill below repeats it exactly)
+    if (skip_prefill) {
+    } else if (mode == GRANITE_AMR_REFERENCE && L > 0) {  // amr.cpp:313-318 (the fill below repeats it exactly)
         if ((e = xfer(c, XFER_PROLONG, X.prolong, 0, 0))) return e;
         ++*n;
         if ((e = level_ghost(c, c->levels[L], GHOST_ZERO_GRADIENT_MASKED, 0, X.d_facemask, n))) return e;
@@ -1721,8 +1728,11 @@ cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long lon
     if ((e = fill_level(c, L, 0, true, mode, n))) return e;  // amr.cpp:329
     if (hook) c->level_time[L] += dt;                         // amr.cpp:326
     if (L + 1 < (int)c->levels.size()) {
-        for (int r = 0; r < 2; ++r)
-            if ((e = subcycle(c, L + 1, dt / 2.0, precision, mode, n, hook))) return e;  // amr.cpp:334-336, :393-397
+        for (int r = 0; r < 2; ++r) {  // amr.cpp:334-336, :393-397
+            // (with a regrid hook the level list may change between the substeps: always fill)
+            const bool skip = r == 1 && !hook && mode == GRANITE_AMR_GHOSTS && L + 2 == (int)c->levels.size();
+            if ((e = subcycle(c, L + 1, dt / 2.0, precision, mode, n, hook, skip))) return e;
+        }
         if (hook && (hook->status = ensure_xfer(c, mode))) return cudaErrorInvalidValue;  // a regrid rebuilt them
         for (const XferList& rl : c->xfer[mode][L].restrict_) {                            // amr.cpp:339-341
             if ((e = xfer(c, XFER_RESTRICT, rl, 0, 0))) return e;

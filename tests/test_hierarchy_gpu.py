@@ -158,3 +158,29 @@ def test_hierarchy_mixed_close_to_fp64(gb, oracle_lib):
     # mixed-precision deviation from the FP64 run, relative to each tensor's scale
     for a, b in zip(res[gb.PRECISION_FP64], res[gb.PRECISION_MIXED]):
         parity(b, a, rtol=1e-5, what="mixed vs fp64")
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_finest_prefill_skip_is_exact(gb, oracle_lib, precision):
+    # the graph-captured step leaves out the fill before the finest level's second
+    # substep (its inputs are those of the fill that ended the first one); the
+    # uncaptured step with the regrid hook (interval 0: no regrid) performs every
+    # fill, as amr.cpp does: the two agree bit for bit
+    h, geoms, levels = small_hierarchy(seed=17, levels=3)
+    states = [oracle.add_noise(oracle_lib.init_brill_lindquist(g, h.masses, h.positions, r_floor=0.5 * g.dx[0]),
+                               1e-10, 90 + i) for i, g in enumerate(geoms)]
+    dt = 0.25 * geoms[0].dx[0]
+    outs = []
+    for hooked in (False, True):
+        ev, blocks = gpu_hierarchy(gb, geoms, levels, states)
+        ev.set_fp64_chi_threshold(0.5)
+        for _ in range(2):
+            if hooked:
+                ev.hierarchy_step_regrid(dt, None, 0, precision=precision, amr_mode=gb.AMR_GHOSTS)
+            else:
+                ev.hierarchy_step(dt, precision, gb.AMR_GHOSTS)
+        ev.download()
+        outs.append([b.array.copy() for b in blocks])
+        ev.close()
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
