@@ -123,6 +123,8 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_measure_fma_rate.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
     lib.granite_ccz4_get_fp64_chi_threshold.argtypes = [vp, C.POINTER(C.c_double)]
     lib.granite_ccz4_regrid_add.argtypes = [vp, C.POINTER(_BlockDesc), C.c_int]
+    lib.granite_ccz4_upload_all.argtypes = [vp, C.POINTER(dp)]
+    lib.granite_ccz4_download_all.argtypes = [vp, C.POINTER(dp)]
     ip = C.POINTER(C.c_int)
     hp = C.POINTER(_HorizonParams)
     lib.granite_ccz4_default_horizon_params.argtypes = [hp]
@@ -477,16 +479,26 @@ class Evolver:
         return n.value
 
     def upload(self, idx: int | None = None, array=None):
-        items = range(len(self.blocks)) if idx is None else [idx]
-        for i in items:
-            a = self.blocks[i].array if array is None else _f64(array)
-            self.ctx.check(self.ctx.lib.granite_ccz4_upload_block(self.ctx.h, i, _dp(a)))
+        """Block idx (all blocks when None) from its host array or ``array`` (for
+        all blocks: a list of arrays, one per block, in block order)."""
+        if idx is None:
+            arrs = [b.array for b in self.blocks] if array is None else [_f64(a) for a in array]
+            ptrs = (C.POINTER(C.c_double) * len(arrs))(*[_dp(a) for a in arrs])
+            self.ctx.check(self.ctx.lib.granite_ccz4_upload_all(self.ctx.h, ptrs))
+            self._keep = arrs  # the copies are stream-ordered: keep the buffers alive
+            return
+        a = self.blocks[idx].array if array is None else _f64(array)
+        self.ctx.check(self.ctx.lib.granite_ccz4_upload_block(self.ctx.h, idx, _dp(a)))
 
     def download(self, idx: int | None = None, out=None):
-        items = range(len(self.blocks)) if idx is None else [idx]
-        for i in items:
-            a = self.blocks[i].array if out is None else _f64(out)
-            self.ctx.check(self.ctx.lib.granite_ccz4_download_block(self.ctx.h, i, _dp(a)))
+        """Block idx (all blocks when None, one synchronisation) into its host array or ``out``."""
+        if idx is None:
+            arrs = [b.array for b in self.blocks] if out is None else [_f64(a) for a in out]
+            ptrs = (C.POINTER(C.c_double) * len(arrs))(*[_dp(a) for a in arrs])
+            self.ctx.check(self.ctx.lib.granite_ccz4_download_all(self.ctx.h, ptrs))
+            return
+        a = self.blocks[idx].array if out is None else _f64(out)
+        self.ctx.check(self.ctx.lib.granite_ccz4_download_block(self.ctx.h, idx, _dp(a)))
 
     def regrid_add(self, blocks):
         """Append GridBlocks to the committed hierarchy; the device fills every cell of

@@ -1133,6 +1133,38 @@ int granite_ccz4_upload_block(void* h, int i, const double* host) {
     return GRANITE_OK;
 }
 
+int granite_ccz4_upload_all(void* h, const double* const* hosts) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (!c->committed) return fail(c, GRANITE_ERR_INVALID, "commit before upload/download");
+    if (!hosts) return fail(c, GRANITE_ERR_INVALID, "null host buffer list");
+    for (size_t i = 0; i < c->descs.size(); ++i)
+        if (!hosts[i]) return fail(c, GRANITE_ERR_INVALID, "null host buffer");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    for (size_t i = 0; i < c->descs.size(); ++i)
+        CK(cudaMemcpyAsync(c->hblocks[i].buf[0], hosts[i], (size_t)c->hblocks[i].stride * NV * sizeof(double),
+                           cudaMemcpyHostToDevice, c->stream),
+           "H2D block");
+    for (size_t L = 0; L < c->level_ghosts_valid.size(); ++L) c->level_ghosts_valid[L] = false;
+    return GRANITE_OK;
+}
+
+int granite_ccz4_download_all(void* h, double* const* hosts) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (!c->committed) return fail(c, GRANITE_ERR_INVALID, "commit before upload/download");
+    if (!hosts) return fail(c, GRANITE_ERR_INVALID, "null host buffer list");
+    for (size_t i = 0; i < c->descs.size(); ++i)
+        if (!hosts[i]) return fail(c, GRANITE_ERR_INVALID, "null host buffer");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    for (size_t i = 0; i < c->descs.size(); ++i)
+        CK(cudaMemcpyAsync(hosts[i], c->hblocks[i].buf[0], (size_t)c->hblocks[i].stride * NV * sizeof(double),
+                           cudaMemcpyDeviceToHost, c->stream),
+           "D2H block");
+    CK(cudaStreamSynchronize(c->stream), "sync");
+    return GRANITE_OK;
+}
+
 int granite_ccz4_download_block(void* h, int i, double* host) {
     Ctx* c = static_cast<Ctx*>(h);
     if (!c) return GRANITE_ERR_INVALID;

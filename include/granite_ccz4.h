@@ -197,6 +197,13 @@ GRANITE_API int granite_ccz4_num_blocks(const void* ctx);
 GRANITE_API int granite_ccz4_arena_bytes(const void* ctx, size_t* bytes);
 GRANITE_API int granite_ccz4_upload_block(void* ctx, int block_index, const double* host_u);
 GRANITE_API int granite_ccz4_download_block(void* ctx, int block_index, double* host_u);
+/* Every block at once: hosts[i] is block i's flatBuffer() (num_blocks entries).
+ * upload_all is stream-ordered and returns at once (keep the buffers until the
+ * next sync); download_all returns when all blocks are on the host. One
+ * synchronisation for the whole hierarchy instead of one per block; pinned
+ * buffers let the copies run at full PCIe rate. */
+GRANITE_API int granite_ccz4_upload_all(void* ctx, const double* const* hosts);
+GRANITE_API int granite_ccz4_download_all(void* ctx, double* const* hosts);
 
 /* ---- stepping -------------------------------------------------------------- */
 
