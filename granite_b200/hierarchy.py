@@ -9,7 +9,8 @@ whose edge lengths are drawn, per axis, from a size set (a tensor product of
 three random compositions of the level's cell count), with the block count per
 level drawn into a requested range. Levels nest with a margin of at least two
 coarse cells, every block corner lies on its level's cell grid, and blocks
-follow level order. The layout is static: there is no regridding.
+follow level order. These workload layouts are static (the benchmarks do not
+regrid); the reference's tracking-sphere regrid is in regrid.py.
 """
 from __future__ import annotations
 
