@@ -2225,7 +2225,8 @@ int horizon_run(Ctx* c, const DevBlock& B, const double* u, const granite_horizo
         tab[2 * nth + j] = std::sin(ph);
         tab[2 * nth + nph + j] = std::cos(ph);
     }
-    const size_t need = 4 * 256 + (tab.size() + (size_t)N + (size_t)HZ_CHUNK * N + 3 * (size_t)N + HZ_CHUNK) * 8;
+    // five pieces, each rounded up to 256 bytes by carve()
+    const size_t need = 5 * 256 + (tab.size() + (size_t)N + (size_t)HZ_CHUNK * N + 3 * (size_t)N + HZ_CHUNK) * 8;
     int r = diag_scratch(c, need);
     if (r) return r;
     char* q = c->s_diag;
