@@ -232,7 +232,9 @@ int check_desc(Ctx* c, const granite_block_desc* b) {
         if (b->ncells[d] < NG) return fail(c, GRANITE_ERR_INVALID, "ncells must be >= 4 per axis");
         if (!(b->hi[d] > b->lo[d])) return fail(c, GRANITE_ERR_INVALID, "hi must exceed lo");
     }
-    if (cells_of(*b) * NV > (1ll << 40)) return fail(c, GRANITE_ERR_INVALID, "block too large");
+    // cell indices within a block are 32-bit in the transfer kernels (2^31 cells
+    // would be 378 GB of state, beyond any one GPU)
+    if (cells_of(*b) >= (1ll << 31)) return fail(c, GRANITE_ERR_INVALID, "block too large: 2^31 cells or more");
     return GRANITE_OK;
 }
 
