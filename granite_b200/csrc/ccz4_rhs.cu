@@ -874,7 +874,7 @@ __global__ void __launch_bounds__(128)
 // ---------------------------------------------------------------------------
 constexpr int V0_TX = 32, V0_TY = 4, V0_TZ = 1;
 constexpr int V1_TX = 16, V1_TY = 4, V1_TZ = 2, V1_NBUF = 3;
-constexpr int V4_NBUF = 4;
+constexpr int V4_NBUF = 3;
 
 int stage_tile_dims(int variant, int* tx, int* ty, int* tz) {
     if (variant == VARIANT_TMA) {
