@@ -163,11 +163,13 @@ public:
 
     void operator()(std::vector<Block*>& blocks, double dt) {
         if (!ctx_ || blocks != bound_) bind(blocks);
-        for (size_t i = 0; i < blocks.size(); ++i)
-            ctx_->check(granite_ccz4_upload_block(ctx_->get(), (int)i, blocks[i]->flatBuffer()), "upload");
+        if (blocks.empty()) return;
+        std::vector<double*> bufs(blocks.size());
+        for (size_t i = 0; i < blocks.size(); ++i) bufs[i] = blocks[i]->flatBuffer();
+        // the whole level in, one step, the whole level out (one synchronisation)
+        ctx_->check(granite_ccz4_upload_all(ctx_->get(), bufs.data()), "upload");
         ctx_->check(granite_ccz4_rk3_step(ctx_->get(), level_, dt, precision_, bc_), "rk3_step");
-        for (size_t i = 0; i < blocks.size(); ++i)
-            ctx_->check(granite_ccz4_download_block(ctx_->get(), (int)i, blocks[i]->flatBuffer()), "download");
+        ctx_->check(granite_ccz4_download_all(ctx_->get(), bufs.data()), "download");
     }
 
 private:
