@@ -110,6 +110,12 @@ def main():
     rows = ref.find_all_horizons(ga, ua, 1500, 1e-2, 8, 1.0)
     cases["horizon_all"] = (ga, dict(rows=rows, max_iterations=1500, tolerance=1e-2, angular_resolution=8,
                                      initial_guess_radius=1.0))
+    g2 = Geom((41, 33, 33), (-2.05, -1.65, -1.65), (2.05, 1.65, 1.65))
+    u2 = ref.init_brill_lindquist(g2, [0.6, 0.4], [[-1.0, 0.0, 0.0], [1.0, 0.0, 0.0]])
+    rows2 = ref.find_all_horizons(g2, u2, 800, 1e-2, 6, 0.4)
+    cases["horizon_all_binary"] = (g2, dict(rows=rows2, max_iterations=800, tolerance=1e-2, angular_resolution=6,
+                                            initial_guess_radius=0.4, masses=np.array([0.6, 0.4]),
+                                            positions=np.array([[-1.0, 0.0, 0.0], [1.0, 0.0, 0.0]])))
 
     for name, (g, data) in cases.items():
         path = os.path.join(OUT, f"{name}.npz")

@@ -96,6 +96,19 @@ def test_find_all_horizons_golden(gb, oracle_lib):
     ev.close()
 
 
+def test_find_all_horizons_binary_golden(gb, oracle_lib):
+    """Two punctures on cell centres: two lapse minima, both horizons found, in
+    the reference's order, values bit for bit."""
+    from granite_b200.horizon import ApparentHorizonFinder
+    g, z = load("horizon_all_binary")
+    u = oracle_lib.init_brill_lindquist(g, list(z["masses"]), z["positions"].tolist())
+    ev = resident(gb, g, u)
+    hs = ApparentHorizonFinder(params(z)).findAllHorizons((ev, 0))
+    rows = [list(h.centroid) + [h.area, h.irreducible_mass, h.spin] for h in hs]
+    assert len(hs) == 2 and np.array_equal(np.array(rows), z["rows"])
+    ev.close()
+
+
 def test_find_horizon_rejects_bad_params(gb, oracle_lib):
     from granite_b200.horizon import ApparentHorizonFinder, HorizonParams
     g = Geom((16, 16, 16), (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0))

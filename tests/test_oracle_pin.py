@@ -37,7 +37,7 @@ def test_golden_files_present():
     for n in ["rhs_random", "rhs_matter", "rhs_random_noko", "constraints_random", "ko_random",
               "rhs_bl", "constraints_bl", "rk3_bl_3steps", "init_bl", "init_gauge_wave",
               "rk3_gauge_wave_periodic_4steps", "prolong", "restrict", "matter_sources", "psi4_modes",
-              "horizon_flow", "horizon_all"]:
+              "horizon_flow", "horizon_all", "horizon_all_binary"]:
         assert n in names, n
 
 
