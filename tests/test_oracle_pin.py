@@ -73,7 +73,7 @@ def test_oracle_matter_sources_golden(oracle_lib):
 
 
 @pytest.mark.skipif(not oracle.reference_available("strict"), reason="reference library not built")
-@pytest.mark.parametrize("seed,superluminal", [(3, 0.0), (4, 0.3)])
+@pytest.mark.parametrize("seed,superluminal", [(3, 0.0), (4, 0.3), (5, 1.0)])
 def test_oracle_matter_sources_vs_reference(oracle_lib, seed, superluminal):
     ref = oracle.Reference("strict")
     g = Geom((9, 7, 5), (-1.0, 0.0, 2.0), (0.8, 1.4, 3.0))
@@ -96,7 +96,7 @@ def test_oracle_psi4_golden(oracle_lib):
 
 
 @pytest.mark.skipif(not oracle.reference_available("strict"), reason="reference library not built")
-@pytest.mark.parametrize("l_max,nth,nph", [(2, 8, 12), (5, 21, 17)])
+@pytest.mark.parametrize("l_max,nth,nph", [(2, 8, 12), (5, 21, 17), (3, 40, 80)])
 def test_oracle_psi4_vs_reference(oracle_lib, l_max, nth, nph):
     ref = oracle.Reference("strict")
     g = Geom((20, 18, 16), (-5.0, -4.5, -4.0), (5.0, 4.5, 4.0))

@@ -163,7 +163,7 @@ def oracle_regrid_hook(planner, tagger=None):
     return hook
 
 
-@pytest.mark.parametrize("interval", [1, 2])
+@pytest.mark.parametrize("interval", [1, 2, 3])
 def test_oracle_in_step_regrid_equals_compiled_hierarchy(oracle_lib, reference_lib, interval):
     """Moving spheres, then two coarse steps with the reference's in-step regrid:
     the oracle (restated subcycle + planner + oracle prolongation) and the
