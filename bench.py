@@ -306,6 +306,22 @@ def run_reference(args, w, rank, world):
 # GPU arm
 # ---------------------------------------------------------------------------
 
+def max_over_ranks(torch, dist, world, value, device):
+    """The largest of the ranks' values (the job's time is its slowest rank's):
+    one all-reduce MAX over the process group; the value itself on one rank."""
+    if world == 1:
+        return float(value)
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(points_per_step, steps, world, ms):
+    """Point-updates per second of all ranks together: every rank advances its own
+    replica of the workload, the job takes the slowest rank's time."""
+    return points_per_step * steps * world / (ms / 1000.0)
+
+
 def timed_steps(torch, dist, world, local, run: Runner, steps: int):
     stream = torch.cuda.ExternalStream(run.ev.stream_handle(), device=local)
     n0 = run.ev.launch_count()
@@ -322,11 +338,8 @@ def timed_steps(torch, dist, world, local, run: Runner, steps: int):
     torch.cuda.synchronize(local)
     if world > 1:
         dist.barrier()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item()), run.ev.launch_count() - n0
+    ms = max_over_ranks(torch, dist, world, e0.elapsed_time(e1), f"cuda:{local}")
+    return ms, run.ev.launch_count() - n0
 
 
 def roofline(gb, run: Runner, workload, prof_steps, kernel):
@@ -456,7 +469,7 @@ def main():
     time.sleep(0.3)
     ms, launches = timed_steps(torch, dist, world, local, run, args.steps)
     clocks = sampler.stop()
-    value = run.points_per_step * args.steps * world / (ms / 1000.0)
+    value = whole_job_rate(run.points_per_step, args.steps, world, ms)
     # kernel time of the same steps (eager launches bracketed by events), clocks sampled again
     prof_steps = max(1, min(args.steps, 5 if hier else 20))
     rsampler = ClockSampler(local)
@@ -483,11 +496,8 @@ def main():
         run.step()
         run.ev.download(None, views)
     run.ev.sync()
-    e2e_ms = (time.perf_counter() - t0) * 1000.0
-    e_t = torch.tensor([e2e_ms], device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(e_t, op=dist.ReduceOp.MAX)
-    e2e_val = run.points_per_step * e2e_steps * world / (float(e_t.item()) / 1000.0)
+    e2e_ms = max_over_ranks(torch, dist, world, (time.perf_counter() - t0) * 1000.0, f"cuda:{local}")
+    e2e_val = whole_job_rate(run.points_per_step, e2e_steps, world, e2e_ms)
 
     # after the headline measurements: the same mixed steps with the FP32 algebra on
     # every tile, then the FP64 comparison runs (these drop and rebuild cached graphs)
