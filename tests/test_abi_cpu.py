@@ -107,6 +107,45 @@ def test_invalid_arguments_rejected(lib):
     assert lib.granite_ccz4_destroy(None) == 0
 
 
+def test_null_context_is_an_error_everywhere(lib):
+    """Every entry point that takes a context answers a null one with
+    GRANITE_ERR_INVALID before touching a device (no GPU needed)."""
+    import granite_b200 as gb
+    d = gb.block_desc((8, 8, 8), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0))
+    buf = (C.c_double * 8)()
+    cnt = C.c_longlong()
+    t = C.c_double()
+    hz = gb._Horizon()
+    hp = gb._HorizonParams()
+    lib.granite_ccz4_default_horizon_params(C.byref(hp))
+    assert (hp.max_iterations, hp.tolerance, hp.angular_resolution, hp.initial_guess_radius) == (200, 1e-10, 50, 1.0)
+    lib.granite_ccz4_default_horizon_params(None)  # tolerated
+    f = C.c_double  # this library handle has no argtypes: doubles go in explicitly
+    calls = [
+        lib.granite_ccz4_regrid_add(None, C.byref(d), 1),
+        lib.granite_ccz4_tag_count(None, 0, 0, f(0.1), C.byref(cnt)),
+        lib.granite_ccz4_level_time(None, 0, C.byref(t)),
+        lib.granite_ccz4_hierarchy_step_regrid(None, f(0.1), 0, 0, 0, None, None),
+        lib.granite_ccz4_enable_matter(None, 1),
+        lib.granite_ccz4_upload_primitives(None, 0, buf),
+        lib.granite_ccz4_set_primitives_device(None, 0, None),
+        lib.granite_ccz4_matter_sources_host(None, C.byref(d), buf, buf, buf, buf, buf),
+        lib.granite_ccz4_matter_sources_device(None, C.byref(d), None, None, None, None, None, None),
+        lib.granite_ccz4_psi4_modes(None, 0, buf, 1, 4, 8, 2, buf, None),
+        lib.granite_ccz4_psi4_modes_host(None, C.byref(d), buf, buf, 1, 4, 8, 2, buf, None),
+        lib.granite_ccz4_find_horizon(None, 0, C.byref(hp), buf, C.byref(hz), None),
+        lib.granite_ccz4_find_horizon_host(None, C.byref(d), buf, C.byref(hp), buf, C.byref(hz), None),
+        lib.granite_ccz4_find_all_horizons(None, 0, C.byref(hp), C.byref(hz), 1, None),
+        lib.granite_ccz4_checkpoint_write(None, b"x", 0, f(0.0)),
+        lib.granite_ccz4_checkpoint_read(None, b"x", None, None),
+        lib.granite_ccz4_upload_all(None, None),
+        lib.granite_ccz4_download_all(None, None),
+    ]
+    assert calls == [-1] * len(calls)
+    n = C.c_int()
+    assert lib.granite_ccz4_checkpoint_header(b"/nonexistent/checkpoint", None, None, None, None, 0, C.byref(n)) == -1
+
+
 def test_gridblock_layout_matches_reference_conventions():
     import granite_b200 as gb
     b = gb.GridBlock(3, 1, (6, 5, 4), (-1.0, 0.0, 2.0), (2.0, 1.0, 3.0), 4, 22)
