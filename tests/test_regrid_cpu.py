@@ -195,3 +195,37 @@ def test_oracle_in_step_regrid_equals_compiled_hierarchy(oracle_lib, reference_l
     assert [(ho.levels[i], ho.geoms[i]) for i in order] == list(zip(rh.levels, rh.geoms))
     for r, i in enumerate(order):
         assert np.array_equal(ho.u[i], rh.get(r)), f"block {r} (level {rh.levels[r]})"
+
+
+def test_planner_edge_cases():
+    """Nothing to place without a parent level, beyond max_levels, or when no
+    sphere reaches the level; a sphere wider than the domain is clamped to it;
+    an initial layout without spheres is the single level-0 block."""
+    from granite_b200.regrid import Box
+    p = RegridPlanner((8, 8, 8), (0.0, 0.0, 0.0), (8.0, 8.0, 8.0), max_levels=2)
+    base = p.initial_layout()
+    assert [(b.level, b.ncells) for b in base] == [(0, (8, 8, 8))]
+    p.add_tracking_sphere((4.0, 4.0, 4.0), 1.0, 5)
+    assert p.plan(1, base) == []                        # no block on level 1
+    lay = p.initial_layout()
+    assert [b.level for b in lay] == [0, 1]             # capped at max_levels - 1
+    assert p.plan(1, lay) == []                         # level 2 would exceed max_levels
+    q = RegridPlanner((8, 8, 8), (0.0, 0.0, 0.0), (8.0, 8.0, 8.0), max_levels=4)
+    q.add_tracking_sphere((0.1, 7.9, 4.0), 1.0, 1)
+    lv1 = [b for b in q.initial_layout() if b.level == 1]
+    assert len(lv1) == 1
+    b = lv1[0]
+    assert b.lo[0] == 0.0 and b.hi[1] == 8.0 and b.ncells == (8, 8, 8)  # clamped to the domain faces
+    assert q.plan(1, [Box(0, (8, 8, 8), (0.0,) * 3, (8.0,) * 3, 0), b]) == []  # min_level 1: nothing finer
+
+
+@pytest.mark.skipif(not oracle.reference_available("strict"), reason="reference library not built")
+@pytest.mark.parametrize("sphere,max_levels", [(((0.1, 7.9, 4.0), 1.0, 1), 4), (((4.0, 4.0, 4.0), 1.0, 5), 2),
+                                              (((7.5, 0.5, 7.5), 3.0, 3), 15)])
+def test_planner_edge_layouts_match_reference(sphere, max_levels):
+    from oracle.hierarchy import RefHierarchy
+    rh = RefHierarchy(oracle.Reference("strict"), (8, 8, 8), (0.0,) * 3, (8.0,) * 3, [sphere], max_levels)
+    p = RegridPlanner((8, 8, 8), (0.0,) * 3, (8.0,) * 3, max_levels=max_levels)
+    p.add_tracking_sphere(*sphere)
+    got = sorted(((b.level, b.ncells, b.lo, b.hi) for b in p.initial_layout()), key=lambda t: t[0])
+    assert got == [(lv, g.n, g.lo, g.hi) for g, lv in zip(rh.geoms, rh.levels)]
