@@ -1185,8 +1185,6 @@ int granite_ccz4_download_block(void* h, int i, double* host) {
 // stepping
 // ---------------------------------------------------------------------------
 
-// The fused stage kernel over one level: one launch over the whole work-list,
-// or (unbatched) one launch per block.
 // One stage over tiles [first, first + count) of a level: one launch, or with
 // per-tile precision (MIXED and a positive chi threshold) a classification of
 // the tiles from the stage input's chi (flag 1: a point below the threshold),
