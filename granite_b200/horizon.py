@@ -68,6 +68,32 @@ def _data(h: _Horizon, radii=None):
                        h.circumference_polar, surface_points(c, radii) if radii is not None else [], h.iterations)
 
 
+def common_horizon_guess(horizons):
+    """Centre and initial radius of the common-horizon search, or None
+    (horizon_finder.cpp:513-543): the irreducible-mass-weighted centroid of the
+    horizons, and 1.2 times the largest centroid distance plus equatorial
+    radius C_eq / (2 pi)."""
+    if len(horizons) < 2:
+        return None
+    total = 0.0
+    cc = [0.0, 0.0, 0.0]
+    for h in horizons:
+        for d in range(3):
+            cc[d] += h.irreducible_mass * h.centroid[d]
+        total += h.irreducible_mass
+    if total < 1.0e-14:
+        return None
+    cc = [x / total for x in cc]
+    max_r = 0.0
+    for h in horizons:
+        dist = 0.0
+        for d in range(3):
+            dd = h.centroid[d] - cc[d]
+            dist += dd * dd
+        max_r = max(max_r, math.sqrt(dist) + h.circumference_equatorial / (2.0 * PI))
+    return cc, 1.2 * max_r
+
+
 class ApparentHorizonFinder:
     """horizon_finder.hpp:43-87. ``source``: (Evolver, block index) for a resident
     block, or (runner, GridBlock) for a host block (runner: any object of this
@@ -115,26 +141,12 @@ class ApparentHorizonFinder:
 
     def findCommonHorizon(self, source, horizons):
         """A horizon about the mass-weighted centroid enclosing all (horizon_finder.cpp:510-551)."""
-        if len(horizons) < 2:
+        guess = common_horizon_guess(horizons)
+        if guess is None:
             return None
-        total = 0.0
-        cc = [0.0, 0.0, 0.0]
-        for h in horizons:
-            for d in range(3):
-                cc[d] += h.irreducible_mass * h.centroid[d]
-            total += h.irreducible_mass
-        if total < 1.0e-14:
-            return None
-        cc = [x / total for x in cc]
-        max_r = 0.0
-        for h in horizons:
-            dist = 0.0
-            for d in range(3):
-                dd = h.centroid[d] - cc[d]
-                dist += dd * dd
-            max_r = max(max_r, math.sqrt(dist) + h.circumference_equatorial / (2.0 * PI))
+        cc, radius = guess
         p = HorizonParams(self.params.max_iterations, self.params.tolerance, self.params.angular_resolution,
-                          1.2 * max_r)
+                          radius)
         out, radii = self._find(source, cc, p)
         if not out.found:
             return None

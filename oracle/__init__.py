@@ -354,6 +354,28 @@ class Reference:
                                            C.c_double(init_r), _p(out), C.c_int(cap))
         return out[:min(n, cap)]
 
+    def find_common_horizon(self, g: Geom, u, centroids, masses, circ_eq, max_iterations=200, tol=1e-10,
+                            ang_res=50, init_r=1.0):
+        """The compiled findCommonHorizon over horizons given by centroid, irreducible
+        mass and equatorial circumference: (found, [area, M_irr, spin, C_eq, C_pol],
+        surface points, (centroid, id))."""
+        nh = len(masses)
+        hz = np.ascontiguousarray(np.reshape(centroids, (nh, 3)), dtype=np.float64)
+        mc = np.ascontiguousarray(np.stack([np.asarray(masses, float), np.asarray(circ_eq, float)], axis=1))
+        res = np.zeros(5)
+        surf = np.zeros((ang_res * 2 * ang_res, 3))
+        cid = np.zeros(4)
+        found = self.lib.ref_find_common_horizon(*self._g(g), _p(np.ascontiguousarray(u, dtype=np.float64)),
+                                                 _p(hz), _p(mc), C.c_int(nh), C.c_int(max_iterations),
+                                                 C.c_double(tol), C.c_int(ang_res), C.c_double(init_r), _p(res),
+                                                 _p(surf), _p(cid))
+        return bool(found), res, surf, (tuple(cid[:3]), int(cid[3]))
+
+    def compute_spin(self, c_eq: float, c_pol: float) -> float:
+        """The compiled ApparentHorizonFinder::computeSpin of a horizon with these circumferences."""
+        self.lib.ref_compute_spin.restype = C.c_double
+        return self.lib.ref_compute_spin(C.c_double(c_eq), C.c_double(c_pol))
+
     def init_flat(self, g: Geom):
         u = g.zeros()
         self.lib.ref_init_flat(*self._g(g), _p(u))

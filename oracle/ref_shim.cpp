@@ -259,6 +259,53 @@ int ref_find_all_horizons(const int* n, int ng, const double* lo, const double* 
     return (int)all.size();
 }
 
+// findCommonHorizon (horizon_finder.cpp:510-551) over nh given horizons, each
+// hz[3 h ..] = centroid x, y, z and mass_circ[2 h ..] = irreducible mass,
+// equatorial circumference (the fields it reads). Same outputs as
+// ref_find_horizon, plus the result's centroid and id in cen_id[0..3].
+int ref_find_common_horizon(const int* n, int ng, const double* lo, const double* hi, const double* u,
+                            const double* hz, const double* mass_circ, int nh, int max_iterations, double tol,
+                            int ang_res, double init_r, double* res, double* surface, double* cen_id) {
+    auto b = block(geo(n, ng, lo, hi));
+    std::memcpy(b->flatBuffer(), u, nbytes(*b));
+    horizon::HorizonParams hp;
+    hp.max_iterations = max_iterations;
+    hp.tolerance = tol;
+    hp.angular_resolution = ang_res;
+    hp.initial_guess_radius = init_r;
+    std::vector<horizon::HorizonData> in(nh);
+    for (int h = 0; h < nh; ++h) {
+        in[h].centroid = {hz[3 * h], hz[3 * h + 1], hz[3 * h + 2]};
+        in[h].irreducible_mass = mass_circ[2 * h];
+        in[h].circumference_equatorial = mass_circ[2 * h + 1];
+    }
+    horizon::ApparentHorizonFinder f(hp);
+    auto r = f.findCommonHorizon(*b, in);
+    if (!r) return 0;
+    res[0] = r->area;
+    res[1] = r->irreducible_mass;
+    res[2] = r->spin;
+    res[3] = r->circumference_equatorial;
+    res[4] = r->circumference_polar;
+    for (size_t q = 0; q < r->surface_points.size(); ++q)
+        for (int d = 0; d < 3; ++d) surface[3 * q + d] = r->surface_points[q][d];
+    for (int d = 0; d < 3; ++d) cen_id[d] = r->centroid[d];
+    cen_id[3] = r->id;
+    return 1;
+}
+
+// ApparentHorizonFinder::computeSpin (horizon_finder.cpp:553-582) of a horizon
+// with the given circumferences (the only fields it reads; the block is unused).
+double ref_compute_spin(double c_eq, double c_pol) {
+    const int n[3] = {4, 4, 4};
+    const double lo[3] = {0.0, 0.0, 0.0}, hi[3] = {1.0, 1.0, 1.0};
+    auto b = block(geo(n, 4, lo, hi));
+    horizon::HorizonData h;
+    h.circumference_equatorial = c_eq;
+    h.circumference_polar = c_pol;
+    return horizon::ApparentHorizonFinder(horizon::HorizonParams{}).computeSpin(*b, h);
+}
+
 // setFlatSpacetime / setGaugeWaveData (ccz4.cpp:1165-1221) on a zeroed block.
 void ref_init_flat(const int* n, int ng, const double* lo, const double* hi, double* u) {
     auto b = block(geo(n, ng, lo, hi));
