@@ -336,6 +336,32 @@ class Reference:
                                 C.c_int(n_theta), C.c_int(n_phi), C.c_int(l_max), _p(out))
         return out[..., 0] + 1j * out[..., 1]
 
+    def psi4_series(self, g: Geom, states, times, radii, n_theta: int, n_phi: int, l_max: int, spectrum_mode):
+        """The compiled Psi4Extractor over a time series (postprocess.cpp:245-475):
+        extract(states[t], times[t]) for every t, then a dict with the recorded
+        series per (radius index, mode index) as [(time, complex)], strain[r, q],
+        energy[r], extrap[q] and the energy spectrum of spectrum_mode = (l, m, radius
+        index) as [(f, dE/df)]."""
+        nt, nr = len(times), len(radii)
+        nm = (l_max + 1) ** 2 - 4
+        u = np.ascontiguousarray(np.stack([np.asarray(s, dtype=np.float64) for s in states]))
+        count = np.zeros((nr, nm), dtype=np.int32)
+        series = np.zeros((nr, nm, nt, 3))
+        strain = np.zeros((nr, nm, 2))
+        energy = np.zeros(nr)
+        extrap = np.zeros((nm, 2))
+        spec = np.zeros((500, 2))
+        sl, sm, sr = spectrum_mode
+        ns = self.lib.ref_psi4_series(*self._g(g), _p(u), _p(np.ascontiguousarray(times, dtype=np.float64)),
+                                      C.c_int(nt), _p(np.ascontiguousarray(radii, dtype=np.float64)), C.c_int(nr),
+                                      C.c_int(n_theta), C.c_int(n_phi), C.c_int(l_max),
+                                      count.ctypes.data_as(C.POINTER(C.c_int)), _p(series), _p(strain), _p(energy),
+                                      _p(extrap), C.c_int(sl), C.c_int(sm), C.c_int(sr), _p(spec), C.c_int(500))
+        rec = {(r, q): [(series[r, q, t, 0], complex(series[r, q, t, 1], series[r, q, t, 2]))
+                        for t in range(count[r, q])] for r in range(nr) for q in range(nm)}
+        return dict(series=rec, strain=strain[..., 0] + 1j * strain[..., 1], energy=energy,
+                    extrap=extrap[:, 0] + 1j * extrap[:, 1], spectrum=[tuple(x) for x in spec[:min(ns, 500)]])
+
     def find_horizon(self, g: Geom, u, center, max_iterations=200, tol=1e-10, ang_res=50, init_r=1.0):
         """The compiled ApparentHorizonFinder::findHorizon: (found, [area, M_irr, spin,
         C_eq, C_pol], surface points [ang_res * 2 ang_res, 3])."""

@@ -211,6 +211,63 @@ void ref_psi4_modes(const int* n, int ng, const double* lo, const double* hi, co
             }
 }
 
+// A Psi4 time series and its analysis (postprocess.cpp:245-475): extract at
+// times[t] from the block states u + t * block size, t < nt, then per radius r
+// and mode q (l = 2..l_max, m = -l..l):
+//   count[r][q]            the recorded entries,
+//   series[r][q][t][3]     their (time, re, im),
+//   strain[r][q][2]        computeStrain,
+//   energy[r]              computeRadiatedEnergy,
+//   extrap[q][2]           extrapolateToInfinity,
+// and computeEnergySpectrum(sl, sm, radii[sr]) into spec[k][2], k < the return value.
+int ref_psi4_series(const int* n, int ng, const double* lo, const double* hi, const double* u, const double* times,
+                    int nt, const double* radii, int nr, int n_theta, int n_phi, int l_max, int* count,
+                    double* series, double* strain, double* energy, double* extrap, int sl, int sm, int sr,
+                    double* spec, int spec_cap) {
+    auto b = block(geo(n, ng, lo, hi));
+    const size_t per = b->totalSize() * NUM_SPACETIME_VARS;
+    postprocess::GWExtractionParams gp;
+    gp.extraction_radii.assign(radii, radii + nr);
+    gp.l_max = l_max;
+    gp.n_theta = n_theta;
+    gp.n_phi = n_phi;
+    postprocess::Psi4Extractor ex(gp);
+    for (int t = 0; t < nt; ++t) {
+        std::memcpy(b->flatBuffer(), u + t * per, nbytes(*b));
+        ex.extract(*b, times[t]);
+    }
+    const int nm = (l_max + 1) * (l_max + 1) - 4;
+    for (int r = 0; r < nr; ++r) {
+        int q = 0;
+        for (int l = 2; l <= l_max; ++l)
+            for (int m = -l; m <= l; ++m, ++q) {
+                const auto& s = ex.getTimeSeries(l, m, radii[r]);
+                const int rq = r * nm + q;
+                count[rq] = (int)s.size();
+                for (size_t t = 0; t < s.size() && (int)t < nt; ++t) {
+                    series[3 * ((size_t)rq * nt + t)] = s[t].first;
+                    series[3 * ((size_t)rq * nt + t) + 1] = s[t].second.real();
+                    series[3 * ((size_t)rq * nt + t) + 2] = s[t].second.imag();
+                }
+                const std::complex<Real> h = ex.computeStrain(l, m, radii[r]);
+                strain[2 * rq] = h.real();
+                strain[2 * rq + 1] = h.imag();
+                if (r == 0) {
+                    const std::complex<Real> e = ex.extrapolateToInfinity(l, m);
+                    extrap[2 * q] = e.real();
+                    extrap[2 * q + 1] = e.imag();
+                }
+            }
+        energy[r] = ex.computeRadiatedEnergy(radii[r]);
+    }
+    const auto sp = ex.computeEnergySpectrum(sl, sm, radii[sr]);
+    for (size_t k = 0; k < sp.size() && (int)k < spec_cap; ++k) {
+        spec[2 * k] = sp[k].first;
+        spec[2 * k + 1] = sp[k].second;
+    }
+    return (int)sp.size();
+}
+
 // ApparentHorizonFinder::findHorizon (horizon_finder.cpp:310-449). Returns 1 and
 // res = area, irreducible mass, spin, equatorial / polar circumference and
 // surface[N][3] when found, 0 otherwise.
