@@ -173,3 +173,54 @@ def test_initial_data_matches_oracle(oracle_lib):
     gb.gauge_wave(b, -0.1, 1.0)
     np.testing.assert_allclose(b.array, oracle_lib.init_gauge_wave(gw, -0.1, 1.0), rtol=1e-14,
                                atol=1e-15)
+
+
+def _prototypes():
+    """{name: parameter count} of every granite_ccz4_* prototype in the header."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(granite_ccz4_\w+)\s*\(([^;{]*?)\)\s*;", text):
+        args = " ".join(m.group(2).split())
+        out[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_ctypes_argtypes_match_the_header():
+    """Every argtypes list the Python mirror sets has the header's arity."""
+    import granite_b200 as gb
+    lib = gb.load_library()
+    protos = _prototypes()
+    assert set(protos) == set(declared_functions())
+    checked = 0
+    for name, n in protos.items():
+        at = getattr(lib, name).argtypes
+        if at is not None:
+            assert len(at) == n, (name, len(at), n)
+            checked += 1
+    assert checked >= 40
+
+
+def test_ctypes_structs_match_the_c_layout(tmp_path):
+    """Sizes and field offsets of the ctypes mirrors equal the C compiler's."""
+    import granite_b200 as gb
+    mirrors = {"granite_ccz4_params": gb._Params, "granite_block_desc": gb._BlockDesc,
+               "granite_horizon_params": gb._HorizonParams, "granite_horizon": gb._Horizon}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "granite_ccz4.h"', 'int main(void) {']
+    for cname, py in mirrors.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["/usr/bin/gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        cname, field, v = line.split()
+        got[(cname, field)] = int(v)
+    for cname, py in mirrors.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
