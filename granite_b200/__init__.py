@@ -522,15 +522,17 @@ class Evolver:
     def regrid(self, planner, level: int, tagger=None):
         """AMRHierarchy::regrid(level, tagger) (amr.cpp:80-301) on the device state.
 
-        ``planner`` is a ``regrid.RegridPlanner``; ``tagger`` is None (never tags)
-        or (var, threshold) for the chi / lapse gradient tagger, consulted only
-        when no tracking sphere requires level + 1, as in the reference. Returns
-        the GridBlocks added (their host arrays stay zero until ``download``).
+        ``planner`` is a ``regrid.RegridPlanner``; ``tagger`` is None (never tags),
+        (var, threshold) for the chi / lapse gradient tagger, or a list of those
+        (compositeTagger), consulted only when no tracking sphere requires
+        level + 1, as in the reference (``regrid.tagger_fires``). Returns the
+        GridBlocks added (their host arrays stay zero until ``download``).
         """
+        from .regrid import tagger_fires
         if not any(b.level == level for b in self.blocks):
             return []
         if not planner.spheres_require(level + 1):
-            if tagger is None or self.tag_count(level, tagger[0], tagger[1]) == 0:
+            if not tagger_fires(tagger, lambda var, threshold: self.tag_count(level, var, threshold)):
                 return []
         new = [GridBlock(bx.id, bx.level, bx.ncells, bx.lo, bx.hi)
                for bx in planner.plan(level, self.blocks)]

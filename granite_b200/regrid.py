@@ -24,6 +24,21 @@ CHI = 0     # SpacetimeVar::CHI
 LAPSE = 18  # SpacetimeVar::LAPSE
 
 
+def tagger_fires(tagger, count) -> bool:
+    """Whether ``tagger`` tags any interior cell of a level (the early-out of
+    amr.cpp:124-133). ``tagger``: None (never tags), ``(var, threshold)`` for
+    gradientChiTagger (var CHI) or gradientLapseTagger (var LAPSE), or a list of
+    taggers for compositeTagger (amr.cpp:723-731: a cell is tagged when any of
+    them tags it, so the level is when any of them tags a cell of it).
+    ``count(var, threshold)`` is the number of interior cells one tagger tags."""
+    if tagger is None:
+        return False
+    if isinstance(tagger, tuple):
+        var, threshold = tagger
+        return count(var, threshold) > 0
+    return any(tagger_fires(t, count) for t in tagger)
+
+
 @dataclass
 class TrackingSphere:
     """amr.hpp:33-37."""

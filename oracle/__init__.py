@@ -426,6 +426,14 @@ class Reference:
         return int(self.lib.ref_tag_count(*self._g(g), _p(np.ascontiguousarray(u, dtype=np.float64)),
                                           C.c_int(var), C.c_double(threshold)))
 
+    def composite_tag_count(self, g: Geom, u, taggers) -> int:
+        """compositeTagger (amr.cpp:723-731) of [(var, threshold), ...] over the interior."""
+        self.lib.ref_composite_tag_count.restype = C.c_longlong
+        v = (C.c_int * len(taggers))(*[int(t[0]) for t in taggers])
+        th = np.ascontiguousarray([float(t[1]) for t in taggers], dtype=np.float64)
+        return int(self.lib.ref_composite_tag_count(*self._g(g), _p(np.ascontiguousarray(u, dtype=np.float64)),
+                                                    C.c_int(len(taggers)), v, _p(th)))
+
     def bl_conformal_factor(self, masses, positions, x, y, z):
         m = np.ascontiguousarray(masses, dtype=np.float64)
         pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)

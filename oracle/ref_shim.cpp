@@ -696,6 +696,22 @@ long long ref_tag_count(const int* n, int ng, const double* lo, const double* hi
     return count;
 }
 
+// compositeTagger (amr.cpp:723-731) of nt gradient taggers (vars[q], thresholds[q])
+// over the interior: the cells it tags.
+long long ref_composite_tag_count(const int* n, int ng, const double* lo, const double* hi, const double* u,
+                                  int nt, const int* vars, const double* thresholds) {
+    auto b = block(geo(n, ng, lo, hi));
+    std::memcpy(b->flatBuffer(), u, nbytes(*b));
+    std::vector<amr::TaggingFunction> ts;
+    for (int q = 0; q < nt; ++q) ts.push_back(tagger_of(vars[q], thresholds[q]));
+    const amr::TaggingFunction t = amr::compositeTagger(std::move(ts));
+    long long count = 0;
+    for (int k = b->istart(2); k < b->iend(2); ++k)
+        for (int j = b->istart(1); j < b->iend(1); ++j)
+            for (int i = b->istart(0); i < b->iend(0); ++i) count += t(*b, i, j, k) ? 1 : 0;
+    return count;
+}
+
 void ref_hier_destroy(void* hp) { delete static_cast<RefHier*>(hp); }
 
 } // extern "C"

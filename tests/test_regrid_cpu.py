@@ -229,3 +229,33 @@ def test_planner_edge_layouts_match_reference(sphere, max_levels):
     p.add_tracking_sphere(*sphere)
     got = sorted(((b.level, b.ncells, b.lo, b.hi) for b in p.initial_layout()), key=lambda t: t[0])
     assert got == [(lv, g.n, g.lo, g.hi) for g, lv in zip(rh.geoms, rh.levels)]
+
+
+def test_tagger_fires_is_the_composite_early_out(reference_lib):
+    """regrid's tagger test (amr.cpp:124-133) for None, one gradient tagger, or a
+    compositeTagger list (amr.cpp:723-731), from per-tagger counts: equal to the
+    compiled compositeTagger tagging any cell, on a puncture block."""
+    from oracle import Geom
+    from granite_b200.regrid import CHI, LAPSE, tagger_fires
+    calls = []
+
+    def fake(var, threshold):
+        calls.append((var, threshold))
+        return {(CHI, 1.0): 0, (LAPSE, 0.5): 3}.get((var, threshold), 0)
+
+    assert not tagger_fires(None, fake) and calls == []
+    assert not tagger_fires((CHI, 1.0), fake)
+    assert tagger_fires([(CHI, 1.0), (LAPSE, 0.5), (CHI, 9.0)], fake)
+    assert calls[-1] == (LAPSE, 0.5)  # stops at the first tagger that fires
+    assert not tagger_fires([], fake)
+    g = Geom((12, 12, 12), (-3.0, -3.0, -3.0), (3.0, 3.0, 3.0))
+    u = reference_lib.init_brill_lindquist(g, [1.0], [[0.1, 0.0, 0.0]])
+
+    def count(var, threshold):
+        return reference_lib.tag_count(g, u, var, threshold)
+
+    for taggers in ([(CHI, 5.0)], [(CHI, 2.0)], [(CHI, 5.0), (LAPSE, 2.0)], [(CHI, 5.0), (LAPSE, 1.0)],
+                    [(LAPSE, 0.5), (CHI, 0.5)]):
+        assert tagger_fires(taggers, count) == (reference_lib.composite_tag_count(g, u, taggers) > 0)
+        if len(taggers) == 1:
+            assert tagger_fires(taggers[0], count) == (count(*taggers[0]) > 0)
