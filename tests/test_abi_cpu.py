@@ -224,3 +224,13 @@ def test_ctypes_structs_match_the_c_layout(tmp_path):
         assert got[(cname, "size")] == C.sizeof(py), cname
         for f, _ in py._fields_:
             assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
+
+
+def test_missing_library_is_an_error_not_a_fallback(monkeypatch, tmp_path):
+    """Without libgranite_ccz4.so the package raises; there is no other path."""
+    import granite_b200 as gb
+    from granite_b200 import build
+    monkeypatch.setattr(gb, "_LIB", None)
+    monkeypatch.setattr(build, "LIB", str(tmp_path / "libgranite_ccz4.so"))
+    with pytest.raises(gb.GraniteError):
+        gb.load_library(build_if_missing=False)
