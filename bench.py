@@ -431,8 +431,11 @@ def main():
     import torch.distributed as dist
     if world > 1:
         import datetime
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if args.impl == "reference":  # host cores only: the ranks just meet at the end
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=900))
+        else:
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     if args.impl == "reference":
         rc = run_reference(args, w, rank, world)
