@@ -101,10 +101,9 @@ BC_PERIODIC = 1
 
 
 def build(force: bool = False) -> None:
-    """Compile liboracle.so (and oracle/_ref when the reference tree exists)."""
-    lib = os.path.join(HERE, "liboracle.so")
-    if force or not os.path.exists(lib) or not os.path.exists(os.path.join(HERE, "_ref")):
-        subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    """Compile liboracle.so (and oracle/_ref when the reference tree exists);
+    make rebuilds what is older than its sources and nothing else."""
+    subprocess.run(["make", "-s", "-C", HERE] + (["-B"] if force else []) + ["all"], check=True)
 
 
 def _cg(g: Geom) -> _orc_geom:
