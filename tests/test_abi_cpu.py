@@ -16,7 +16,6 @@ import subprocess
 import numpy as np
 import pytest
 
-import oracle
 from oracle import Geom
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

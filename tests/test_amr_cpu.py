@@ -5,7 +5,6 @@ the errors) with a stand-in for the device Evolver that records its calls."""
 import numpy as np
 import pytest
 
-import oracle
 from oracle.hierarchy import RefHierarchy
 from granite_b200 import AMR_GHOSTS, AMR_REFERENCE, PRECISION_FP64, PRECISION_MIXED, GraniteError, GridBlock
 from granite_b200.amr import (AMRHierarchy, AMRParams, SimulationParams, compositeTagger, gradientChiTagger,

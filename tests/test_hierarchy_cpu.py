@@ -7,7 +7,6 @@ evolve_func. The seeded block-hierarchy generator of the product is checked for
 the properties the transfer lists rely on.
 """
 import numpy as np
-import pytest
 
 import oracle
 from oracle import Params

@@ -13,7 +13,6 @@ import math
 import numpy as np
 import pytest
 
-import oracle
 from oracle import Geom
 from granite_b200.horizon import ApparentHorizonFinder, HorizonData, common_horizon_guess, surface_points
 
