@@ -102,8 +102,12 @@ BC_PERIODIC = 1
 
 def build(force: bool = False) -> None:
     """Compile liboracle.so (and oracle/_ref when the reference tree exists);
-    make rebuilds what is older than its sources and nothing else."""
-    subprocess.run(["make", "-s", "-C", HERE] + (["-B"] if force else []) + ["all"], check=True)
+    make rebuilds what is older than its sources and nothing else. Where make
+    cannot run but the libraries are already built, those are used."""
+    r = subprocess.run(["make", "-s", "-C", HERE] + (["-B"] if force else []) + ["all"], capture_output=True,
+                       text=True)
+    if r.returncode != 0 and (force or not os.path.exists(os.path.join(HERE, "liboracle.so"))):
+        raise RuntimeError(f"oracle build failed:\n{r.stdout[-2000:]}\n{r.stderr[-2000:]}")
 
 
 def _cg(g: Geom) -> _orc_geom:
