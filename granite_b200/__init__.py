@@ -234,6 +234,10 @@ class GridBlock:
     def flatBuffer(self):
         return self.array.reshape(-1)
 
+    def rawData(self, var):
+        """Field ``var``'s plane of the flat buffer (grid.hpp:125-129), a view."""
+        return self.array[var].reshape(-1)
+
     def numCells(self):
         return self.ncells
 
