@@ -6,7 +6,8 @@ import numpy as np
 import pytest
 
 from oracle.hierarchy import RefHierarchy
-from granite_b200 import AMR_GHOSTS, AMR_REFERENCE, PRECISION_FP64, PRECISION_MIXED, GraniteError, GridBlock
+from granite_b200 import (AMR_GHOSTS, AMR_REFERENCE, PRECISION_FP64, PRECISION_MIXED, Evolver, GraniteError,
+                          GridBlock)
 from granite_b200.amr import (AMRHierarchy, AMRParams, SimulationParams, compositeTagger, gradientChiTagger,
                               gradientLapseTagger)
 from granite_b200.regrid import CHI, LAPSE
@@ -54,6 +55,18 @@ class FakeEvolver:
 
     def level_time(self, level):
         return 0.5 * level
+
+    # the real Evolver.regrid host logic over stand-in device calls
+    def tag_count(self, level, var, threshold):
+        self.calls.append(("tag_count", level, var, threshold))
+        return 0
+
+    def regrid_add(self, blocks):
+        self.calls.append(("regrid_add", [b.id for b in blocks]))
+        self.blocks.extend(blocks)
+
+    def regrid(self, planner, level, tagger=None):
+        return Evolver.regrid(self, planner, level, tagger)
 
     def close(self):
         self.closed = True
@@ -155,3 +168,30 @@ def test_errors_and_reinitialize():
         AMRHierarchy(AMRParams(refinement_ratio=4), SIM)
     with pytest.raises(GraniteError):
         AMRHierarchy(AMRParams(), SimulationParams(ghost_cells=3))
+
+
+def test_reference_amr_smoke_tests():
+    """tests/amr/test_amr_basic.cpp:85-205 of GRANITE (T1 construction, T2 one
+    level without spheres, T5 a regrid with nothing tagged keeps the level count)
+    on this AMRHierarchy; T3 / T4 (constant-field prolongation / restriction)
+    are device transfers, pinned through the oracle's known answers."""
+    params = AMRParams(max_levels=3, refinement_ratio=2, regrid_interval=4)
+    sim = SimulationParams(ncells=(8, 8, 8), domain_lo=(-1.0, -1.0, -1.0), domain_hi=(1.0, 1.0, 1.0),
+                           ghost_cells=4)
+    AMRHierarchy(params, sim, evolver_factory=FakeEvolver)
+    h = AMRHierarchy(params, sim, evolver_factory=FakeEvolver)
+    h.initialize()
+    assert h.numLevels() >= 1
+    fakes = []
+    h = AMRHierarchy(params, sim, evolver_factory=lambda: fakes.append(FakeEvolver()) or fakes[-1])
+    h.addTrackingSphere((0.0, 0.0, 0.0), 1.0, 2)
+    h.initialize()
+    h.getLevel(0)[0].array[:] = 0.0
+    before = h.numLevels()
+    assert h.regrid(0, None) == [] and h.numLevels() == before == 3
+    assert not any(c[0] == "tag_count" or (c[0] == "regrid_add" and c[1]) for c in fakes[0].calls)
+    assert h.regrid(2, gradientChiTagger(0.1)) == []  # level 3 is beyond max_levels
+    h2 = AMRHierarchy(params, sim, evolver_factory=lambda: fakes.append(FakeEvolver()) or fakes[-1])
+    h2.initialize()
+    assert h2.regrid(0, gradientChiTagger(0.1)) == [] and h2.numLevels() == 1
+    assert ("tag_count", 0, CHI, 0.1) in fakes[1].calls  # no sphere: the tagger is asked
