@@ -1164,7 +1164,7 @@ int granite_ccz4_download_all(void* h, double* const* hosts) {
                            cudaMemcpyDeviceToHost, c->stream),
            "D2H block");
     CK(cudaStreamSynchronize(c->stream), "sync");
-    return GRANITE_OK;
+    return check_errflag(c);  // a stage whose tile wait gave up has left no valid state
 }
 
 int granite_ccz4_download_block(void* h, int i, double* host) {
@@ -1178,7 +1178,7 @@ int granite_ccz4_download_block(void* h, int i, double* host) {
                        cudaMemcpyDeviceToHost, c->stream),
        "D2H block");
     CK(cudaStreamSynchronize(c->stream), "sync");
-    return GRANITE_OK;
+    return check_errflag(c);
 }
 
 // ---------------------------------------------------------------------------
