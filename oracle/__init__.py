@@ -464,11 +464,18 @@ class Reference:
                               C.c_int(clevel), _p(uc), ng)
         return uc
 
-    def rk3_steps(self, p: Params, g: Geom, u, dt: float, nsteps: int, bc: int = BC_SOMMERFELD):
+    def rk3_steps(self, p: Params, g: Geom, u, dt: float, nsteps: int, bc: int = BC_SOMMERFELD,
+                  matter=None):
+        """nsteps RK3 steps; ``matter`` = (rho, Si, Sij, S) held fixed, or None (vacuum)."""
         u = np.array(u, dtype=np.float64, copy=True)
         p6 = p.as6()
-        self.lib.ref_rk3_steps(_p(p6), *self._g(g), _p(u), C.c_double(dt), C.c_int(nsteps),
-                               C.c_int(bc))
+        if matter is None:
+            self.lib.ref_rk3_steps(_p(p6), *self._g(g), _p(u), C.c_double(dt), C.c_int(nsteps),
+                                   C.c_int(bc))
+        else:
+            m = [np.ascontiguousarray(a, dtype=np.float64) for a in matter]
+            self.lib.ref_rk3_steps_matter(_p(p6), *self._g(g), _p(u), C.c_double(dt), C.c_int(nsteps),
+                                          C.c_int(bc), *[_p(a) for a in m])
         return u
 
 

@@ -458,12 +458,26 @@ void ref_fill_level0(const int* n, int ng, const double* lo, const double* hi, d
     std::memcpy(u, b->flatBuffer(), nbytes(*b));
 }
 
+void ref_rk3_steps_matter(const double* p6, const int* n, int ng, const double* lo, const double* hi,
+                          double* u, double dt, int nsteps, int bc, const double* rho, const double* Si,
+                          const double* Sij, const double* S);
+
 // nsteps single-level coarse steps: AMRHierarchy::subcycle(0) (fillGhostZones,
 // evolve, fillGhostZones; amr.cpp:303-330) around the spacetime part of
 // TimeIntegrator::sspRK3Step (main.cpp:673-689) with the reference
 // computeRHSVacuum. bc: 0 = reference zero-gradient + 1/r falloff, 1 = periodic.
 void ref_rk3_steps(const double* p6, const int* n, int ng, const double* lo, const double* hi,
                    double* u, double dt, int nsteps, int bc) {
+    ref_rk3_steps_matter(p6, n, ng, lo, hi, u, dt, nsteps, bc, nullptr, nullptr, nullptr, nullptr);
+}
+
+// The same with matter sources held fixed over the steps (rho[N], Si[N][3],
+// Sij[N][6], S[N], N = totalSize()), every stage calling the reference
+// computeRHS with them as applyRHS does (main.cpp:300-301); all NULL = vacuum
+// (computeRHSVacuum).
+void ref_rk3_steps_matter(const double* p6, const int* n, int ng, const double* lo, const double* hi,
+                          double* u, double dt, int nsteps, int bc, const double* rho, const double* Si,
+                          const double* Sij, const double* S) {
     amr::AMRParams ap;
     ap.max_levels = 1;
     SimulationParams sp;
@@ -487,6 +501,24 @@ void ref_rk3_steps(const double* p6, const int* n, int ng, const double* lo, con
     spacetime::CCZ4Evolution ev(params(p6));
     const orc_geom og = ogeom(st);
     const long N = static_cast<long>(st.totalSize()) * NUM_SPACETIME_VARS;
+    const size_t cells = st.totalSize();
+    std::vector<Real> m_rho, m_S;
+    std::vector<std::array<Real, DIM>> m_si;
+    std::vector<std::array<Real, SYM_TENSOR_COMPS>> m_sij;
+    if (rho) {
+        m_rho.assign(rho, rho + cells);
+        m_S.assign(S, S + cells);
+        m_si.resize(cells);
+        m_sij.resize(cells);
+        for (size_t c = 0; c < cells; ++c) {
+            for (int a = 0; a < 3; ++a) m_si[c][a] = Si[3 * c + a];
+            for (int a = 0; a < 6; ++a) m_sij[c][a] = Sij[6 * c + a];
+        }
+    }
+    auto rhs_of = [&](const GridBlock& in) {
+        if (rho) ev.computeRHS(in, *rhs, m_rho, m_si, m_sij, m_S);
+        else ev.computeRHSVacuum(in, *rhs);
+    };
     auto level_fill = [&]() {
         if (bc == ORC_BC_PERIODIC) orc_fill_periodic(&og, st.flatBuffer());
         else h.fillGhostZones(0);
@@ -508,15 +540,15 @@ void ref_rk3_steps(const double* p6, const int* n, int ng, const double* lo, con
     (void)N;
     for (int s = 0; s < nsteps; ++s) {
         level_fill();
-        ev.computeRHSVacuum(st, *rhs);
+        rhs_of(st);
         combine(*stage, st, 1.0, st, 0.0, 1.0);
         orc_floors(&og, stage->flatBuffer());
         outer(*stage);
-        ev.computeRHSVacuum(*stage, *rhs);
+        rhs_of(*stage);
         combine(*stage, st, 0.75, *stage, 0.25, 0.25);
         orc_floors(&og, stage->flatBuffer());
         outer(*stage);
-        ev.computeRHSVacuum(*stage, *rhs);
+        rhs_of(*stage);
         combine(st, st, 1.0 / 3.0, *stage, 2.0 / 3.0, 2.0 / 3.0);
         orc_floors(&og, st.flatBuffer());
         orc_algebraic(&og, st.flatBuffer());

@@ -219,6 +219,26 @@ def test_oracle_equals_reference_rk3(oracle_lib, reference_lib):
     assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("bc", [oracle.BC_SOMMERFELD, oracle.BC_PERIODIC])
+def test_oracle_equals_reference_rk3_with_matter(oracle_lib, reference_lib, bc):
+    """The oracle's RK3 step with fixed matter sources (the checker of the resident
+    matter path) against the reference's computeRHS with the same sources in
+    every stage, sources from the compiled computeMatterSources."""
+    g = Geom((12, 10, 8), (-3.0, -2.5, -2.0), (3.0, 2.5, 2.0))
+    u = oracle_lib.init_brill_lindquist(g, [1.0], [[0.1, -0.2, 0.05]])
+    u = u + 1e-6 * oracle.hash_noise(g.shape, 6)
+    prim = oracle.seeded_primitives(g, 31, superluminal=0.0)
+    prim[0] *= 1e-3  # a dilute, weakly magnetised fluid: the coupling acts, the state stays finite
+    prim[4] *= 1e-4
+    prim[5:8] *= 1e-2
+    m = reference_lib.matter_sources(g, prim)
+    dt = 0.25 * g.dx[0]
+    a = oracle_lib.rk3_steps(Params(), g, u, dt, 3, bc, matter=m)
+    b = reference_lib.rk3_steps(Params(), g, u, dt, 3, bc, matter=m)
+    assert np.isfinite(a).all() and np.array_equal(a, b)
+    assert not np.array_equal(a, reference_lib.rk3_steps(Params(), g, u, dt, 3, bc))
+
+
 def test_oracle_level_fill_equals_reference(oracle_lib, reference_lib):
     g = Geom((6, 5, 7), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0))
     u = oracle.seeded_state(g, 9)
