@@ -364,7 +364,8 @@ GRANITE_API int granite_ccz4_profile_get(void* ctx, int kernel_class, double* to
  * 4-cell halo into a ring of shared-memory slots with tensor-map (TMA) loads;
  * blocks it cannot map (odd x extent, fewer than 16 x or 4 y/z interior cells)
  * send their level to GRANITE_VARIANT_GLOBAL. A TMA load that does not complete
- * within its wait limit makes the next granite_ccz4_sync return GRANITE_ERR_CUDA.
+ * within its wait limit makes the next granite_ccz4_sync, block download
+ * (download_block / download_all) or compute_rhs_host return GRANITE_ERR_CUDA.
  * All variants compute identical FP64 results. */
 #define GRANITE_VARIANT_GLOBAL 0
 #define GRANITE_VARIANT_SMEM 1
