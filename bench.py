@@ -372,31 +372,59 @@ def roofline(gb, run: Runner, workload, prof_steps, kernel):
 
 
 def accuracy(gb, a: Runner, b: Runner, steps: int):
-    """Mixed (b) against FP64 (a) after the same steps: per-field max deviation
-    relative to the field's tensor scale over all blocks, and ||H||_2 ratio."""
-    a.ev.sync()
-    b.ev.sync()
-    dev = np.zeros(NV)
-    scale = np.zeros(NV)
-    for i in range(len(a.blocks)):
-        ua = np.empty_like(a.blocks[i].array)
-        ub = np.empty_like(ua)
-        a.ev.download(i, ua)
-        b.ev.download(i, ub)
-        it = a.blocks[i].interior()
-        d = np.abs(ua[it] - ub[it]).reshape(NV, -1).max(axis=1)
-        s = np.abs(ua[it]).reshape(NV, -1).max(axis=1)
-        dev = np.maximum(dev, d)
-        scale = np.maximum(scale, s)
+    """Mixed (b) against FP64 (a) after the same steps, on the device: per-field
+    max deviation over the interior of all blocks relative to the largest |FP64|
+    of the field's tensor group, ||H||_2 and ||M||_2 ratios, and whether the
+    FP64 state is still finite."""
+    dev, mag, nf = a.ev.compare_states(b.ev)
     gscale = np.zeros(NV)
     for grp in GROUPS:
-        gscale[grp] = scale[grp].max()
+        gscale[grp] = mag[grp].max()
     rel = dev / np.maximum(gscale, 1e-300)
     ha, ma = a.ev.constraint_norms(-1)
     hb, mb = b.ev.constraint_norms(-1)
+    finite = nf[0] == 0 and bool(np.isfinite(ha) and np.isfinite(ma))
     return {"coarse_steps": steps, "max_rel_dev": float(rel.max()),
             "max_rel_dev_field": int(rel.argmax()), "h_l2_fp64": ha, "h_l2_mixed": hb,
-            "h_l2_ratio": hb / ha if ha else None, "m_l2_ratio": mb / ma if ma else None}
+            "h_l2_ratio": hb / ha if ha else None, "m_l2_ratio": mb / ma if ma else None,
+            "fp64_finite": finite, "nonfinite_fp64": int(nf[0]), "nonfinite_mixed": int(nf[1])}
+
+
+def accuracy_run(gb, a: Runner, b: Runner, steps: int, every: int, seconds: float):
+    """FP64 (a) and mixed (b) stepped side by side from the same initial state
+    (re-uploaded), compared every `every` steps up to `steps` or until the FP64
+    state goes non-finite (the reference's equations on puncture data are not
+    long-term stable) or `seconds` of wall time pass. Reports the comparison
+    at the last step where the FP64 state was finite, the largest deviation up
+    to there, and a thinned history [step, max_rel_dev, h_l2_ratio]."""
+    for r in (a, b):
+        r.ev.upload()
+        r.ev.sync()
+    last, worst, hist, stop = None, 0.0, [], "steps"
+    t0 = time.perf_counter()
+    for s in range(1, steps + 1):
+        a.step()
+        b.step()
+        if s % every and s != steps:
+            continue
+        r = accuracy(gb, a, b, s)
+        if not r["fp64_finite"]:
+            stop = "fp64 state non-finite"
+            first_bad = s
+            break
+        last = r
+        worst = max(worst, r["max_rel_dev"])
+        hist.append([s, r["max_rel_dev"], r["h_l2_ratio"]])
+        if time.perf_counter() - t0 > seconds:
+            stop = "time cap"
+            break
+    out = dict(last) if last else {"coarse_steps": 0}
+    out.update({"steps_requested": steps, "check_every": every, "stopped_by": stop,
+                "max_rel_dev_over_run": worst, "wall_s": time.perf_counter() - t0,
+                "history": hist[:: max(1, len(hist) // 20)] + ([hist[-1]] if hist else [])})
+    if stop == "fp64 state non-finite":
+        out["fp64_nonfinite_by_step"] = first_bad
+    return out
 
 
 def main():
@@ -417,6 +445,15 @@ def main():
     ap.add_argument("--fp64-chi", type=float, default=0.5,
                     help="mixed precision: tiles with a point of chi below this run the FP64 algebra "
                          "(0 = FP32 algebra everywhere)")
+    ap.add_argument("--accuracy-steps", type=int, default=1000,
+                    help="mixed runs: step FP64 and mixed side by side from the initial state for up to "
+                         "this many steps (coarse steps of a hierarchy), or until the FP64 state goes "
+                         "non-finite, and report the deviation there (0 = only after the warm-up)")
+    ap.add_argument("--accuracy-every", type=int, default=10, help="steps between accuracy checks")
+    ap.add_argument("--accuracy-seconds", type=float, default=420.0,
+                    help="wall-time cap of the accuracy run")
+    ap.add_argument("--no-amr-reference", action="store_true",
+                    help="skip the GRANITE_AMR_REFERENCE hierarchy timing")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -453,7 +490,7 @@ def main():
     if prec == gb.PRECISION_MIXED and args.fp64_chi > 0.0:
         run.ev.set_fp64_chi_threshold(args.fp64_chi)
     compare = None
-    if hier and prec == gb.PRECISION_MIXED and not args.no_compare:
+    if prec == gb.PRECISION_MIXED and not args.no_compare:
         compare = Runner(gb, args.workload, w, gb.PRECISION_FP64, variant, local)
 
     for r in (run, compare):
@@ -529,6 +566,34 @@ def main():
                     "mixed_over_fp64": value / cvalue,
                     "fp64_unbatched_value": uvalue, "fp64_unbatched_ms_per_step": ums / ksteps,
                     "fp64_unbatched_steps": ksteps, "mixed_over_fp64_unbatched": value / uvalue}
+
+    # the reference's own hierarchy semantics (GRANITE_AMR_REFERENCE: prolongation
+    # into every fine cell before and after each fine step, amr.cpp:313-329)
+    amr_ref = None
+    if hier and not args.no_amr_reference:
+        amr_ref = {"amr_mode": "reference", "steps": max(1, min(args.steps, 5))}
+        for tag, r in (("mixed", run), ("fp64", compare)):
+            if r is None:
+                continue
+            r.ev.upload()
+            for _ in range(2):
+                r.ev.hierarchy_step(r.dt, r.prec, gb.AMR_REFERENCE)
+            orig = r.step
+            r.step = lambda r=r: r.ev.hierarchy_step(r.dt, r.prec, gb.AMR_REFERENCE)
+            rms, _ = timed_steps(torch, dist, world, local, r, amr_ref["steps"])
+            r.step = orig
+            amr_ref[f"{tag}_value"] = r.points_per_step * amr_ref["steps"] * world / (rms / 1000.0)
+            amr_ref[f"{tag}_ms_per_step"] = rms / amr_ref["steps"]
+        if "fp64_value" in amr_ref:
+            amr_ref["mixed_over_fp64"] = amr_ref["mixed_value"] / amr_ref["fp64_value"]
+
+    # mixed against FP64 from the same initial state, as far as the FP64 state stays finite
+    if compare is not None and args.accuracy_steps > 0:
+        if prec == gb.PRECISION_MIXED and args.fp64_chi > 0.0:
+            run.ev.set_fp64_chi_threshold(args.fp64_chi)
+        acc = accuracy_run(gb, compare, run, args.accuracy_steps, args.accuracy_every, args.accuracy_seconds)
+        acc["fp64_chi_threshold"] = args.fp64_chi
+    if compare is not None:
         compare.ev.close()
         compare = None
 
@@ -561,6 +626,8 @@ def main():
             line["fp32_algebra_all_tiles"] = fp32_line
         if acc:
             line["accuracy_mixed_vs_fp64"] = acc
+        if amr_ref:
+            line["amr_reference"] = amr_ref
         print(json.dumps(line))
     run.ev.close()
     if world > 1:

@@ -149,6 +149,8 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_hierarchy_step_regrid.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.c_int, _REGRID_FN, vp]
     lib.granite_ccz4_level_time.argtypes = [vp, C.c_int, dp]
     lib.granite_ccz4_tag_count.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_longlong)]
+    lib.granite_ccz4_test_withhold_tile_load.argtypes = [vp, C.c_int]
+    lib.granite_ccz4_compare_states.argtypes = [vp, vp, dp, dp, C.POINTER(C.c_longlong)]
     _LIB = lib
     return lib
 
@@ -612,6 +614,22 @@ class Evolver:
 
     def sync(self):
         self.ctx.check(self.ctx.lib.granite_ccz4_sync(self.ctx.h))
+
+    def compare_states(self, other: "Evolver"):
+        """(max |a - b|, max |a|) per field over the interior cells of all blocks
+        (numpy arrays of 22), and the non-finite counts (a, b); a = this
+        context's state, b = other's (same block geometry, same device)."""
+        dev = np.zeros(22)
+        mag = np.zeros(22)
+        nf = (C.c_longlong * 2)()
+        self.ctx.check(self.ctx.lib.granite_ccz4_compare_states(self.ctx.h, other.ctx.h, _dp(dev), _dp(mag), nf))
+        return dev, mag, (nf[0], nf[1])
+
+    def test_withhold_tile_load(self, item: int):
+        """Test switch: the next rk3_step's first stage leaves ring item `item` of
+        the first persistent CTA unissued, so its bounded wait runs out and the
+        next sync() raises GraniteError (GRANITE_ERR_CUDA)."""
+        self.ctx.check(self.ctx.lib.granite_ccz4_test_withhold_tile_load(self.ctx.h, int(item)))
 
     def constraint_norms(self, level: int = -1):
         h = C.c_double()

@@ -158,6 +158,8 @@ struct Ctx {
     long long launches = 0;
     unsigned long long* d_nonfinite = nullptr;
     unsigned int* d_errflag = nullptr;   // set by a TMA stage kernel whose bounded wait gave up
+    int test_withhold = 0;               // armed test switch (StageArgs::test_withhold) of the next rk3_step
+    unsigned long long* d_cmp = nullptr; // granite_ccz4_compare_states results (46 words)
     CUtensorMap* d_tmaps = nullptr;      // TMA variant: 3 maps per resident block (slot 0, 1, 2)
     CUtensorMap* s_tmap = nullptr;       // TMA variant: map of the stateless single-block input
 
@@ -578,6 +580,7 @@ int granite_ccz4_destroy(void* h) {
     cudaFree(c->s_sum);
     cudaFree(c->d_nonfinite);
     cudaFree(c->d_errflag);
+    cudaFree(c->d_cmp);
     cudaFree(c->s_tmap);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -602,6 +605,15 @@ static int check_errflag(Ctx* c) {
         CK(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
         return fail(c, GRANITE_ERR_CUDA, "stage kernel: a tensor-map tile load did not complete within its wait limit");
     }
+    return GRANITE_OK;
+}
+
+int granite_ccz4_test_withhold_tile_load(void* h, int item) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (item < 0) return fail(c, GRANITE_ERR_INVALID, "item must be >= 0");
+    if (c->variant != VARIANT_TMA) return fail(c, GRANITE_ERR_INVALID, "the switch acts on the TMA stage kernel only");
+    c->test_withhold = item + 1;
     return GRANITE_OK;
 }
 
@@ -1257,7 +1269,11 @@ static cudaError_t enqueue_level_step(Ctx* c, int level, double dt, int precisio
     // stage 1: u1 = u + dt L(u)                       main.cpp:673
     a.in_sel = 0; a.n_sel = 0; a.out_sel = 1; a.final_stage = 0;
     a.a1 = 1.0; a.a2 = 0.0; a.a3dt = 1.0 * dt;
-    if ((e = level_stage(c, L, precision, a, &n))) return e;
+    a.test_withhold = c->test_withhold;  // one-shot test switch (eager steps only)
+    c->test_withhold = 0;
+    e = level_stage(c, L, precision, a, &n);
+    a.test_withhold = 0;
+    if (e) return e;
     if ((e = level_ghost(c, L, outer_mode, 1, nullptr, &n))) return e;
     // stage 2: u2 = 3/4 u + 1/4 u1 + 1/4 dt L(u1)      main.cpp:679
     a.in_sel = 1; a.n_sel = 0; a.out_sel = 2;
@@ -1287,7 +1303,7 @@ int granite_ccz4_rk3_step(void* h, int level, double dt, int precision, int bc) 
     if (!std::isfinite(dt)) return fail(c, GRANITE_ERR_INVALID, "dt must be finite");
     CK(cudaSetDevice(c->device), "cudaSetDevice");
     const bool prefill = !c->level_ghosts_valid[level];
-    if (c->profiling || !c->batched) {
+    if (c->profiling || !c->batched || c->test_withhold) {  // (an armed test switch is never captured)
         long long nl = 0;
         cudaError_t e = enqueue_level_step(c, level, dt, precision, bc, prefill, &nl);
         if (e != cudaSuccess) return cuda_fail(c, e, "enqueue step");
@@ -1900,6 +1916,36 @@ int granite_ccz4_constraint_norms(void* h, int level, double* h_l2, double* m_l2
     if (npts == 0) return fail(c, GRANITE_ERR_INVALID, "no points");
     *h_l2 = std::sqrt(sh / (double)npts);
     *m_l2 = std::sqrt(sm / (double)npts);
+    return GRANITE_OK;
+}
+
+int granite_ccz4_compare_states(void* ha, void* hb, double* max_dev, double* max_abs, long long* nonfinite) {
+    Ctx* c = static_cast<Ctx*>(ha);
+    Ctx* o = static_cast<Ctx*>(hb);
+    if (!c || !o) return GRANITE_ERR_INVALID;
+    if (!max_dev || !max_abs || !nonfinite) return fail(c, GRANITE_ERR_INVALID, "null output");
+    if (!c->committed || !o->committed) return fail(c, GRANITE_ERR_INVALID, "commit both contexts first");
+    if (c->device != o->device) return fail(c, GRANITE_ERR_INVALID, "contexts on different devices");
+    if (c->descs.size() != o->descs.size()) return fail(c, GRANITE_ERR_INVALID, "different block counts");
+    for (size_t i = 0; i < c->descs.size(); ++i)
+        for (int d = 0; d < 3; ++d)
+            if (c->descs[i].ncells[d] != o->descs[i].ncells[d])
+                return fail(c, GRANITE_ERR_INVALID, "different block geometry");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    if (!c->d_cmp) CK(cudaMalloc(&c->d_cmp, (2 * NV + 2) * sizeof(unsigned long long)), "cudaMalloc(compare)");
+    CK(cudaStreamSynchronize(o->stream), "cudaStreamSynchronize");  // the other context's steps have landed
+    CK(launch_compare_states(c->d_blocks, o->d_blocks, (int)c->descs.size(), c->d_cmp, c->stream),
+       "launch compare");
+    ++c->launches;
+    unsigned long long r[2 * NV + 2];
+    CK(cudaMemcpyAsync(r, c->d_cmp, sizeof(r), cudaMemcpyDeviceToHost, c->stream), "D2H compare");
+    CK(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    for (int v = 0; v < NV; ++v) {
+        std::memcpy(&max_dev[v], &r[v], sizeof(double));
+        std::memcpy(&max_abs[v], &r[NV + v], sizeof(double));
+    }
+    nonfinite[0] = (long long)r[2 * NV];
+    nonfinite[1] = (long long)r[2 * NV + 1];
     return GRANITE_OK;
 }
 

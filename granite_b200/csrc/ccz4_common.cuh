@@ -65,6 +65,10 @@ struct StageArgs {
     // Per-tile precision (nullable): the launch covers only tiles ti with tile_prec[ti] == want_prec.
     const unsigned char* tile_prec;
     int want_prec;
+    // Test switch of the TMA variant, 0 = off: CTA 0 never issues ring item
+    // test_withhold - 1, so its bounded wait for that item runs out (no copy is
+    // in flight for it) and the launch reports through errflag.
+    int test_withhold;
 };
 
 __host__ __device__ inline long long cell_index(const DevBlock& b, int i, int j, int k) {

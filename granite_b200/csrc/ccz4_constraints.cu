@@ -380,10 +380,100 @@ __global__ void noalloc_norms_kernel(const double* __restrict__ p, int n, double
 }
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
-double* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};  // device address of g_noalloc_partials per device
+// Device address of g_noalloc_partials per device, and the context it was looked
+// up in: a device reset (or anything else that recreates the primary context)
+// can load the module at a new address, so a changed context means a new lookup.
+double* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+void* g_noalloc_ctx[NOALLOC_MAX_DEVICES] = {};
 std::mutex g_noalloc_mutex;
 
+// The current driver context (CUcontext as an opaque pointer), through the
+// runtime's driver entry point (no link against libcuda); null if unavailable.
+void* current_driver_context() {
+    using GetCurrent = int (*)(void**);
+    static GetCurrent fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<GetCurrent>(f);
+    });
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
+
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// State comparison of two block lists of identical geometry (diagnostics):
+// per field, the largest |a - b| and |a| over the interior cells of slot 0 of
+// every block, as the bits of non-negative doubles (atomicMax on the bit
+// patterns orders them as values), and the counts of non-finite values in a
+// and in b (out[44], out[45]). NaN differences do not enter the maxima.
+// ---------------------------------------------------------------------------
+namespace {
+
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* p, double v) {
+    atomicMax(p, (unsigned long long)__double_as_longlong(v));
+}
+
+__global__ void __launch_bounds__(256)
+    compare_states_kernel(const DevBlock* __restrict__ A, const DevBlock* __restrict__ Bl, unsigned long long* out) {
+    const DevBlock& a = A[blockIdx.y];
+    const DevBlock& b = Bl[blockIdx.y];
+    const long long n = (long long)a.n[0] * a.n[1] * a.n[2];
+    double dev[NV], mag[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) dev[v] = mag[v] = 0.0;
+    unsigned long long bad_a = 0, bad_b = 0;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p % a.n[0]), j = (int)((p / a.n[0]) % a.n[1]), k = (int)(p / ((long long)a.n[0] * a.n[1]));
+        const long long c = cell_index(a, i + NG, j + NG, k + NG);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const double x = __ldg(a.buf[0] + (long long)v * a.stride + c);
+            const double y = __ldg(b.buf[0] + (long long)v * b.stride + c);
+            bad_a += !isfinite(x);
+            bad_b += !isfinite(y);
+            dev[v] = fmax(dev[v], fabs(x - y));
+            mag[v] = fmax(mag[v], fabs(x));
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        for (int o = 16; o > 0; o >>= 1) {
+            dev[v] = fmax(dev[v], __shfl_down_sync(0xffffffffu, dev[v], o));
+            mag[v] = fmax(mag[v], __shfl_down_sync(0xffffffffu, mag[v], o));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        bad_a += __shfl_down_sync(0xffffffffu, bad_a, o);
+        bad_b += __shfl_down_sync(0xffffffffu, bad_b, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            atomic_max_nonneg(out + v, dev[v]);
+            atomic_max_nonneg(out + NV + v, mag[v]);
+        }
+        if (bad_a) atomicAdd(out + 2 * NV, bad_a);
+        if (bad_b) atomicAdd(out + 2 * NV + 1, bad_b);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_compare_states(const DevBlock* a, const DevBlock* b, int nblocks, unsigned long long* out,
+                                  cudaStream_t stream) {
+    if (nblocks <= 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(out, 0, (2 * NV + 2) * sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return e;
+    compare_states_kernel<<<dim3(32, nblocks), 256, 0, stream>>>(a, b, out);
+    return cudaGetLastError();
+}
 
 }  // namespace granite_b200
 
@@ -401,16 +491,15 @@ extern "C" GRANITE_API int granite_ccz4_constraint_norms_noalloc(const granite_b
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return GRANITE_ERR_NO_DEVICE;
     double* partials = nullptr;
     {
-        // once per device, with that device current: host code must not use the
-        // array's name as a device address
+        // once per device (and again if its context was recreated), with that
+        // device current: host code must not use the array's name as a device address
+        const void* ctx = current_driver_context();
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_addr[dev]) {
+        if (!g_noalloc_addr[dev] || g_noalloc_ctx[dev] != ctx) {
             void* p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) {
-                cudaGetLastError();
-                return GRANITE_ERR_CUDA;
-            }
+            if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) return GRANITE_ERR_CUDA;
             g_noalloc_addr[dev] = static_cast<double*>(p);
+            g_noalloc_ctx[dev] = const_cast<void*>(ctx);
         }
         partials = g_noalloc_addr[dev];
     }
@@ -431,8 +520,21 @@ extern "C" GRANITE_API int granite_ccz4_constraint_norms_noalloc(const granite_b
     B.inv4hh[2] = 1.0 / (4.0 * B.dx[1] * B.dx[2]);
     B.level = b->level;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    constraints_noalloc_kernel<<<(unsigned)ntiles, dim3(CT_X, CT_Y, 1), 0, s>>>(B, u_dev, ntx, nty, partials);
-    const double npts = (double)b->ncells[0] * b->ncells[1] * b->ncells[2];
-    noalloc_norms_kernel<<<1, 256, 0, s>>>(partials, (int)ntiles, npts, norms_dev);
-    return cudaGetLastError() == cudaSuccess ? GRANITE_OK : GRANITE_ERR_CUDA;
+    // cudaLaunchKernel returns the status of each launch itself, so the result
+    // reflects this call only (an error left by the caller's earlier work is
+    // neither reported here nor cleared)
+    {
+        void* args[] = {&B, const_cast<double**>(&u_dev), const_cast<int*>(&ntx), const_cast<int*>(&nty),
+                        &partials};
+        if (cudaLaunchKernel(reinterpret_cast<const void*>(constraints_noalloc_kernel), dim3((unsigned)ntiles),
+                             dim3(CT_X, CT_Y, 1), args, 0, s) != cudaSuccess)
+            return GRANITE_ERR_CUDA;
+    }
+    double npts = (double)b->ncells[0] * b->ncells[1] * b->ncells[2];
+    int n = (int)ntiles;
+    void* args[] = {&partials, &n, &npts, &norms_dev};
+    if (cudaLaunchKernel(reinterpret_cast<const void*>(noalloc_norms_kernel), dim3(1), dim3(256), args, 0, s) !=
+        cudaSuccess)
+        return GRANITE_ERR_CUDA;
+    return GRANITE_OK;
 }

@@ -172,6 +172,12 @@ cudaError_t launch_horizon_surface(const DevBlock& B, const double* u, const Hor
 cudaError_t launch_lapse_minima(const DevBlock& B, const double* u, long long* out, unsigned int* count,
                                 unsigned int cap, cudaStream_t stream);
 
+// Per field v: out[v] = max |a - b|, out[22 + v] = max |a| over the interior
+// cells of slot 0 of blocks a[i], b[i] (i < nblocks, identical geometry), as the
+// bits of non-negative doubles; out[44], out[45] = non-finite values in a, in b.
+cudaError_t launch_compare_states(const DevBlock* a, const DevBlock* b, int nblocks, unsigned long long* out,
+                                  cudaStream_t stream);
+
 // Deterministic fixed-order sum of n partial pairs into out[2].
 cudaError_t launch_sum_partials(const double* partials, int n, double* out, cudaStream_t stream);
 

@@ -243,6 +243,7 @@ struct TmaSource {
     bool failed;       // a wait of this thread gave up (at item fail_q); thread 0 then stops issuing
     unsigned int* err;
     int fail_q;
+    int withhold;      // test switch: 1 + the item CTA 0 leaves unissued (0: none)
 
     // Tile of the CTA's r-th round: blockIdx.x + r gridDim.x, or with per-tile
     // precision (SEL) the r-th tile of that sequence whose flag the launch takes.
@@ -256,6 +257,7 @@ struct TmaSource {
     __device__ __forceinline__ void issue(int q) const {
         const int ti = round_tile(q / NV);
         if (ti >= ntiles) return;
+        if (withhold != 0 && q == withhold - 1 && blockIdx.x == 0) return;  // test switch: never issued
         const Tile t = tiles[ti];
         const int s = q % NBUF;
         const unsigned bar = bar0 + 8u * s;
@@ -818,7 +820,7 @@ __global__ void __launch_bounds__(V4_NT, 1)
     const int lx = tid % V4_TX, ly = (tid / V4_TX) % V4_TY, lz = tid / (V4_TX * V4_TY);
     TmaSource<NBUF, SEL> S{blocks, tiles, static_cast<const unsigned char*>(A.tmaps), ntiles, A.in_sel, ring, bar0,
                          nullptr, (lx + 4) + R::BX * ((ly + 4) + R::BY * (lz + 4)), 0, false,
-                         A.errflag, 0};
+                         A.errflag, 0, A.test_withhold};
     if (tid == 0)
         for (int q = 0; q < NBUF - 1; ++q) S.issue(q);
     for (int r = 0;; ++r) {
@@ -839,13 +841,17 @@ __global__ void __launch_bounds__(V4_NT, 1)
     }
     // Every issued item was consumed (issue() skips items past this CTA's last
     // tile), so no copy into the ring is in flight when the CTA exits. If
-    // thread 0 gave up waiting at item f, it issued nothing after item
-    // f + NBUF - 1: give those loads one more bounded wait before exiting.
+    // thread 0 gave up waiting at item f (which already had its full wait), it
+    // had issued items up to f + NBUF - 1 and nothing after: each of
+    // f + 1 .. f + NBUF - 1 that was issued gets its own bounded wait, whatever
+    // the others do, so no copy into this CTA's shared memory outlives it.
     if (S.failed && tid == 0) {
         const int f = S.fail_q;
-        S.failed = false;
-        for (int q = f; q < f + NBUF && !S.failed; ++q)
-            if (S.round_tile(q / NV) < ntiles) S.wait(q);
+        for (int q = f + 1; q < f + NBUF; ++q) {
+            if (S.round_tile(q / NV) >= ntiles) continue;
+            S.failed = false;
+            S.wait(q);
+        }
     }
 }
 

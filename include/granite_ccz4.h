@@ -327,6 +327,16 @@ GRANITE_API int granite_ccz4_level_time(void* ctx, int level, double* t);
  * interior points of the given level (-1 = all levels). Deterministic. */
 GRANITE_API int granite_ccz4_constraint_norms(void* ctx, int level, double* h_l2, double* m_l2);
 
+/* Compares the evolved states (slot 0) of two committed contexts of identical
+ * block geometry on one device, e.g. the same hierarchy stepped in
+ * GRANITE_PRECISION_FP64 and _MIXED (no counterpart in the reference). Per
+ * field v over the interior cells of all blocks: max_dev[v] = max |a - b|,
+ * max_abs[v] = max |a| (22 values each; NaN differences are left out of the
+ * maxima); nonfinite[0], nonfinite[1] = the non-finite values in a and in b.
+ * Waits for both contexts' streams. */
+GRANITE_API int granite_ccz4_compare_states(void* ctx_a, void* ctx_b, double* max_dev, double* max_abs,
+                                            long long* nonfinite);
+
 /* Number of non-finite chi/alpha values met by the floors since the last call
  * (the floors repair them, main.cpp:586-608); a health signal, not an error. */
 GRANITE_API int granite_ccz4_nonfinite_count(void* ctx, long long* count);
@@ -374,6 +384,17 @@ GRANITE_API int granite_ccz4_profile_get(void* ctx, int kernel_class, double* to
 #define GRANITE_VARIANT_TMA 4
 GRANITE_API int granite_ccz4_set_kernel_variant(void* ctx, int variant);
 GRANITE_API int granite_ccz4_get_kernel_variant(const void* ctx, int* variant);
+
+/* Test switch of the wait limit above (no counterpart in the reference, which
+ * has no device waits; its failure detection is the NaN scan of
+ * main.cpp:525-568): the next granite_ccz4_rk3_step runs uncaptured and, in its
+ * first stage launch, the first persistent CTA never issues ring item `item`
+ * (item q = field q % 22 of the CTA's tile round q / 22). Nothing is in flight
+ * for that item, so the CTA's bounded waits run out (about 2 s), the step's
+ * state is garbage, and the next granite_ccz4_sync returns GRANITE_ERR_CUDA
+ * with the wait-limit message; the sync after that returns GRANITE_OK and the
+ * context keeps working. One-shot; TMA variant only. */
+GRANITE_API int granite_ccz4_test_withhold_tile_load(void* ctx, int item);
 
 /* Per-tile precision of GRANITE_PRECISION_MIXED steps (no counterpart in the
  * reference): in every RK stage of granite_ccz4_rk3_step /

@@ -226,6 +226,8 @@ class HierarchyOracle:
                     inx = (X >= gc.lo[0]) & (X < gc.hi[0])
                     iny = (Y >= gc.lo[1]) & (Y < gc.hi[1])
                     inz = (Z >= gc.lo[2]) & (Z < gc.hi[2])
+                    if not (inx.any() and iny.any() and inz.any()):
+                        continue
                     m = ghost & inz[:, None, None] & iny[None, :, None] & inx[None, None, :]
                     if m.any():
                         pro.append((c, np.ascontiguousarray(m.astype(np.uint8))))
@@ -237,6 +239,8 @@ class HierarchyOracle:
                 inx = (X >= ga.lo[0]) & (X < ga.hi[0])
                 iny = (Y >= ga.lo[1]) & (Y < ga.hi[1])
                 inz = (Z >= ga.lo[2]) & (Z < ga.hi[2])
+                if not (inx.any() and iny.any() and inz.any()):
+                    continue
                 m = ghost & inz[:, None, None] & iny[None, :, None] & inx[None, None, :]
                 if not m.any():
                     continue

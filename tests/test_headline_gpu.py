@@ -1,0 +1,101 @@
+"""Parity at the benchmark sizes (plain FP64).
+
+* The 4-level binary-puncture hierarchy bench.py times (376 blocks, 8.39 M
+  interior points, 9.4 GB resident): one subcycled coarse step (15 level steps,
+  45 stage launches) in GRANITE_AMR_GHOSTS against the hierarchy oracle's
+  restated Berger-Oliger step (oracle/hierarchy.py, whose per-block RK3 stage
+  is pinned bit for bit to the compiled reference's computeRHS), with the
+  scaled per-point bound of the multi-step tests on every block and the
+  constraint norms of all levels.
+* The single-puncture workload at its configured 128^3 (dx = 0.25, 1e-10
+  noise): 20 RK3 steps against the oracle, state and constraint norms.
+
+Both run the OpenMP oracle on the host's cores; they take minutes, not seconds.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from oracle import Geom, Params
+from oracle.hierarchy import HierarchyOracle
+
+from test_parity_gpu import parity
+
+pytestmark = pytest.mark.gpu
+
+RTOL_STEPS = 1e-10
+
+
+@pytest.fixture(scope="module")
+def gb():
+    import granite_b200
+    return granite_b200
+
+
+def test_binary_hierarchy_full_size_one_coarse_step(gb, oracle_lib):
+    h = gb.make_binary_hierarchy()
+    blocks = gb.block_states(h, noise=1e-10, seed=12345)
+    geoms = [Geom(tuple(b.ncells), tuple(b.lo), tuple(b.hi)) for b in h.blocks]
+    levels = [b.level for b in h.blocks]
+    assert len(blocks) == 376 and h.interior_points() == 8388608
+    dt = 0.25 * h.level_dx[0]
+
+    ev = gb.Evolver(gb.CCZ4Params(device=0), gb.VARIANT_TMA)
+    for b in blocks:
+        ev.add_block(b)
+    ev.commit()
+    ev.upload()
+    ev.hierarchy_step(dt, gb.PRECISION_FP64, gb.AMR_GHOSTS)
+    ev.download()  # into the blocks' host arrays
+    h_gpu, m_gpu = ev.constraint_norms(-1)
+    ev.close()
+
+    ho = HierarchyOracle(geoms, levels, oracle_lib)
+    init = gb.block_states(h, noise=1e-10, seed=12345)
+    for i, b in enumerate(init):
+        ho.u[i][...] = b.array
+    del init
+    ho.step(Params(), dt, "ghosts", 1)
+
+    worst = 0.0
+    for i, b in enumerate(blocks):
+        it = geoms[i].interior()
+        worst = max(worst, parity(b.array[it], ho.u[i][it], rtol=RTOL_STEPS,
+                                  what=f"block {i} level {levels[i]}"))
+    sh = sm = 0.0
+    npts = 0
+    for i, g in enumerate(geoms):
+        a, c, n = oracle_lib.constraint_sums(g, ho.u[i])
+        sh += a
+        sm += c
+        npts += n
+    h_ref, m_ref = np.sqrt(sh / npts), np.sqrt(sm / npts)
+    assert abs(h_gpu - h_ref) <= 1e-10 * h_ref, (h_gpu, h_ref)
+    assert abs(m_gpu - m_ref) <= 1e-10 * m_ref, (m_gpu, m_ref)
+    assert worst <= 1.0
+
+
+def test_single_puncture_128_twenty_steps(gb, oracle_lib):
+    g = Geom((128, 128, 128), (-16.0, -16.0, -16.0), (16.0, 16.0, 16.0))
+    u = oracle_lib.init_brill_lindquist(g, [1.0], [[0.0, 0.0, 0.0]], r_floor=0.5 * g.dx[0])
+    u = oracle.add_noise(u, 1e-10, 12345)
+    dt = 0.25 * g.dx[0]
+    n = 20
+
+    ev = gb.Evolver(gb.CCZ4Params(device=0), gb.VARIANT_TMA)
+    b = gb.GridBlock(0, 0, g.n, g.lo, g.hi)
+    b.array[...] = u
+    ev.add_block(b)
+    ev.commit()
+    ev.upload()
+    for _ in range(n):
+        ev.rk3_step(0, dt, gb.PRECISION_FP64, gb.BC_REFERENCE)
+    ev.download()
+    h, m = ev.constraint_norms(0)
+    ev.close()
+
+    ref = oracle_lib.rk3_steps(Params(), g, u, dt, n)
+    parity(b.array, ref, rtol=RTOL_STEPS, what="128^3 puncture, 20 steps")
+    h_ref, m_ref, npts = oracle_lib.constraint_sums(g, ref)
+    assert abs(h - np.sqrt(h_ref / npts)) <= 1e-10 * np.sqrt(h_ref / npts)
+    assert abs(m - np.sqrt(m_ref / npts)) <= 1e-10 * np.sqrt(m_ref / npts)

@@ -8,7 +8,8 @@ the caller's device buffer with a fixed scratch array inside the library.
 Checked here through the C ABI against the context-based
 granite_ccz4_constraint_norms on the same state, for two calls in a row (the
 second on a different state, so stale partial sums from the first call would
-show), plus the rejection of a block beyond the fixed capacity. The file is
+show), that the second call leaves the device's free memory unchanged, plus
+the rejection of a block beyond the fixed capacity. The file is
 named to be collected last; it must also pass alone in a fresh process (the
 first call does the per-device set-up).
 """
@@ -60,13 +61,19 @@ def test_noalloc_norms_match_context_path():
     torch.cuda.set_device(0)
     stream = torch.cuda.current_stream()
     out = torch.zeros(2, dtype=torch.float64, device="cuda:0")
-    for u in states:  # two calls in a row through the same static scratch
+    for call, u in enumerate(states):  # two calls in a row through the same static scratch
         u_dev = torch.from_numpy(u.reshape(-1).copy()).to("cuda:0")
         out.fill_(-1.0)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info(0)[0]
         rc = fn(C.byref(desc), C.c_void_p(u_dev.data_ptr()), C.c_void_p(out.data_ptr()),
                 C.c_void_p(stream.cuda_stream))
         assert rc == 0
         torch.cuda.synchronize()
+        if call == 1:
+            # after the first call has loaded the library's device data, a call
+            # takes no device memory at all
+            assert torch.cuda.mem_get_info(0)[0] == free_before
         h, m = out.cpu().numpy()
         h_ref, m_ref = _context_norms(gb, g, u)
         assert h_ref > 0 and m_ref > 0
