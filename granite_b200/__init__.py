@@ -33,6 +33,9 @@ AMR_GHOSTS = 1
 KERNEL_STAGE, KERNEL_GHOST, KERNEL_TRANSFER, KERNEL_CONSTRAINTS = 0, 1, 2, 3
 VARIANT_GLOBAL, VARIANT_SMEM, VARIANT_GLOBAL_R168, VARIANT_GLOBAL_R128, VARIANT_TMA = 0, 1, 2, 3, 4
 VARIANT_NAMES = {"global": 0, "smem": 1, "global_r168": 2, "global_r128": 3, "tma": 4}
+# configurations of the TMA stage kernel and the block-size classes they are tuned for
+STAGE_CONFIGS = 5
+STAGE_CLASS_EDGES = (16, 24, 32, 48, 64, 96)
 
 _ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "no sm_100 device", -4: "out of memory",
            -5: "non-finite state", -6: "unsupported", -7: "timeout"}
@@ -150,6 +153,12 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_level_time.argtypes = [vp, C.c_int, dp]
     lib.granite_ccz4_tag_count.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_longlong)]
     lib.granite_ccz4_test_withhold_tile_load.argtypes = [vp, C.c_int]
+    ip_ = C.POINTER(C.c_int)
+    lib.granite_ccz4_set_stage_config.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+    lib.granite_ccz4_get_stage_config.argtypes = [vp, C.c_int, C.c_int, ip_]
+    lib.granite_ccz4_force_stage_config.argtypes = [vp, C.c_int]
+    lib.granite_ccz4_stage_config_info.argtypes = [C.c_int, ip_, ip_, ip_, ip_]
+    lib.granite_ccz4_block_stage_class.argtypes = [C.POINTER(_BlockDesc), ip_]
     lib.granite_ccz4_compare_states.argtypes = [vp, vp, dp, dp, C.POINTER(C.c_longlong)]
     _LIB = lib
     return lib
@@ -164,6 +173,28 @@ def _dp(a):
 # ---------------------------------------------------------------------------
 # GridBlock (include/granite/core/grid.hpp:44-162)
 # ---------------------------------------------------------------------------
+
+def stage_config_info(cfg: int) -> dict:
+    """Tile depth, ring slots and shared-memory options of a TMA configuration."""
+    lib = load_library()
+    v = [C.c_int() for _ in range(4)]
+    rc = lib.granite_ccz4_stage_config_info(int(cfg), *[C.byref(x) for x in v])
+    if rc != GRANITE_OK:
+        raise GraniteError(rc, f"unknown stage configuration {cfg}")
+    return {"tile": (16, 4, v[0].value), "ring_slots": v[1].value, "shared_input": bool(v[2].value),
+            "shared_hessian": bool(v[3].value)}
+
+
+def block_stage_class(ncells) -> int:
+    """Block-size class (index into STAGE_CLASS_EDGES) of a block with these interior cells."""
+    lib = load_library()
+    d = block_desc(ncells, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0))
+    v = C.c_int()
+    rc = lib.granite_ccz4_block_stage_class(C.byref(d), C.byref(v))
+    if rc != GRANITE_OK:
+        raise GraniteError(rc, "bad block size")
+    return v.value
+
 
 def measure_fma_rate(device: int = 0, precision: int = 0) -> float:
     """Sustained FMA rate of a device in TFLOP/s: FP64 (precision 0) or FP32 (1)."""
@@ -442,6 +473,26 @@ class Evolver:
 
     def set_batching(self, batched: bool):
         self.ctx.check(self.ctx.lib.granite_ccz4_set_batching(self.ctx.h, int(bool(batched))))
+
+    def set_stage_config(self, precision: int, cls: int, cfg: int):
+        """TMA configuration of block-size class cls (-1: every class) for steps
+        in `precision`; cfg -1 restores the built-in default. Before commit."""
+        self.ctx.check(self.ctx.lib.granite_ccz4_set_stage_config(self.ctx.h, int(precision), int(cls), int(cfg)))
+
+    def stage_config(self, precision: int, cls: int) -> int:
+        v = C.c_int()
+        self.ctx.check(self.ctx.lib.granite_ccz4_get_stage_config(self.ctx.h, int(precision), int(cls), C.byref(v)))
+        return v.value
+
+    def force_stage_config(self, cfg: int):
+        """One TMA configuration for every block and precision (-1: the per-class table). Before commit."""
+        self.ctx.check(self.ctx.lib.granite_ccz4_force_stage_config(self.ctx.h, int(cfg)))
+
+    def apply_stage_table(self, table: dict):
+        """A tuner table {"fp64": [cfg per class], "mixed": [...]} (granite_b200.tuner)."""
+        for name, prec in (("fp64", PRECISION_FP64), ("mixed", PRECISION_MIXED)):
+            for cls, cfg in enumerate(table.get(name, [])):
+                self.set_stage_config(prec, cls, int(cfg))
 
     def set_fp64_chi_threshold(self, chi_fp64: float):
         """MIXED steps: tiles with a point of chi below chi_fp64 run the FP64 algebra (0 = off)."""

@@ -31,10 +31,10 @@ using namespace granite_b200;
 namespace granite_b200 {
 
 // Tensor map of one block buffer for the TMA stage kernel: 4-D (x, y, z,
-// field) over the cells incl. ghosts, FP64, box = 16x4x4 tile + 4-cell halo,
-// no swizzle, zero fill outside the block. The driver's encoder is looked up
-// once through the runtime (no link against libcuda).
-bool encode_block_tmap(void* map128, const double* base, const DevBlock& d) {
+// field) over the cells incl. ghosts, FP64, box = 16 x 4 x tz tile + 4-cell
+// halo, no swizzle, zero fill outside the block. The driver's encoder is looked
+// up once through the runtime (no link against libcuda).
+bool encode_block_tmap(void* map128, const double* base, const DevBlock& d, int tz) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     static std::once_flag once;
     std::call_once(once, [] {
@@ -50,11 +50,12 @@ bool encode_block_tmap(void* map128, const double* base, const DevBlock& d) {
     if (!encode || !base) return false;
     // global address 16-byte aligned, every stride a multiple of 16 bytes (x extent even)
     if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (d.tx & 1) != 0) return false;
-    if (d.tx < TMA_BOX[0] || d.ty < TMA_BOX[1] || d.tz < TMA_BOX[2]) return false;
+    const int bz = tz + 8;
+    if (d.tx < TMA_BOX_X || d.ty < TMA_BOX_Y || d.tz < bz) return false;
     const cuuint64_t dims[4] = {(cuuint64_t)d.tx, (cuuint64_t)d.ty, (cuuint64_t)d.tz, (cuuint64_t)NV};
     const cuuint64_t strides[3] = {(cuuint64_t)d.tx * sizeof(double), (cuuint64_t)d.tx * d.ty * sizeof(double),
                                    (cuuint64_t)d.stride * sizeof(double)};
-    const cuuint32_t box[4] = {(cuuint32_t)TMA_BOX[0], (cuuint32_t)TMA_BOX[1], (cuuint32_t)TMA_BOX[2], 1};
+    const cuuint32_t box[4] = {(cuuint32_t)TMA_BOX_X, (cuuint32_t)TMA_BOX_Y, (cuuint32_t)bz, 1};
     const cuuint32_t estride[4] = {1, 1, 1, 1};
     const CUresult r = encode(static_cast<CUtensorMap*>(map128), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
                               const_cast<double*>(base), dims, strides, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -67,6 +68,11 @@ bool encode_block_tmap(void* map128, const double* base, const DevBlock& d) {
 
 namespace {
 
+// Stage configuration per (precision: FP64, MIXED) and block-size class
+// (GRANITE_STAGE_CLASS_EDGES) until a caller sets its own: the winners of the
+// autotuner (granite_b200/tuner.py) on a B200.
+constexpr int DEFAULT_CLASS_CFG[2][GRANITE_STAGE_CLASSES] = {{0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0}};
+
 static_assert(sizeof(CUtensorMap) == 128, "tensor maps are 128 bytes");
 static_assert(alignof(CUtensorMap) >= 64, "tensor maps are 64-byte aligned");
 
@@ -78,11 +84,21 @@ struct Graph {
     long long launches = 0;
 };
 
+// Tiles of one stage-kernel configuration within a level's work-list: one launch.
+struct StageGroup {
+    int cfg;          // TMA configuration (TMA_CFGS), 0 for the other variants
+    int first, count; // range of the level's tiles
+};
+
 struct LevelLists {
     std::vector<int> blocks;
     int variant = VARIANT_GLOBAL;  // stage kernel of this level: the context's variant, or GLOBAL
                                    // when a block cannot be mapped for TMA
-    Tile* d_tiles = nullptr;   // stage-kernel tiles (shape of the level's variant)
+    // stage-kernel tiles: per precision (0 FP64, 1 MIXED) grouped by
+    // configuration (groups), each block's tiles contiguous (tile_range)
+    Tile* d_tiles = nullptr;
+    std::vector<StageGroup> groups[2];
+    std::vector<int> block_cfg[2];  // per block of the level: its configuration
     int ntiles = 0;
     unsigned char* d_flags = nullptr;  // per-tile precision of MIXED steps (1 = FP64 algebra)
     Tile* d_mtiles = nullptr;  // constraint-monitor tiles (variant-0 shape)
@@ -90,8 +106,8 @@ struct LevelLists {
     GhostItem* d_ghost = nullptr;
     int nghost = 0;
     long long interior_points = 0;
-    // per block of the level: [first, first + count) of its tiles / ghost chunks
-    std::vector<std::pair<int, int>> tile_range, ghost_range;
+    // per block of the level: [first, first + count) of its tiles (per precision) / ghost chunks
+    std::vector<std::pair<int, int>> tile_range[2], ghost_range;
 };
 
 // Device copy of a list of transfer boxes and the chunks that cover them.
@@ -146,6 +162,10 @@ struct Ctx {
     granite_ccz4_params p{};
     int device = 0;
     int variant = VARIANT_TMA;     // stage-kernel variant (granite_ccz4_set_kernel_variant)
+    // TMA configuration per precision and block-size class (granite_ccz4_set_stage_config);
+    // forced_cfg >= 0 overrides the table for every block
+    int class_cfg[2][GRANITE_STAGE_CLASSES];
+    int forced_cfg = -1;
     bool batched = true;           // one launch per level and stage + CUDA graphs (else per block, eager)
     bool matter = false;           // resident matter sources (granite_ccz4_enable_matter)
     double* d_matter = nullptr;    // rho[N] | Si[N][3] | Sij[N][6] | S[N], N = matter_cells (all blocks)
@@ -160,7 +180,7 @@ struct Ctx {
     unsigned int* d_errflag = nullptr;   // set by a TMA stage kernel whose bounded wait gave up
     int test_withhold = 0;               // armed test switch (StageArgs::test_withhold) of the next rk3_step
     unsigned long long* d_cmp = nullptr; // granite_ccz4_compare_states results (46 words)
-    CUtensorMap* d_tmaps = nullptr;      // TMA variant: 3 maps per resident block (slot 0, 1, 2)
+    CUtensorMap* d_tmaps = nullptr;      // TMA variant: per box shape, 3 maps per resident block (slots 0-2)
     CUtensorMap* s_tmap = nullptr;       // TMA variant: map of the stateless single-block input
 
     // stateless scratch (grow-only)
@@ -266,9 +286,10 @@ DevBlock make_devblock(const granite_block_desc& b, double sigma) {
 // Tiles of one block. adaptive (global-load stage kernels only): pick the tile
 // width w in {32, 16, 8} (128 / w rows) that leaves the fewest idle threads on
 // this block's x-y face, preferring the wider tile on ties (longer coalesced rows).
-void tiles_of(int block, const granite_block_desc& b, std::vector<Tile>& out, int variant, bool adaptive = false) {
+void tiles_of(int block, const granite_block_desc& b, std::vector<Tile>& out, int variant, bool adaptive = false,
+              int cfg = 0) {
     int TX, TY, TZ;
-    stage_tile_dims(variant, &TX, &TY, &TZ);
+    stage_tile_dims(variant, cfg, &TX, &TY, &TZ);
     int w = 0;
     if (adaptive) {
         long long best = -1;
@@ -290,6 +311,18 @@ void tiles_of(int block, const granite_block_desc& b, std::vector<Tile>& out, in
             for (int i = 0; i < b.ncells[0]; i += TX) out.push_back(Tile{block, i, j, k, w});
 }
 
+// Block-size class of a block for the per-class stage configuration: the class
+// edge (GRANITE_STAGE_CLASS_EDGES) nearest, on a log scale, to the cube root of
+// its interior volume.
+int stage_class_of(const granite_block_desc& b) {
+    static const int edges[GRANITE_STAGE_CLASSES] = {GRANITE_STAGE_CLASS_EDGES};
+    const double e = std::cbrt((double)b.ncells[0] * b.ncells[1] * b.ncells[2]);
+    int best = 0;
+    for (int q = 1; q < GRANITE_STAGE_CLASSES; ++q)
+        if (std::fabs(std::log(e / edges[q])) < std::fabs(std::log(e / edges[best]))) best = q;
+    return best;
+}
+
 long long ghost_count(const granite_block_desc& b) {
     return cells_of(b) - (long long)b.ncells[0] * b.ncells[1] * b.ncells[2];
 }
@@ -297,6 +330,12 @@ long long ghost_count(const granite_block_desc& b) {
 void ghost_chunks_of(int block, const granite_block_desc& b, std::vector<GhostItem>& out) {
     const long long n = ghost_count(b);
     for (long long r = 0; r < n; r += 256) out.push_back(GhostItem{block, (int)r});
+}
+
+// TMA configuration of a block for precision index pr (0 FP64, 1 MIXED).
+int block_cfg(const Ctx* c, int pr, const granite_block_desc& b) {
+    if (c->forced_cfg >= 0) return c->forced_cfg;
+    return c->class_cfg[pr][stage_class_of(b)];
 }
 
 StageArgs base_args(const Ctx* c) {
@@ -356,9 +395,9 @@ int stage_single(Ctx* c, const granite_block_desc* b, double* u_dev, int* ntiles
     if (r) return r;
     DevBlock d = make_devblock(*b, c->p.ko_sigma);
     d.buf[0] = u_dev ? u_dev : c->s_u;
-    if (variant == VARIANT_TMA) {
+    if (variant == VARIANT_TMA) {  // configuration 0 (the one with the store epilogue)
         CUtensorMap m;
-        if (encode_block_tmap(&m, d.buf[0], d))
+        if (encode_block_tmap(&m, d.buf[0], d, TMA_CFGS[0].tz))
             CK(cudaMemcpyAsync(c->s_tmap, &m, sizeof(m), cudaMemcpyHostToDevice, s), "upload tensor map");
         else
             variant = VARIANT_GLOBAL;
@@ -467,6 +506,54 @@ int granite_ccz4_set_kernel_variant(void* h, int variant) {
     return GRANITE_OK;
 }
 
+int granite_ccz4_set_stage_config(void* h, int precision, int cls, int cfg) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (c->committed) return fail(c, GRANITE_ERR_INVALID, "set stage configurations before commit");
+    if (precision != GRANITE_PRECISION_FP64 && precision != GRANITE_PRECISION_MIXED)
+        return fail(c, GRANITE_ERR_INVALID, "precision must be GRANITE_PRECISION_FP64 or _MIXED");
+    if (cls < -1 || cls >= GRANITE_STAGE_CLASSES) return fail(c, GRANITE_ERR_INVALID, "unknown block-size class");
+    if (cfg < -1 || cfg >= NUM_TMA_CFGS) return fail(c, GRANITE_ERR_INVALID, "unknown stage configuration");
+    const int pr = precision == GRANITE_PRECISION_MIXED ? 1 : 0;
+    for (int q = 0; q < GRANITE_STAGE_CLASSES; ++q)
+        if (cls < 0 || q == cls) c->class_cfg[pr][q] = cfg < 0 ? DEFAULT_CLASS_CFG[pr][q] : cfg;
+    return GRANITE_OK;
+}
+
+int granite_ccz4_get_stage_config(const void* h, int precision, int cls, int* cfg) {
+    const Ctx* c = static_cast<const Ctx*>(h);
+    if (!c || !cfg || cls < 0 || cls >= GRANITE_STAGE_CLASSES) return GRANITE_ERR_INVALID;
+    if (precision != GRANITE_PRECISION_FP64 && precision != GRANITE_PRECISION_MIXED) return GRANITE_ERR_INVALID;
+    *cfg = c->forced_cfg >= 0 ? c->forced_cfg : c->class_cfg[precision == GRANITE_PRECISION_MIXED ? 1 : 0][cls];
+    return GRANITE_OK;
+}
+
+int granite_ccz4_force_stage_config(void* h, int cfg) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    if (c->committed) return fail(c, GRANITE_ERR_INVALID, "set stage configurations before commit");
+    if (cfg < -1 || cfg >= NUM_TMA_CFGS) return fail(c, GRANITE_ERR_INVALID, "unknown stage configuration");
+    c->forced_cfg = cfg;
+    return GRANITE_OK;
+}
+
+int granite_ccz4_stage_config_info(int cfg, int* tile_z, int* ring_slots, int* shared_input, int* shared_hessian) {
+    if (cfg < 0 || cfg >= NUM_TMA_CFGS) return GRANITE_ERR_INVALID;
+    if (tile_z) *tile_z = TMA_CFGS[cfg].tz;
+    if (ring_slots) *ring_slots = TMA_CFGS[cfg].nbuf;
+    if (shared_input) *shared_input = TMA_CFGS[cfg].tin;
+    if (shared_hessian) *shared_hessian = TMA_CFGS[cfg].hs;
+    return GRANITE_OK;
+}
+
+int granite_ccz4_block_stage_class(const granite_block_desc* b, int* cls) {
+    if (!b || !cls) return GRANITE_ERR_INVALID;
+    for (int d = 0; d < 3; ++d)
+        if (b->ncells[d] <= 0) return GRANITE_ERR_INVALID;
+    *cls = stage_class_of(*b);
+    return GRANITE_OK;
+}
+
 int granite_ccz4_set_fp64_chi_threshold(void* h, double chi) {
     Ctx* c = static_cast<Ctx*>(h);
     if (!c) return GRANITE_ERR_INVALID;
@@ -535,6 +622,7 @@ int granite_ccz4_create(const granite_ccz4_params* p, void** out) {
     if (cudaGetDeviceProperties(&prop, p->device) != cudaSuccess) return GRANITE_ERR_NO_DEVICE;
     if (prop.major != 10) return GRANITE_ERR_NO_DEVICE;  // kernels are built for sm_100a only
     Ctx* c = new Ctx();
+    std::memcpy(c->class_cfg, DEFAULT_CLASS_CFG, sizeof(c->class_cfg));
     c->p = *p;
     c->device = p->device;
     cudaError_t e = cudaSetDevice(c->device);
@@ -669,7 +757,7 @@ int granite_ccz4_compute_rhs_device(void* h, const granite_block_desc* b, const 
     a.Sij = Sij;
     a.S = S;
     a.tmaps = c->s_tmap;  // block 0, slot 0
-    CK(launch_stage(variant, precision, EPI_STORE, c->s_desc, c->s_tiles, nt, a, s), "launch RHS");
+    CK(launch_stage(variant, 0, precision, EPI_STORE, c->s_desc, c->s_tiles, nt, a, s), "launch RHS");
     c->launches += 1;
     return GRANITE_OK;
 }
@@ -924,14 +1012,18 @@ static int build_lists(Ctx* c) {
     CK(upload_vec(c->hblocks, &c->d_blocks, c->stream), "upload block table");
     int maxlev = 0;
     for (const auto& d : c->descs) maxlev = std::max(maxlev, d.level);
-    // TMA variant: one tensor map per (block, slot); a block that cannot be
-    // mapped sends its whole level to the global-load kernel
-    std::vector<char> mapped(c->descs.size(), 0);
+    // TMA variant: one tensor map per (box shape, block, slot); a block that
+    // cannot be mapped sends its whole level to the global-load kernel
+    const size_t nb = c->descs.size();
+    std::vector<char> mapped(nb, 0);
     if (c->variant == VARIANT_TMA) {
-        std::vector<CUtensorMap> maps(3 * c->descs.size());
-        for (size_t i = 0; i < c->descs.size(); ++i) {
+        std::vector<CUtensorMap> maps(TMA_SHAPES * 3 * nb);
+        for (size_t i = 0; i < nb; ++i) {
             bool ok = true;
-            for (int sl = 0; sl < 3; ++sl) ok = ok && encode_block_tmap(&maps[3 * i + sl], c->hblocks[i].buf[sl], c->hblocks[i]);
+            for (int sh = 0; sh < TMA_SHAPES; ++sh)
+                for (int sl = 0; sl < 3; ++sl)
+                    ok = ok && encode_block_tmap(&maps[(sh * nb + i) * 3 + sl], c->hblocks[i].buf[sl], c->hblocks[i],
+                                                 TMA_SHAPE_TZ[sh]);
             mapped[i] = ok;
         }
         CK(upload_vec(maps, &c->d_tmaps, c->stream), "upload tensor maps");
@@ -945,14 +1037,29 @@ static int build_lists(Ctx* c) {
         ll.variant = c->variant;
         for (size_t i = 0; i < c->descs.size(); ++i)
             if (c->descs[i].level == L && c->variant == VARIANT_TMA && !mapped[i]) ll.variant = VARIANT_GLOBAL;
-        for (size_t i = 0; i < c->descs.size(); ++i) {
-            if (c->descs[i].level != L) continue;
-            ll.blocks.push_back((int)i);
-            const int t0 = (int)tiles.size(), g0 = (int)ghosts.size();
-            tiles_of((int)i, c->descs[i], tiles, ll.variant, adaptive_tiles(ll.variant));
-            tiles_of((int)i, c->descs[i], mtiles, VARIANT_GLOBAL);
-            ghost_chunks_of((int)i, c->descs[i], ghosts);
-            ll.tile_range.push_back({t0, (int)tiles.size() - t0});
+        for (size_t i = 0; i < c->descs.size(); ++i)
+            if (c->descs[i].level == L) ll.blocks.push_back((int)i);
+        // per precision: stage tiles grouped by configuration (one launch per
+        // group), each block's tiles contiguous
+        for (int pr = 0; pr < 2; ++pr) {
+            for (int i : ll.blocks) ll.block_cfg[pr].push_back(ll.variant == VARIANT_TMA ? block_cfg(c, pr, c->descs[i]) : 0);
+            ll.tile_range[pr].assign(ll.blocks.size(), {0, 0});
+            for (int cfg = 0; cfg < NUM_TMA_CFGS; ++cfg) {
+                const int g0 = (int)tiles.size();
+                for (size_t q = 0; q < ll.blocks.size(); ++q) {
+                    if (ll.block_cfg[pr][q] != cfg) continue;
+                    const int t0 = (int)tiles.size();
+                    tiles_of(ll.blocks[q], c->descs[ll.blocks[q]], tiles, ll.variant, adaptive_tiles(ll.variant), cfg);
+                    ll.tile_range[pr][q] = {t0, (int)tiles.size() - t0};
+                }
+                if ((int)tiles.size() > g0) ll.groups[pr].push_back({cfg, g0, (int)tiles.size() - g0});
+            }
+        }
+        for (size_t q = 0; q < ll.blocks.size(); ++q) {
+            const int i = ll.blocks[q];
+            const int g0 = (int)ghosts.size();
+            tiles_of(i, c->descs[i], mtiles, VARIANT_GLOBAL);
+            ghost_chunks_of(i, c->descs[i], ghosts);
             ll.ghost_range.push_back({g0, (int)ghosts.size() - g0});
             ll.interior_points += (long long)c->descs[i].ncells[0] * c->descs[i].ncells[1] * c->descs[i].ncells[2];
         }
@@ -1203,36 +1310,49 @@ int granite_ccz4_download_block(void* h, int i, double* host) {
 // then the FP32 kernel over the unflagged tiles and the FP64 kernel over the
 // flagged ones. The two passes write disjoint tiles, so the in-place last
 // stage is safe and no tile is computed twice.
-static cudaError_t stage_range(Ctx* c, LevelLists& L, int precision, const StageArgs& a, int first, int count,
-                               long long* n) {
+static cudaError_t stage_range(Ctx* c, LevelLists& L, int cfg, int precision, const StageArgs& a0, int first,
+                               int count, long long* n) {
     const Tile* tiles = L.d_tiles + first;
+    StageArgs a = a0;
+    if (L.variant == VARIANT_TMA)  // the tensor maps of this configuration's box shape
+        a.tmaps = c->d_tmaps + (size_t)tma_shape_of(cfg) * 3 * c->descs.size();
     // (the TMA kernel keeps a CTA's selected tiles in shared memory: bounded count)
     const bool split = precision == GRANITE_PRECISION_MIXED && c->fp64_chi > 0.0 &&
-        (L.variant != VARIANT_TMA || (long long)count <= (long long)tma_grid() * TMA_SEL_CAP);
+        (L.variant != VARIANT_TMA || (long long)count <= (long long)tma_grid(cfg) * TMA_SEL_CAP);
     if (!split) {
         ++*n;
-        return launch_stage(L.variant, precision, EPI_RK, c->d_blocks, tiles, count, a, c->stream);
+        return launch_stage(L.variant, cfg, precision, EPI_RK, c->d_blocks, tiles, count, a, c->stream);
     }
     unsigned char* flags = L.d_flags + first;
-    cudaError_t e = launch_classify(L.variant, c->d_blocks, tiles, 0, count, a.in_sel, c->fp64_chi, flags, c->stream);
+    cudaError_t e = launch_classify(L.variant, cfg, c->d_blocks, tiles, 0, count, a.in_sel, c->fp64_chi, flags,
+                                    c->stream);
     if (e != cudaSuccess) return e;
     StageArgs b = a;
     b.tile_prec = flags;
     b.want_prec = 0;
-    if ((e = launch_stage(L.variant, PM_MIXED, EPI_RK, c->d_blocks, tiles, count, b, c->stream))) return e;
+    if ((e = launch_stage(L.variant, cfg, PM_MIXED, EPI_RK, c->d_blocks, tiles, count, b, c->stream))) return e;
     b.want_prec = 1;
     *n += 3;
-    return launch_stage(L.variant, PM_FP64F, EPI_RK, c->d_blocks, tiles, count, b, c->stream);
+    return launch_stage(L.variant, cfg, PM_FP64F, EPI_RK, c->d_blocks, tiles, count, b, c->stream);
 }
 
 // The fused stage kernel over one level: the whole work-list at once, or
 // (unbatched) block by block.
 static cudaError_t level_stage(Ctx* c, LevelLists& L, int precision, const StageArgs& a, long long* n) {
-    if (c->batched)
-        return timed(c, GRANITE_KERNEL_STAGE, [&] { return stage_range(c, L, precision, a, 0, L.ntiles, n); });
-    for (const auto& r : L.tile_range) {
-        cudaError_t e = timed(c, GRANITE_KERNEL_STAGE,
-                              [&] { return stage_range(c, L, precision, a, r.first, r.second, n); });
+    const int pr = precision == GRANITE_PRECISION_MIXED ? 1 : 0;
+    if (c->batched) {
+        for (const auto& g : L.groups[pr]) {
+            cudaError_t e = timed(c, GRANITE_KERNEL_STAGE,
+                                  [&] { return stage_range(c, L, g.cfg, precision, a, g.first, g.count, n); });
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+    for (size_t q = 0; q < L.tile_range[pr].size(); ++q) {
+        const auto& r = L.tile_range[pr][q];
+        cudaError_t e = timed(c, GRANITE_KERNEL_STAGE, [&] {
+            return stage_range(c, L, L.block_cfg[pr][q], precision, a, r.first, r.second, n);
+        });
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;

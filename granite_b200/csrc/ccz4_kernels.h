@@ -21,21 +21,41 @@ enum {
     NUM_VARIANTS = 5
 };
 
-// Tile shape of a stage-kernel variant (points per CTA along x, y, z).
-int stage_tile_dims(int variant, int* tx, int* ty, int* tz);
+// Tile shape of a stage-kernel variant (points per CTA along x, y, z); cfg
+// selects the TMA configuration.
+int stage_tile_dims(int variant, int cfg, int* tx, int* ty, int* tz);
 
-// TMA variant: the box (cells incl. the 4-cell halo) one tensor-map load brings
-// in per field, and the tensor map of one 22-field block buffer
-// (dims x, y, z, field; cells incl. ghosts). Returns false when the buffer
-// cannot be described (odd x extent, misaligned base, box larger than the
-// block); such blocks use the global-load kernel.
-constexpr int TMA_BOX[3] = {16 + 8, 4 + 8, 4 + 8};
+// Configurations of the TMA variant (the autotuner's candidates): tiles of
+// 16 x 4 x tz points (tz * 64 threads per CTA; tz = 2 asks for two resident
+// CTAs per SM), a ring of nbuf field boxes; tin: the stage input's centre values
+// are kept in shared memory for the RK epilogue and the epilogue's u^n and the
+// next tile's pointwise cells are prefetched into L2; hs: the Hessian-field
+// loop's 36 values live in shared memory instead of local memory.
+// Configuration 0 is the untuned default and the only one with the
+// store (drop-in RHS) epilogue.
+struct TmaCfg {
+    int tz, nbuf, tin, hs;
+};
+constexpr int NUM_TMA_CFGS = 5;
+constexpr TmaCfg TMA_CFGS[NUM_TMA_CFGS] = {{4, 3, 0, 0}, {4, 3, 1, 1}, {2, 3, 1, 1}, {2, 2, 1, 1}, {2, 3, 1, 0}};
+// The box (cells incl. the 4-cell halo) one tensor-map load brings in per
+// field: 24 x 12 x (tz + 8). Tensor maps exist per box shape: shape 0 (tz = 4)
+// and shape 1 (tz = 2).
+constexpr int TMA_BOX_X = 16 + 8, TMA_BOX_Y = 4 + 8;
+constexpr int TMA_SHAPES = 2;
+constexpr int TMA_SHAPE_TZ[TMA_SHAPES] = {4, 2};
+constexpr int tma_shape_of(int cfg) { return TMA_CFGS[cfg].tz == 4 ? 0 : 1; }
 // Per-tile precision launches of the TMA kernel keep each CTA's selected tiles
 // in shared memory: at most TMA_SEL_CAP per CTA, i.e. ntiles <= grid x TMA_SEL_CAP.
-constexpr int TMA_SEL_CAP = 2048;
-// The persistent grid of the TMA kernel on the current device (0 before configure_stage_kernels).
-int tma_grid();
-bool encode_block_tmap(void* map128, const double* base, const DevBlock& d);
+constexpr int TMA_SEL_CAP = 1024;
+// The persistent grid of a TMA configuration's MIXED RK kernel on the current
+// device (0 before configure_stage_kernels).
+int tma_grid(int cfg);
+// Tensor map of one 22-field block buffer (dims x, y, z, field; cells incl.
+// ghosts) with the box of tile depth tz. Returns false when the buffer cannot
+// be described (odd x extent, misaligned base, box larger than the block);
+// such blocks use the global-load kernel.
+bool encode_block_tmap(void* map128, const double* base, const DevBlock& d, int tz);
 
 // Per-device kernel attributes (shared-memory opt-in); call with the device current.
 cudaError_t configure_stage_kernels();
@@ -47,14 +67,16 @@ cudaError_t configure_stage_kernels();
 enum { PM_FP64 = 0, PM_MIXED = 1, PM_FP64F = 2 };
 
 // Fused RHS (+KO) over a tile work-list in precision mode `precision` (PM_*);
-// with args.tile_prec set, only the tiles flagged args.want_prec.
-cudaError_t launch_stage(int variant, int precision, int epi, const DevBlock* blocks,
+// with args.tile_prec set, only the tiles flagged args.want_prec. cfg: the TMA
+// configuration (ignored by the other variants); args.tmaps must hold the
+// tensor maps of that configuration's box shape.
+cudaError_t launch_stage(int variant, int cfg, int precision, int epi, const DevBlock* blocks,
                          const Tile* tiles, int ntiles, const StageArgs& args, cudaStream_t stream);
 
 // Per-tile precision flags of tiles [first, first + ntiles): flag[ti] = 1 when a
 // point of the tile has chi < chi_fp64 in slot `sel` (FP64 algebra), else 0.
-cudaError_t launch_classify(int variant, const DevBlock* blocks, const Tile* tiles, int first, int ntiles, int sel,
-                            double chi_fp64, unsigned char* flag, cudaStream_t stream);
+cudaError_t launch_classify(int variant, int cfg, const DevBlock* blocks, const Tile* tiles, int first, int ntiles,
+                            int sel, double chi_fp64, unsigned char* flag, cudaStream_t stream);
 
 // KO dissipation only: rhs += KO(u) at interior points of one block.
 cudaError_t launch_dissipation(const DevBlock* block, int in_sel, double* rhs, int ntiles,

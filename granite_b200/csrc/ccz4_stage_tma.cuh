@@ -1,0 +1,359 @@
+// ccz4_stage_tma.cuh -- the TMA-ring stage kernel, templated on its tuning
+// configuration. Each ccz4_tma_cfg<k>.cu instantiates one entry of TMA_CFGS
+// (ccz4_kernels.h), so the configurations compile in parallel and the
+// autotuner can pick one per block-size class at run time.
+//
+// A persistent CTA walks its tiles (blockIdx.x, + gridDim.x, ...) and consumes
+// a stream of items q = (tile round q / NV, field FIELD_ORDER[q % NV]). Item q
+// is one (16 + 8) x (4 + 8) x (TZ + 8)-cell box (the 16 x 4 x TZ tile and its
+// 4-cell halo) of one field, brought into ring slot q % NBUF by a single
+// cp.async.bulk.tensor load that completes on that slot's mbarrier. Thread 0
+// issues item q + NBUF - 1 when the CTA starts on item q, so loads run NBUF - 1
+// fields ahead and across tile boundaries. Rows of 24 doubles put the 16-wide x
+// rows of a warp in distinct shared-memory banks for every stencil offset.
+//
+// Options of a configuration:
+//   TIN  every field's centre value is copied from the ring into a per-thread
+//        column of shared memory as it streams through, and the RK epilogue
+//        reads the stage input there instead of from global memory; the
+//        epilogue's u^n cells and the next tile's pointwise cells are
+//        prefetched into L2 at the start of each tile;
+//   HS   the 36 values of the Hessian-field loop live in a per-thread column of
+//        shared memory instead of local memory.
+#pragma once
+
+#include <cstdint>
+#include <type_traits>
+
+#include "ccz4_point.cuh"
+
+namespace granite_b200 {
+
+namespace {
+
+template <int TZ_, int NBUF_, bool TIN_, bool HS_>
+struct TmaCfgT {
+    static constexpr int TZ = TZ_, NBUF = NBUF_;
+    static constexpr bool TIN = TIN_, HS = HS_;
+    static constexpr int TX = 16, TY = 4, NT = TX * TY * TZ;
+    static constexpr int MINB = TZ == 2 ? 2 : 1;  // resident CTAs per SM asked of the register allocator
+    static constexpr int BX = TX + 8, BY = TY + 8, BZ = TZ + 8;
+    static constexpr int BOX = BX * BY * BZ;
+    static constexpr unsigned BYTES = BOX * sizeof(double);  // complete_tx count of one item
+    static_assert(BYTES % 128 == 0, "slots stay 128-byte aligned");
+    static_assert(BX == TMA_BOX_X && BY == TMA_BOX_Y, "box = tile + halo");
+    // dynamic shared memory: ring | mbarriers | stage-input column | Hessian slots
+    static constexpr size_t OFF_BAR = (size_t)NBUF * BYTES;
+    static constexpr size_t OFF_TIN = (OFF_BAR + NBUF * sizeof(unsigned long long) + 127) / 128 * 128;
+    static constexpr size_t OFF_HS = OFF_TIN + (TIN ? (size_t)NV * NT * sizeof(double) : 0);
+    template <typename P>
+    static constexpr size_t smem() {
+        return OFF_HS + (HS ? (size_t)36 * NT * sizeof(P) : 0) + 128;  // + alignment of the base
+    }
+};
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// One box of a 4-D tensor map (x, y, z, field) into shared memory.
+__device__ __forceinline__ void tma_load_box(unsigned dst, const void* map, int x, int y, int z, int f,
+                                             unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(dst),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(f), "r"(bar)
+        : "memory");
+}
+// Bring the line holding p into L2 with the evict-last priority (a hint: no
+// register, no completion to wait for).
+__device__ __forceinline__ void prefetch_l2(const double* p) {
+    asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(p));
+}
+
+// Wait limit of one ring slot: 2 s of wall time, then the kernel records the
+// failure in StageArgs::errflag and stops waiting (results are then garbage
+// and the host reports the error).
+constexpr unsigned long long TMA_WAIT_NS = 2000000000ull;
+
+// Per-tile precision launches: the CTA's selected tiles, in order, and their
+// count at [TMA_SEL_CAP] (shared memory at a fixed address, so the per-point
+// body keeps no register for them).
+__shared__ int g_sel_list[TMA_SEL_CAP + 1];
+
+template <class C, bool SEL>
+struct TmaSource {
+    static constexpr bool HS = C::HS;
+    static constexpr int NT = C::NT;
+    const DevBlock* blocks;
+    const Tile* tiles;
+    const unsigned char* maps;  // CUtensorMap array of this box shape, 128 bytes each
+    int ntiles, in_sel;
+    double* ring;      // NBUF slots of C::BOX doubles
+    unsigned bar0;     // shared address of the slot mbarriers (8 bytes apart)
+    double* tin;       // TIN: this thread's stage-input column (field v at tin[v * NT])
+    void* hs;          // HS: this thread's Hessian-loop column (slot q at hs[q * NT])
+    const DevBlock* B; // block of the current tile (stencil coefficients)
+    int lin;           // this thread's point within a slot
+    int next;          // next item to consume
+    bool failed;       // a wait of this thread gave up (at item fail_q); thread 0 then stops issuing
+    unsigned int* err;
+    int fail_q;
+    int withhold;      // test switch: 1 + the item CTA 0 leaves unissued (0: none)
+
+    template <typename P>
+    __device__ __forceinline__ P* hess_slots() const {
+        return static_cast<P*>(hs);
+    }
+    // Tile of the CTA's r-th round: blockIdx.x + r gridDim.x, or with per-tile
+    // precision (SEL) the r-th tile of that sequence whose flag the launch takes.
+    __device__ __forceinline__ int round_tile(int r) const {
+        if constexpr (SEL)
+            return r < g_sel_list[TMA_SEL_CAP] ? g_sel_list[r] : ntiles;
+        else
+            return blockIdx.x + r * gridDim.x;
+    }
+    // thread 0 only
+    __device__ __forceinline__ void issue(int q) const {
+        const int ti = round_tile(q / NV);
+        if (ti >= ntiles) return;
+        if (withhold != 0 && q == withhold - 1 && blockIdx.x == 0) return;  // test switch: never issued
+        const Tile t = tiles[ti];
+        const int s = q % C::NBUF;
+        const unsigned bar = bar0 + 8u * s;
+        mbar_expect_tx(bar, C::BYTES);
+        // box origin = tile origin - 4 cells = interior index (cells incl. ghosts start 4 lower)
+        tma_load_box(smem_addr(ring + (size_t)s * C::BOX), maps + (size_t)(3 * t.block + in_sel) * 128, t.i0,
+                     t.j0, t.k0, FIELD_ORDER[q % NV], bar);
+    }
+    __device__ __forceinline__ void wait(int q) {
+        if (failed) return;
+        const unsigned bar = bar0 + 8u * (q % C::NBUF), parity = (q / C::NBUF) & 1;
+        unsigned long long t0 = 0;
+        for (unsigned it = 1;; ++it) {
+            if (mbar_try_wait(bar, parity)) return;
+            if ((it & 255u) == 0) {
+                const unsigned long long now = global_ns();
+                if (t0 == 0) {
+                    t0 = now;
+                } else if (now - t0 > TMA_WAIT_NS) {
+                    failed = true;
+                    fail_q = q;
+                    if (err) atomicExch(err, 1u);
+                    return;
+                }
+            }
+        }
+    }
+    // Every thread of the CTA calls der() for every item in order (the call
+    // carries the CTA barrier that frees the slot the next load overwrites).
+    template <bool HESS, bool EXACT, typename P>
+    __device__ __forceinline__ FieldDer<P> der(int v, const double beta[3], P w) {
+        __syncthreads();
+        if (threadIdx.x == 0 && !failed) issue(next + C::NBUF - 1);
+        wait(next);
+        const double* box = ring + (size_t)(next % C::NBUF) * C::BOX + lin;
+        if constexpr (C::TIN) tin[v * NT] = box[0];
+        const SharedLoad L{box};
+        ++next;
+        const long long off[3] = {1, C::BX, C::BX * C::BY};
+        return field_der_l<P, HESS, true, SharedLoad, EXACT>(*B, L, off, beta, w);
+    }
+};
+
+}  // namespace
+
+// Persistent CTAs (grid <= SMs x resident CTAs), one 16 x 4 x TZ tile at a
+// time, every field streamed through the TMA ring. Threads of partial tiles
+// (past the block edge) compute on the zero-filled box and store nothing.
+template <int PM, int EPI, class C, bool SEL>
+__global__ void __launch_bounds__(C::NT, C::MINB)
+    ccz4_stage_tma_kernel(const DevBlock* __restrict__ blocks, const Tile* __restrict__ tiles, int ntiles,
+                          StageArgs A) {
+    using P = typename std::conditional<PM == PM_MIXED, float, double>::type;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) &
+                                                           ~uintptr_t(127));
+    double* ring = reinterpret_cast<double*>(base);
+    const unsigned bar0 = smem_addr(base + C::OFF_BAR);
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < C::NBUF; ++s) mbar_init(bar0 + 8u * s, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    // SEL: the CTA's tiles blockIdx.x + m gridDim.x whose flag equals want_prec,
+    // compacted in order into shared memory once (ballot scan over NT candidates
+    // at a time); the host keeps ntiles <= gridDim.x * TMA_SEL_CAP.
+    __shared__ int warp_cnt[C::NT / 32];
+    if constexpr (SEL) {
+        int nsel = 0;
+        const int ncand = ntiles > (int)blockIdx.x ? (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+        const int lane = tid & 31, warp = tid >> 5;
+        for (int m0 = 0; m0 < ncand; m0 += C::NT) {
+            const int m = m0 + tid;
+            const int ti = blockIdx.x + m * gridDim.x;
+            const bool take = m < ncand && A.tile_prec[ti] == A.want_prec;
+            const unsigned bal = __ballot_sync(0xffffffffu, take);
+            if (lane == 0) warp_cnt[warp] = __popc(bal);
+            __syncthreads();
+            int off = 0, tot = 0;
+#pragma unroll
+            for (int w = 0; w < C::NT / 32; ++w) {
+                off += w < warp ? warp_cnt[w] : 0;
+                tot += warp_cnt[w];
+            }
+            const int pos = nsel + off + __popc(bal & ((1u << lane) - 1u));
+            if (take && pos < TMA_SEL_CAP) g_sel_list[pos] = ti;
+            nsel += tot;
+            __syncthreads();
+        }
+        if (tid == 0) g_sel_list[TMA_SEL_CAP] = nsel < TMA_SEL_CAP ? nsel : TMA_SEL_CAP;  // (host keeps it below)
+    }
+    __syncthreads();
+    const int lx = tid % C::TX, ly = (tid / C::TX) % C::TY, lz = tid / (C::TX * C::TY);
+    double* tin = C::TIN ? reinterpret_cast<double*>(base + C::OFF_TIN) + tid : nullptr;
+    void* hs = C::HS ? static_cast<void*>(reinterpret_cast<P*>(base + C::OFF_HS) + tid) : nullptr;
+    TmaSource<C, SEL> S{blocks, tiles, static_cast<const unsigned char*>(A.tmaps), ntiles, A.in_sel, ring, bar0,
+                        tin, hs, nullptr, (lx + 4) + C::BX * ((ly + 4) + C::BY * (lz + 4)), 0, false,
+                        A.errflag, 0, A.test_withhold};
+    if (tid == 0)
+        for (int q = 0; q < C::NBUF - 1; ++q) S.issue(q);
+    for (int r = 0;; ++r) {
+        const int ti = S.round_tile(r);
+        if (ti >= ntiles) break;
+        const Tile t = tiles[ti];
+        const DevBlock& B = blocks[t.block];
+        S.B = &B;
+        const int i = t.i0 + lx, j = t.j0 + ly, k = t.k0 + lz;
+        const bool valid = i < B.n[0] && j < B.n[1] && k < B.n[2];
+        // pointwise loads of threads outside the block use a valid cell; their results are dropped
+        const int ic = min(i, B.n[0] - 1), jc = min(j, B.n[1] - 1), kc = min(k, B.n[2] - 1);
+        const long long c = cell_index(B, ic + NG, jc + NG, kc + NG);
+        const double* __restrict__ uin = B.buf[A.in_sel];
+        if constexpr (C::TIN) {
+            // L2 prefetches: this tile's u^n (read by the epilogue; stage 1 takes
+            // it from the ring) and the next tile's pointwise cells
+            if (EPI == EPI_RK && A.n_sel != A.in_sel) {
+                const double* un = B.buf[A.n_sel] + c;
+#pragma unroll
+                for (int v = 0; v < NV; ++v) prefetch_l2(un + (long long)v * B.stride);
+            }
+            const int tn = S.round_tile(r + 1);
+            if (tn < ntiles) {
+                const Tile t2 = tiles[tn];
+                const DevBlock& B2 = blocks[t2.block];
+                const long long c2 = cell_index(B2, min(t2.i0 + lx, B2.n[0] - 1) + NG, min(t2.j0 + ly, B2.n[1] - 1) + NG,
+                                                min(t2.k0 + lz, B2.n[2] - 1) + NG);
+                const double* u2 = B2.buf[A.in_sel] + c2;
+#pragma unroll
+                for (int v = 0; v < NV; ++v) prefetch_l2(u2 + (long long)v * B2.stride);
+            }
+        }
+        double L[NV];
+        point_pm<PM>(B, uin, c, A, S, L);
+        if (valid) stage_epilogue<EPI>(B, A, c, L, tin, C::NT);
+    }
+    // Every issued item was consumed (issue() skips items past this CTA's last
+    // tile), so no copy into the ring is in flight when the CTA exits. If
+    // thread 0 gave up waiting at item f (which already had its full wait), it
+    // had issued items up to f + NBUF - 1 and nothing after: each of
+    // f + 1 .. f + NBUF - 1 that was issued gets its own bounded wait, whatever
+    // the others do, so no copy into this CTA's shared memory outlives it.
+    if (S.failed && tid == 0) {
+        const int f = S.fail_q;
+        for (int q = f + 1; q < f + C::NBUF; ++q) {
+            if (S.round_tile(q / NV) >= ntiles) continue;
+            S.failed = false;
+            S.wait(q);
+        }
+    }
+}
+
+// Launchers of one configuration: grids[pm][epi][sel] is the persistent grid
+// (SMs x resident CTAs) measured by tma_configure; 0 = not instantiated.
+template <class C>
+struct TmaConfigOps {
+    template <int PM, int EPI, bool SEL>
+    static cudaError_t configure_one(int nsm, int grids[3][2][2]) {
+        using P = typename std::conditional<PM == PM_MIXED, float, double>::type;
+        auto k = ccz4_stage_tma_kernel<PM, EPI, C, SEL>;
+        constexpr size_t bytes = C::template smem<P>();
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, C::NT, bytes))) return e;
+        grids[PM][EPI][SEL ? 1 : 0] = nsm * (per_sm > 0 ? per_sm : 1);
+        return cudaSuccess;
+    }
+    template <int PM, int EPI, bool SEL>
+    static cudaError_t launch_one(const DevBlock* blocks, const Tile* tiles, int ntiles, const StageArgs& args,
+                                  cudaStream_t stream, int grid) {
+        using P = typename std::conditional<PM == PM_MIXED, float, double>::type;
+        ccz4_stage_tma_kernel<PM, EPI, C, SEL>
+            <<<grid, C::NT, C::template smem<P>(), stream>>>(blocks, tiles, ntiles, args);
+        return cudaGetLastError();
+    }
+    // The RK-epilogue kernels every configuration has (FP64; MIXED with and
+    // without per-tile selection; the FP64 pass of the per-tile precision),
+    // plus the store epilogue where STORE is set.
+    template <bool STORE>
+    static cudaError_t configure(int nsm, int grids[3][2][2]) {
+        cudaError_t e;
+        if ((e = configure_one<PM_FP64, EPI_RK, false>(nsm, grids))) return e;
+        if ((e = configure_one<PM_MIXED, EPI_RK, false>(nsm, grids))) return e;
+        if ((e = configure_one<PM_MIXED, EPI_RK, true>(nsm, grids))) return e;
+        if ((e = configure_one<PM_FP64F, EPI_RK, true>(nsm, grids))) return e;
+        if constexpr (STORE) {
+            if ((e = configure_one<PM_FP64, EPI_STORE, false>(nsm, grids))) return e;
+            if ((e = configure_one<PM_MIXED, EPI_STORE, false>(nsm, grids))) return e;
+        }
+        return cudaSuccess;
+    }
+    template <bool STORE>
+    static cudaError_t launch(int pm, int epi, bool sel, const DevBlock* blocks, const Tile* tiles, int ntiles,
+                              const StageArgs& args, cudaStream_t stream, int grid) {
+        if (epi == EPI_RK) {
+            if (pm == PM_FP64 && !sel) return launch_one<PM_FP64, EPI_RK, false>(blocks, tiles, ntiles, args, stream, grid);
+            if (pm == PM_MIXED && !sel) return launch_one<PM_MIXED, EPI_RK, false>(blocks, tiles, ntiles, args, stream, grid);
+            if (pm == PM_MIXED && sel) return launch_one<PM_MIXED, EPI_RK, true>(blocks, tiles, ntiles, args, stream, grid);
+            if (pm == PM_FP64F && sel) return launch_one<PM_FP64F, EPI_RK, true>(blocks, tiles, ntiles, args, stream, grid);
+        } else if constexpr (STORE) {
+            if (pm == PM_FP64 && !sel) return launch_one<PM_FP64, EPI_STORE, false>(blocks, tiles, ntiles, args, stream, grid);
+            if (pm == PM_MIXED && !sel) return launch_one<PM_MIXED, EPI_STORE, false>(blocks, tiles, ntiles, args, stream, grid);
+        }
+        return cudaErrorInvalidValue;
+    }
+};
+
+}  // namespace granite_b200
+
+// One translation unit per configuration k of TMA_CFGS defines its entry points.
+#define GRANITE_TMA_CFG_UNIT(K, STORE)                                                                               \
+    namespace granite_b200 {                                                                                         \
+    using TmaCfg##K = TmaCfgT<TMA_CFGS[K].tz, TMA_CFGS[K].nbuf, TMA_CFGS[K].tin != 0, TMA_CFGS[K].hs != 0>;           \
+    cudaError_t configure_tma_cfg##K(int nsm, int grids[3][2][2]) {                                                  \
+        return TmaConfigOps<TmaCfg##K>::configure<STORE>(nsm, grids);                                                \
+    }                                                                                                                \
+    cudaError_t launch_tma_cfg##K(int pm, int epi, bool sel, const DevBlock* blocks, const Tile* tiles, int ntiles,  \
+                                  const StageArgs& args, cudaStream_t stream, int grid) {                            \
+        return TmaConfigOps<TmaCfg##K>::launch<STORE>(pm, epi, sel, blocks, tiles, ntiles, args, stream, grid);      \
+    }                                                                                                                \
+    }

@@ -385,6 +385,32 @@ GRANITE_API int granite_ccz4_profile_get(void* ctx, int kernel_class, double* to
 GRANITE_API int granite_ccz4_set_kernel_variant(void* ctx, int variant);
 GRANITE_API int granite_ccz4_get_kernel_variant(const void* ctx, int* variant);
 
+/* Per-class configurations of GRANITE_VARIANT_TMA (no counterpart in the
+ * reference, whose computeRHS runs one OpenMP loop per block, ccz4.cpp:267-270).
+ * The TMA stage kernel exists in GRANITE_STAGE_CONFIGS configurations (see
+ * granite_ccz4_stage_config_info): tiles of 16 x 4 x tile_z points, ring_slots
+ * field boxes in flight, the stage input's centre values kept in shared memory
+ * for the RK epilogue (shared_input), the Hessian-field loop's values in shared
+ * memory (shared_hessian). Every block belongs to the block-size class whose
+ * edge (GRANITE_STAGE_CLASS_EDGES) is nearest on a log scale to the cube root of
+ * its interior volume; each (precision, class) has a configuration, the
+ * autotuner's B200 winners by default (granite_b200/tuner.py re-tunes and
+ * writes a table a caller can apply). A level's blocks of different
+ * configurations run as one launch per configuration. Set before commit.
+ * All configurations compute identical FP64 results. */
+#define GRANITE_STAGE_CONFIGS 5
+#define GRANITE_STAGE_CLASSES 6
+#define GRANITE_STAGE_CLASS_EDGES 16, 24, 32, 48, 64, 96
+/* cls: class index (0 .. GRANITE_STAGE_CLASSES - 1) or -1 for every class;
+ * cfg: configuration or -1 for the built-in default. */
+GRANITE_API int granite_ccz4_set_stage_config(void* ctx, int precision, int cls, int cfg);
+GRANITE_API int granite_ccz4_get_stage_config(const void* ctx, int precision, int cls, int* cfg);
+/* One configuration for every block and precision (-1: back to the per-class table). */
+GRANITE_API int granite_ccz4_force_stage_config(void* ctx, int cfg);
+GRANITE_API int granite_ccz4_stage_config_info(int cfg, int* tile_z, int* ring_slots, int* shared_input,
+                                               int* shared_hessian);
+GRANITE_API int granite_ccz4_block_stage_class(const granite_block_desc* b, int* cls);
+
 /* Test switch of the wait limit above (no counterpart in the reference, which
  * has no device waits; its failure detection is the NaN scan of
  * main.cpp:525-568): the next granite_ccz4_rk3_step runs uncaptured and, in its

@@ -233,3 +233,19 @@ def test_missing_library_is_an_error_not_a_fallback(monkeypatch, tmp_path):
     monkeypatch.setattr(build, "LIB", str(tmp_path / "libgranite_ccz4.so"))
     with pytest.raises(gb.GraniteError):
         gb.load_library(build_if_missing=False)
+
+
+def test_stage_configs_and_classes_without_a_device():
+    """The TMA configuration table and the block-size classes of the autotuner
+    are host data: readable without a GPU."""
+    import granite_b200 as gb
+    for k in range(gb.STAGE_CONFIGS):
+        info = gb.stage_config_info(k)
+        assert info["tile"][:2] == (16, 4) and info["tile"][2] in (2, 4)
+        assert info["ring_slots"] in (2, 3, 4)
+    with pytest.raises(gb.GraniteError):
+        gb.stage_config_info(gb.STAGE_CONFIGS)
+    assert [gb.block_stage_class((e, e, e)) for e in gb.STAGE_CLASS_EDGES] == list(range(6))
+    assert gb.block_stage_class((16, 24, 32)) == 1  # cube root of the volume 22.9: nearest edge 24
+    assert gb.block_stage_class((32, 32, 16)) == 1  # 25.4 -> 24
+    assert gb.block_stage_class((200, 200, 200)) == 5
