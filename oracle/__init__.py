@@ -304,6 +304,12 @@ class Reference:
     def max_threads(self) -> int:
         return int(self.lib.ref_max_threads())
 
+    def last_loop_seconds(self) -> float:
+        """Wall seconds of the step loop alone of the last rk3_steps call (without
+        the hierarchy set-up, block allocation and copies around it)."""
+        self.lib.ref_last_loop_seconds.restype = C.c_double
+        return float(self.lib.ref_last_loop_seconds())
+
     def rhs(self, p: Params, g: Geom, u, rho=None, Si=None, Sij=None, S=None):
         out = g.zeros()
         p6 = p.as6()

@@ -22,6 +22,7 @@
 
 #include "ccz4_oracle.h"
 
+#include <chrono>
 #include <cstring>
 #include <iostream>
 #include <memory>
@@ -462,6 +463,12 @@ void ref_rk3_steps_matter(const double* p6, const int* n, int ng, const double* 
                           double* u, double dt, int nsteps, int bc, const double* rho, const double* Si,
                           const double* Sij, const double* S);
 
+// Wall seconds of the step loop alone of the last ref_rk3_steps(_matter) call
+// on this thread: the hierarchy, block allocation and the copies in and out
+// are set-up, not the reference's step (the CPU baseline times only this).
+static thread_local double g_last_loop_seconds = 0.0;
+double ref_last_loop_seconds() { return g_last_loop_seconds; }
+
 // nsteps single-level coarse steps: AMRHierarchy::subcycle(0) (fillGhostZones,
 // evolve, fillGhostZones; amr.cpp:303-330) around the spacetime part of
 // TimeIntegrator::sspRK3Step (main.cpp:673-689) with the reference
@@ -538,6 +545,7 @@ void ref_rk3_steps_matter(const double* p6, const int* n, int ng, const double* 
                             a3 * dt * rhs->data(v, i, j, k);
     };
     (void)N;
+    const auto t_loop = std::chrono::steady_clock::now();
     for (int s = 0; s < nsteps; ++s) {
         level_fill();
         rhs_of(st);
@@ -555,6 +563,7 @@ void ref_rk3_steps_matter(const double* p6, const int* n, int ng, const double* 
         outer(st);
         level_fill();
     }
+    g_last_loop_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_loop).count();
     std::memcpy(u, st.flatBuffer(), nbytes(st));
 }
 
