@@ -94,9 +94,11 @@ def ncu_traffic(workload: str, kernel: str):
 class Runner:
     """One workload on one device through the library's resident-block API."""
 
-    def __init__(self, gb, name, w, precision, variant, device):
+    def __init__(self, gb, name, w, precision, variant, device, stage_config=-1):
         self.gb, self.w, self.prec = gb, w, precision
         self.ev = gb.Evolver(gb.CCZ4Params(device=device), variant)
+        if stage_config >= 0:
+            self.ev.force_stage_config(stage_config)
         if w["kind"] == "hier":
             build = gb.make_binary_hierarchy if w["builder"] == "binary" else gb.make_triple_hierarchy
             self.h = build()
@@ -457,6 +459,8 @@ def main():
     ap.add_argument("--accuracy-every", type=int, default=10, help="steps between accuracy checks")
     ap.add_argument("--accuracy-seconds", type=float, default=420.0,
                     help="wall-time cap of the accuracy run")
+    ap.add_argument("--stage-config", type=int, default=-1,
+                    help="one TMA stage-kernel configuration for every block (default: the per-class table)")
     ap.add_argument("--no-amr-reference", action="store_true",
                     help="skip the GRANITE_AMR_REFERENCE hierarchy timing")
     args = ap.parse_args()
@@ -491,12 +495,12 @@ def main():
     kname = {gb.VARIANT_SMEM: "ccz4_stage_smem_kernel", gb.VARIANT_TMA: "ccz4_stage_tma_kernel"}.get(
         variant, "ccz4_stage_kernel")
     prec = gb.PRECISION_MIXED if precision == "mixed" else gb.PRECISION_FP64
-    run = Runner(gb, args.workload, w, prec, variant, local)
+    run = Runner(gb, args.workload, w, prec, variant, local, args.stage_config)
     if prec == gb.PRECISION_MIXED and args.fp64_chi > 0.0:
         run.ev.set_fp64_chi_threshold(args.fp64_chi)
     compare = None
     if prec == gb.PRECISION_MIXED and not args.no_compare:
-        compare = Runner(gb, args.workload, w, gb.PRECISION_FP64, variant, local)
+        compare = Runner(gb, args.workload, w, gb.PRECISION_FP64, variant, local, args.stage_config)
 
     for r in (run, compare):
         if r is None:
@@ -611,7 +615,10 @@ def main():
                   "sample": f"failed: {ex}"}
 
     if rank == 0:
+        cls_cfg = {p: [run.ev.stage_config(q, c) for c in range(len(gb.STAGE_CLASS_EDGES))]
+                   for p, q in (("fp64", gb.PRECISION_FP64), ("mixed", gb.PRECISION_MIXED))}
         cfg = {"workload": args.workload, "precision": precision, "kernel_variant": args.variant,
+               "stage_configs": {"class_edges": list(gb.STAGE_CLASS_EDGES), **cls_cfg},
                "fp64_chi_threshold": args.fp64_chi if prec == gb.PRECISION_MIXED else None,
                "ghosts": 4, "fields": NV, "point_updates_per_step": run.points_per_step, "dt": run.dt,
                "l2": f"inputs larger than L2: {3 * run.state_bytes / 1e9:.2f} GB resident state",

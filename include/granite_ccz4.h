@@ -470,7 +470,10 @@ GRANITE_API int granite_ccz4_launch_count(const void* ctx, long long* count);
  *     the legacy default stream) of the current device; nothing is synchronised.
  *   - The first call on a device looks up the array's device address on that
  *     device (it must be the current device); make that first call before any
- *     stream capture.
+ *     stream capture. The address is looked up again when the device's context
+ *     has changed since (after a device reset, the module can load elsewhere).
+ *   - The status reflects this call's own launches only: an error left by the
+ *     caller's earlier work is neither reported here nor cleared.
  *   - Every call shares the one array: calls whose kernels may overlap on the
  *     GPU (other streams, other host threads) race on it. Each call rewrites
  *     every partial it reads, so nothing needs clearing between calls. */
