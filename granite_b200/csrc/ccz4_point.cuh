@@ -26,6 +26,8 @@
 // values of the Hessian-field loop.
 #pragma once
 
+#include <type_traits>
+
 #include "ccz4_common.cuh"
 #include "ccz4_kernels.h"
 #include "ccz4_stencil.cuh"
@@ -71,7 +73,7 @@ struct GlobalSource {
 // EXACT: FP64 stencils in the reference's operation order (P = double only).
 template <typename P, bool EXACT, typename Src>
 __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __restrict__ u,
-                                           long long c, const StageArgs& A, Src& S, double out[NV]) {
+                                           long long c, const StageArgs& A, Src& S, P out[NV]) {
     const long long st = B.stride;
     const double* __restrict__ uc = u + c;
 #define FP(v) (uc + (long long)(v) * st)
@@ -327,7 +329,7 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
     // ---- RHS assembly ----------------------------------------------------------
     // chi (ccz4.cpp:580)
     // each field: (RHS incl. advection) + KO, the order of ccz4.cpp:864,930
-    out[CHI] = (double)(((P)(2.0 / 3.0) * chiP * (alpha * K - divb) + fchi.adv) + fchi.ko);
+    out[CHI] = (((P)(2.0 / 3.0) * chiP * (alpha * K - divb) + fchi.adv) + fchi.ko);
     // gt (ccz4.cpp:586-607)
     if constexpr (Src::HS) {
 #pragma unroll
@@ -344,13 +346,13 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
             P lie = agt[ij];
 #pragma unroll
             for (int d = 0; d < 3; ++d) lie += gt[sy(i, d)] * db[d][j] + gt[sy(j, d)] * db[d][i];
-            out[GXX + ij] = (double)(((P)-2 * alpha * At[ij] + lie - (P)(2.0 / 3.0) * gt[ij] * divb) + kgt[ij]);
+            out[GXX + ij] = (((P)-2 * alpha * At[ij] + lie - (P)(2.0 / 3.0) * gt[ij] * divb) + kgt[ij]);
         }
     // K (ccz4.cpp:650-652)
     {
         FieldDer<P> fK = S.template der<false, EXACT>(KTR, beta, w);
         const P k1 = (P)A.kappa1, k2 = (P)A.kappa2;
-        out[KTR] = (double)((-phys_lap_alpha + alpha * (AtAt + K * K / (P)3) + (P)4 * PI * alpha * (rho + Str) +
+        out[KTR] = ((-phys_lap_alpha + alpha * (AtAt + K * K / (P)3) + (P)4 * PI * alpha * (rho + Str) +
                             k1 * ((P)1 - k2) * alpha * Theta + fK.adv) + fK.ko);
         // Gamma-hat (ccz4.cpp:747-815)
         const P c3a = (P)(3.0 * alpha_d / (chi + 1e-30));
@@ -369,14 +371,14 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
             P T7 = -(Gh[0] * db[i][0] + Gh[1] * db[i][1] + Gh[2] * db[i][2]);
             T7 += aGh[i] + (P)(2.0 / 3.0) * Gh[i] * divb;
             const P T8 = (P)-2 * (P)A.kappa1 * alpha * Gh[i];
-            out[GHX + i] = (double)((T1 + T2 + T3 + T4 + T5[i] + T6 + T7 + T8) + kGh[i]);
+            out[GHX + i] = ((T1 + T2 + T3 + T4 + T5[i] + T6 + T7 + T8) + kGh[i]);
         }
     }
     // Theta (ccz4.cpp:662-665)
     {
         FieldDer<P> fT = S.template der<false, EXACT>(THETA, beta, w);
         const P k1 = (P)A.kappa1, k2 = (P)A.kappa2;
-        out[THETA] = (double)(((P)0.5 * alpha * (Rs - AtAt + (P)2 * K * K / (P)3 - (P)16 * PI * rho) -
+        out[THETA] = (((P)0.5 * alpha * (Rs - AtAt + (P)2 * K * K / (P)3 - (P)16 * PI * rho) -
                               alpha * k1 * ((P)2 + k2) * Theta + fT.adv) + fT.ko);
     }
     // A-tilde (ccz4.cpp:671-726): the advection is part of Lie_At and is
@@ -402,14 +404,14 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
         const P tr = gtu[0] * raw[0] + gtu[3] * raw[3] + gtu[5] * raw[5] +
             (P)2 * (gtu[1] * raw[1] + gtu[2] * raw[2] + gtu[4] * raw[4]);
 #pragma unroll
-        for (int a = 0; a < 6; ++a) out[AXX + a] = (double)(raw[a] - (P)(1.0 / 3.0) * gt[a] * tr + koA[a]);
+        for (int a = 0; a < 6; ++a) out[AXX + a] = (raw[a] - (P)(1.0 / 3.0) * gt[a] * tr + koA[a]);
     }
     // lapse (ccz4.cpp:820) and shift (ccz4.cpp:825-831)
-    out[ALPHA] = (double)(((P)-2 * alpha * K + fal.adv) + fal.ko);
+    out[ALPHA] = (((P)-2 * alpha * K + fal.adv) + fal.ko);
     {
         const P eta = (P)A.eta;
 #pragma unroll
-        for (int d = 0; d < 3; ++d) out[BETAX + d] = (double)(((P)0.75 * Gh[d] - eta * (P)beta[d] + abe[d]) + kbe[d]);
+        for (int d = 0; d < 3; ++d) out[BETAX + d] = (((P)0.75 * Gh[d] - eta * (P)beta[d] + abe[d]) + kbe[d]);
     }
 #undef FP
 }
@@ -458,9 +460,15 @@ __device__ __forceinline__ double rk_combine(double a1, double un, double a2, do
 }  // namespace
 
 // The RHS at one point with the algebra of precision mode PM.
+// The algebra's type of precision mode PM; the RHS values stay in it until the
+// epilogue widens them to FP64 (exact), so the FP32 form keeps 22 registers
+// instead of 44 for them.
+template <int PM>
+using AlgebraT = typename std::conditional<PM == PM_MIXED, float, double>::type;
+
 template <int PM, typename Src>
 __device__ __forceinline__ void point_pm(const DevBlock& B, const double* __restrict__ u, long long c,
-                                         const StageArgs& A, Src& S, double L[NV]) {
+                                         const StageArgs& A, Src& S, AlgebraT<PM> L[NV]) {
     if constexpr (PM == PM_FP64)
         ccz4_point<double, true>(B, u, c, A, S, L);
     else if constexpr (PM == PM_FP64F)
@@ -473,8 +481,8 @@ __device__ __forceinline__ void point_pm(const DevBlock& B, const double* __rest
 // u_in: the stage input at the point, from global memory, or (tin != nullptr)
 // from a per-thread column of shared memory that the stencil source filled with
 // each field's centre value, field v at tin[v * tin_stride].
-template <int EPI>
-__device__ __forceinline__ void stage_epilogue(const DevBlock& B, const StageArgs& A, long long c, const double L[NV],
+template <int EPI, typename T>
+__device__ __forceinline__ void stage_epilogue(const DevBlock& B, const StageArgs& A, long long c, const T L[NV],
                                                const double* tin = nullptr, int tin_stride = 0) {
     const long long st = B.stride;
     if (EPI == EPI_STORE) {

@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(TX* TY* TZ, MINB)
     const long long c = cell_index(B, i + NG, j + NG, k + NG);
     const double* __restrict__ uin = B.buf[A.in_sel];
     GlobalSource S{B, uin, c};
-    double L[NV];
+    AlgebraT<PM> L[NV];
     point_pm<PM>(B, uin, c, A, S, L);
     stage_epilogue<EPI>(B, A, c, L);
 }
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(TX* TY* TZ, 2)
     // pointwise loads of threads outside the block use a valid cell; their results are dropped
     const int ic = i < B.n[0] ? i : B.n[0] - 1, jc = j < B.n[1] ? j : B.n[1] - 1, kc = k < B.n[2] ? k : B.n[2] - 1;
     const long long c = cell_index(B, ic + NG, jc + NG, kc + NG);
-    double L[NV];
+    AlgebraT<PM> L[NV];
     point_pm<PM>(B, uin, c, A, S, L);
     if (!valid) return;  // no barrier follows the last field
     stage_epilogue<EPI>(B, A, c, L);

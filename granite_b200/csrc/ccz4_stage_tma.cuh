@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
                 for (int v = 0; v < NV; ++v) prefetch_l2(u2 + (long long)v * B2.stride);
             }
         }
-        double L[NV];
+        AlgebraT<PM> L[NV];
         point_pm<PM>(B, uin, c, A, S, L);
         if (valid) stage_epilogue<EPI>(B, A, c, L, tin, C::NT);
     }

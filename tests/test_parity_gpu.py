@@ -34,15 +34,18 @@ GROUPS = [[0], [1, 2, 3, 4, 5, 6], [7, 8, 9, 10, 11, 12], [13], [14, 15, 16], [1
 GROUP_OF = {v: g for g in GROUPS for v in g}
 
 
-def parity(gpu, ref, rtol=RTOL, what=""):
-    """Scaled per-point bound over the leading (field) axis; returns the worst ratio."""
+def parity(gpu, ref, rtol=RTOL, what="", scale=None):
+    """Scaled per-point bound over the leading (field) axis; returns the worst ratio.
+    scale: per-field magnitudes to use for s_v instead of this array's own
+    maxima (for one block of a multi-block state: the field's magnitude over all
+    blocks)."""
     worst = 0.0
     nf = ref.shape[0]
     for v in range(nf):
         o = ref[v]
         g = gpu[v]
         grp = GROUP_OF[v] if nf == 22 else [v]
-        s = max(np.abs(ref[w]).max() for w in grp)
+        s = max((np.abs(ref[w]).max() if scale is None else scale[w]) for w in grp)
         bound = rtol * np.maximum(np.abs(o), s)
         err = np.abs(g - o)
         if s == 0.0:
