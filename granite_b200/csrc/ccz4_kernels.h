@@ -31,13 +31,16 @@ int stage_tile_dims(int variant, int cfg, int* tx, int* ty, int* tz);
 // are kept in shared memory for the RK epilogue and the epilogue's u^n and the
 // next tile's pointwise cells are prefetched into L2; hs: the Hessian-field
 // loop's 36 values live in shared memory instead of local memory.
-// Configuration 0 is the untuned default and the only one with the
-// store (drop-in RHS) epilogue.
+// ws: the mixed RK kernels are warp-specialized (stencil warps feed algebra
+// warps through shared memory; ccz4_stage_ws.cuh), the FP64 ones those of
+// configuration 4. Configuration 0 is the untuned default and the only one
+// with the store (drop-in RHS) epilogue.
 struct TmaCfg {
-    int tz, nbuf, tin, hs;
+    int tz, nbuf, tin, hs, ws;
 };
-constexpr int NUM_TMA_CFGS = 5;
-constexpr TmaCfg TMA_CFGS[NUM_TMA_CFGS] = {{4, 3, 0, 0}, {4, 3, 1, 1}, {2, 3, 1, 1}, {2, 2, 1, 1}, {2, 3, 1, 0}};
+constexpr int NUM_TMA_CFGS = 6;
+constexpr TmaCfg TMA_CFGS[NUM_TMA_CFGS] = {{4, 3, 0, 0, 0}, {4, 3, 1, 1, 0}, {2, 3, 1, 1, 0},
+                                           {2, 2, 1, 1, 0}, {2, 3, 1, 0, 0}, {2, 3, 0, 0, 1}};
 // The box (cells incl. the 4-cell halo) one tensor-map load brings in per
 // field: 24 x 12 x (tz + 8). Tensor maps exist per box shape: shape 0 (tz = 4)
 // and shape 1 (tz = 2).

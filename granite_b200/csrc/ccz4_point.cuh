@@ -23,7 +23,8 @@
 // A stencil source S provides der<HESS, EXACT>(v, beta, w), the derivatives of
 // field v, called for the fields in FIELD_ORDER; S::HS says whether it also
 // provides per-thread shared-memory slots (hess_slots, stride S::NT) for the
-// values of the Hessian-field loop.
+// values of the Hessian-field loop, and S::UNROLL whether that loop may be
+// unrolled (a source whose der() is short).
 #pragma once
 
 #include <type_traits>
@@ -55,7 +56,8 @@ __device__ __forceinline__ bool tile_selected(const unsigned char* prec, int wan
 // evaluates the stencils of one field in the precision of the caller's algebra
 // (P = double or float, deduced from the blend weight w).
 struct GlobalSource {
-    static constexpr bool HS = false;  // the Hessian-field loop's values stay in (local) registers
+    static constexpr bool HS = false;      // the Hessian-field loop's values stay in (local) registers
+    static constexpr bool UNROLL = false;  // and the loop stays rolled (stencil code is long)
     const DevBlock& B;
     const double* __restrict__ u;
     long long c;
@@ -147,6 +149,18 @@ __device__ __forceinline__ void ccz4_point(const DevBlock& B, const double* __re
         for (int a = 0; a < 6; ++a)
 #pragma unroll
             for (int d = 0; d < 3; ++d) dg[a][d] = hs[(3 * a + d) * T];
+    } else if constexpr (Src::UNROLL) {
+        // a source that evaluates no stencils has a short loop body: unrolled, in registers
+#pragma unroll
+        for (int a = 0; a < 6; ++a) {
+            FieldDer<P> fd = S.template der<true, EXACT>(GXX + a, beta, w);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) dg[a][d] = fd.d[d];
+            Rt[a] = (P)-0.5 * (gtu[0] * fd.h[0] + gtu[3] * fd.h[3] + gtu[5] * fd.h[5] +
+                               (P)2 * (gtu[1] * fd.h[1] + gtu[2] * fd.h[2] + gtu[4] * fd.h[4]));
+            agt[a] = fd.adv;
+            kgt[a] = fd.ko;
+        }
     } else {
 #pragma unroll 1
         for (int a = 0; a < 6; ++a) {

@@ -101,7 +101,7 @@ __shared__ int g_sel_list[TMA_SEL_CAP + 1];
 
 template <class C, bool SEL>
 struct TmaSource {
-    static constexpr bool HS = C::HS;
+    static constexpr bool HS = C::HS, UNROLL = false;
     static constexpr int NT = C::NT;
     const DevBlock* blocks;
     const Tile* tiles;
