@@ -387,7 +387,8 @@ def accuracy(gb, a: Runner, b: Runner, steps: int):
     gscale = np.zeros(NV)
     for grp in GROUPS:
         gscale[grp] = mag[grp].max()
-    rel = dev / np.maximum(gscale, 1e-300)
+    with np.errstate(invalid="ignore"):
+        rel = np.where(np.isfinite(dev), dev / np.maximum(gscale, 1e-300), np.inf)
     ha, ma = a.ev.constraint_norms(-1)
     hb, mb = b.ev.constraint_norms(-1)
     finite = nf[0] == 0 and bool(np.isfinite(ha) and np.isfinite(ma))
@@ -403,11 +404,15 @@ def accuracy_run(gb, a: Runner, b: Runner, steps: int, every: int, seconds: floa
     state goes non-finite (the reference's equations on puncture data are not
     long-term stable) or `seconds` of wall time pass. Reports the comparison
     at the last step where the FP64 state was finite, the largest deviation up
-    to there, and a thinned history [step, max_rel_dev, h_l2_ratio]."""
+    to there and while ||H||_2 of the FP64 state stayed within 10x of its
+    initial value (the solution still bounded), and a thinned history
+    [step, max_rel_dev, h_l2_ratio, h_l2_fp64]."""
     for r in (a, b):
         r.ev.upload()
         r.ev.sync()
+    h0 = a.ev.constraint_norms(-1)[0]
     last, worst, hist, stop = None, 0.0, [], "steps"
+    worst_bounded, bounded_until, still_bounded = 0.0, 0, True
     t0 = time.perf_counter()
     for s in range(1, steps + 1):
         a.step()
@@ -421,13 +426,20 @@ def accuracy_run(gb, a: Runner, b: Runner, steps: int, every: int, seconds: floa
             break
         last = r
         worst = max(worst, r["max_rel_dev"])
-        hist.append([s, r["max_rel_dev"], r["h_l2_ratio"]])
+        if still_bounded and r["h_l2_fp64"] <= 10.0 * h0:
+            worst_bounded = max(worst_bounded, r["max_rel_dev"])
+            bounded_until = s
+        else:
+            still_bounded = False
+        hist.append([s, r["max_rel_dev"], r["h_l2_ratio"], r["h_l2_fp64"]])
         if time.perf_counter() - t0 > seconds:
             stop = "time cap"
             break
     out = dict(last) if last else {"coarse_steps": 0}
     out.update({"steps_requested": steps, "check_every": every, "stopped_by": stop,
-                "max_rel_dev_over_run": worst, "wall_s": time.perf_counter() - t0,
+                "max_rel_dev_over_run": worst, "h_l2_fp64_initial": h0,
+                "bounded_until_step": bounded_until, "max_rel_dev_while_bounded": worst_bounded,
+                "wall_s": time.perf_counter() - t0,
                 "history": hist[:: max(1, len(hist) // 20)] + ([hist[-1]] if hist else [])})
     if stop == "fp64 state non-finite":
         out["fp64_nonfinite_by_step"] = first_bad
@@ -456,7 +468,7 @@ def main():
                     help="mixed runs: step FP64 and mixed side by side from the initial state for up to "
                          "this many steps (coarse steps of a hierarchy), or until the FP64 state goes "
                          "non-finite, and report the deviation there (0 = only after the warm-up)")
-    ap.add_argument("--accuracy-every", type=int, default=10, help="steps between accuracy checks")
+    ap.add_argument("--accuracy-every", type=int, default=1, help="steps between accuracy checks")
     ap.add_argument("--accuracy-seconds", type=float, default=420.0,
                     help="wall-time cap of the accuracy run")
     ap.add_argument("--stage-config", type=int, default=-1,

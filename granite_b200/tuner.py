@@ -86,9 +86,10 @@ def time_config(blocks, dx: float, precision: int, cfg: int, steps: int = 3, war
 
 
 def tune(classes=None, configs=None, precisions=("fp64", "mixed"), steps: int = 3, fp64_chi: float = 0.5,
-         device: int = 0, target_points: int = 1 << 21, log=None) -> dict:
+         device: int = 0, target_points: int = 1 << 21, margin: float = 0.01, log=None) -> dict:
     """Time every configuration for every class and precision; returns the
-    table (fastest configuration per class; classes not tuned keep None) and
+    table (per class the fastest configuration, or configuration 0 unless the
+    fastest beats it by more than `margin`; classes not tuned keep None) and
     the timings in ns per point-stage."""
     classes = list(STAGE_CLASS_EDGES if classes is None else classes)
     configs = list(range(STAGE_CONFIGS) if configs is None else configs)
@@ -108,10 +109,14 @@ def tune(classes=None, configs=None, precisions=("fp64", "mixed"), steps: int = 
                     log(f"class {edge:3d} {pname:5s} cfg {cfg}: {row[cfg]:.4f} ns/point-stage "
                         f"({time.perf_counter() - t0:.1f} s)")
             timings[pname][str(edge)] = {str(k): v for k, v in row.items()}
-            table[pname][cls] = min(row, key=row.get)
+            best = min(row, key=row.get)
+            # configuration 0 unless another is faster by more than run-to-run noise
+            if 0 in row and row[best] > (1.0 - margin) * row[0]:
+                best = 0
+            table[pname][cls] = best
     return {"classes": list(STAGE_CLASS_EDGES), "table": table, "timings_ns_per_point_stage": timings,
             "configs": {str(k): stage_config_info(k) for k in configs}, "steps": steps,
-            "fp64_chi_threshold": fp64_chi, "target_points": target_points}
+            "fp64_chi_threshold": fp64_chi, "target_points": target_points, "margin": margin}
 
 
 def main(argv=None) -> int:
