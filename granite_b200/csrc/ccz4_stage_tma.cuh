@@ -69,6 +69,18 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
         : "memory");
     return ok != 0;
 }
+// The same test with a suspend-time hint: a thread whose phase is not complete
+// yet is suspended (issuing nothing) until it completes or about hint_ns pass,
+// instead of spinning.
+__device__ __forceinline__ bool mbar_try_wait_sleep(unsigned bar, unsigned parity, unsigned hint_ns) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -93,6 +105,8 @@ __device__ __forceinline__ void prefetch_l2(const double* p) {
 // failure in StageArgs::errflag and stops waiting (results are then garbage
 // and the host reports the error).
 constexpr unsigned long long TMA_WAIT_NS = 2000000000ull;
+// Suspend-time hint of one wait attempt (the limit is checked between attempts).
+constexpr unsigned TMA_WAIT_HINT_NS = 100000u;
 
 // Per-tile precision launches: the CTA's selected tiles, in order, and their
 // count at [TMA_SEL_CAP] (shared memory at a fixed address, so the per-point
@@ -147,19 +161,15 @@ struct TmaSource {
     __device__ __forceinline__ void wait(int q) {
         if (failed) return;
         const unsigned bar = bar0 + 8u * (q % C::NBUF), parity = (q / C::NBUF) & 1;
-        unsigned long long t0 = 0;
-        for (unsigned it = 1;; ++it) {
-            if (mbar_try_wait(bar, parity)) return;
-            if ((it & 255u) == 0) {
-                const unsigned long long now = global_ns();
-                if (t0 == 0) {
-                    t0 = now;
-                } else if (now - t0 > TMA_WAIT_NS) {
-                    failed = true;
-                    fail_q = q;
-                    if (err) atomicExch(err, 1u);
-                    return;
-                }
+        if (mbar_try_wait(bar, parity)) return;
+        const unsigned long long t0 = global_ns();
+        for (;;) {
+            if (mbar_try_wait_sleep(bar, parity, TMA_WAIT_HINT_NS)) return;
+            if (global_ns() - t0 > TMA_WAIT_NS) {
+                failed = true;
+                fail_q = q;
+                if (err) atomicExch(err, 1u);
+                return;
             }
         }
     }

@@ -55,22 +55,26 @@ __device__ __forceinline__ void mbar_arrive(unsigned bar) {
 }
 // Bounded wait for the completion of the phase of parity `parity`; on a
 // timeout the failure is recorded and the thread's later waits are skipped.
+// (A waiting warp is suspended rather than spinning, so it takes no issue
+// slots from the warps it waits for.)
 __device__ __forceinline__ void ws_wait(unsigned bar, unsigned parity, bool& failed, unsigned int* err) {
     if (failed) return;
-    unsigned long long t0 = 0;
-    for (unsigned it = 1;; ++it) {
-        if (mbar_try_wait(bar, parity)) return;
-        if ((it & 255u) == 0) {
-            const unsigned long long now = global_ns();
-            if (t0 == 0) {
-                t0 = now;
-            } else if (now - t0 > TMA_WAIT_NS) {
-                failed = true;
-                if (err) atomicExch(err, 1u);
-                return;
-            }
+    if (mbar_try_wait(bar, parity)) return;
+    const unsigned long long t0 = global_ns();
+    for (;;) {
+        if (mbar_try_wait_sleep(bar, parity, TMA_WAIT_HINT_NS)) return;
+        if (global_ns() - t0 > TMA_WAIT_NS) {
+            failed = true;
+            if (err) atomicExch(err, 1u);
+            return;
         }
     }
+}
+// One arrival per warp, after every lane's shared-memory accesses (the warp
+// barrier orders them before lane 0's release).
+__device__ __forceinline__ void warp_arrive(unsigned bar) {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) mbar_arrive(bar);
 }
 __device__ __forceinline__ void producer_barrier() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
 
@@ -102,7 +106,7 @@ struct DerivSource {
         r.ko = s[4 * C::NP];
 #pragma unroll
         for (int a = 0; a < 6; ++a) r.h[a] = HESS ? s[(5 + a) * C::NP] : (P)0;
-        mbar_arrive(empty0 + 8u * d);
+        warp_arrive(empty0 + 8u * d);
         ++q;
         return r;
     }
@@ -126,8 +130,8 @@ __global__ void __launch_bounds__(C::NTHR, C::MINB)
     if (tid == 0) {
         for (int s = 0; s < C::NBUF; ++s) mbar_init(tbar0 + 8u * s, 1);
         for (int s = 0; s < C::DBUF; ++s) {
-            mbar_init(full0 + 8u * s, C::NP);   // every producer thread arrives
-            mbar_init(empty0 + 8u * s, C::NP);  // every consumer thread arrives
+            mbar_init(full0 + 8u * s, C::NP / 32);   // every producer warp arrives
+            mbar_init(empty0 + 8u * s, C::NP / 32);  // every consumer warp arrives
         }
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
@@ -232,7 +236,7 @@ __global__ void __launch_bounds__(C::NTHR, C::MINB)
 #pragma unroll
                     for (int a = 0; a < 6; ++a) s[(5 + a) * C::NP] = fd.h[a];
                 }
-                mbar_arrive(full0 + 8u * d);
+                warp_arrive(full0 + 8u * d);
             }
         }
         // no bulk copy into shared memory may outlive the CTA: when a wait of the

@@ -89,37 +89,43 @@ __device__ __forceinline__ AxisDer<double> axis_exact(const L& f, long long s, d
     return r;
 }
 
-// Pair-difference evaluation; the upwind side is selected without a branch as
-// in axis_exact. The pair differences and their weighted sums stay FP64
-// (small, exactly cancelled numbers) and each stencil result is rounded to P
-// once: for P = float one conversion per derivative instead of one per pair;
-// for P = double this is the contraction-friendly FP64 form (no reference
-// operation order) used where bit parity with the host code is not required.
+// Pair-difference evaluation (P = float: the mixed form; P = double: the FP64
+// pass of the per-tile precision, equal to the reference-order form to
+// rounding). The pair differences and their weighted sums stay FP64 (small,
+// exactly cancelled numbers) and each derivative the algebra uses is rounded
+// to P once. The advection and KO terms are sums over the three axes: they
+// are accumulated in FP64 (upd, kod) and rounded once per field by the caller,
+// which saves two conversions per axis.
+//
+// The upwind stencil (ccz4.cpp:109-152) takes the side of the shift: for
+// beta >= 0, e = 25 f0 - 48 g1 + 36 g2 - 16 g3 + 3 g4 with g_k = f[-k], and
+// beta e goes into the advection sum; for beta < 0 the mirror (g_k = f[+k])
+// with -e, so the term is |beta| e either way and needs no select of e. The
+// fourth neighbour is loaded once from the selected side (sgn_s = -s or +s).
 template <bool WANT_D2, bool WANT_KO, typename P, typename L>
-__device__ __forceinline__ AxisDer<P> axis_pairs(const L& f, long long s, double f0,
-                                                double beta, double inv12h, double inv12h2, double kocf,
-                                                P& ko) {
-    const double fm1 = f(-s), fp1 = f(s);
-    const double fm2 = f(-2 * s), fp2 = f(2 * s);
-    const double fm3 = f(-3 * s), fp3 = f(3 * s);
-    const double fm4 = f(-4 * s), fp4 = f(4 * s);
-    AxisDer<P> r;
+__device__ __forceinline__ void axis_pairs(const L& f, long long s, long long sgn_s, double f0, double beta,
+                                           double inv12h, double inv12h2, double kocf, P& d1, P& d2,
+                                           double& upd, double& kod) {
+    // differences from the centre, a_k = f[-k] - f0 and b_k = f[+k] - f0, shared by
+    // every stencil below
+    const double a1 = f(-s) - f0, b1 = f(s) - f0;
+    const double a2 = f(-2 * s) - f0, b2 = f(2 * s) - f0;
+    const double a3 = f(-3 * s) - f0, b3 = f(3 * s) - f0;
+    const double c4 = f(4 * sgn_s) - f0;
     // 8 (f+1 - f-1) - (f+2 - f-2)
-    r.d1 = (P)inv12h * (P)(8.0 * (fp1 - fm1) - (fp2 - fm2));
+    d1 = (P)inv12h * (P)(8.0 * (b1 - a1) - (b2 - a2));
     const bool pos = beta >= 0.0;
-    const double g1 = pos ? fm1 : fp1, g2 = pos ? fm2 : fp2, g3 = pos ? fm3 : fp3, g4 = pos ? fm4 : fp4;
-    // 25 f0 - 48 g1 + 36 g2 - 16 g3 + 3 g4 with weights summing to zero; negated for the + side
-    const double e = 48.0 * (f0 - g1) - 36.0 * (f0 - g2) + 16.0 * (f0 - g3) - 3.0 * (f0 - g4);
-    r.up = (P)inv12h * (P)(pos ? e : -e);
-    const double t1 = (fp1 - f0) + (fm1 - f0);
-    const double t2 = (fp2 - f0) + (fm2 - f0);
-    r.d2 = WANT_D2 ? (P)inv12h2 * (P)(16.0 * t1 - t2) : (P)0;
+    const double x1 = pos ? a1 : b1, x2 = pos ? a2 : b2, x3 = pos ? a3 : b3;
+    // 25 f0 - 48 g1 + 36 g2 - 16 g3 + 3 g4 (g: the upwind side), weights summing to zero
+    const double e = -48.0 * x1 + 36.0 * x2 - 16.0 * x3 + 3.0 * c4;
+    upd += (fabs(beta) * inv12h) * e;
+    const double t1 = b1 + a1;
+    const double t2 = b2 + a2;
+    d2 = WANT_D2 ? (P)inv12h2 * (P)(16.0 * t1 - t2) : (P)0;
     if (WANT_KO) {
-        const double t3 = (fp3 - f0) + (fm3 - f0);
         // (f-3 + f+3) - 6 (f-2 + f+2) + 15 (f-1 + f+1) - 20 f0
-        ko += (P)kocf * (P)(t3 - 6.0 * t2 + 15.0 * t1);
+        kod += kocf * ((b3 + a3) - 6.0 * t2 + 15.0 * t1);
     }
-    return r;
 }
 
 // 2nd-order mixed derivative, ccz4.cpp:185-222: inv4hh * (f++ - f+- - f-+ + f--),
@@ -151,24 +157,34 @@ __device__ __forceinline__ FieldDer<P> field_der_l(const DevBlock& B, const L& f
     static_assert(!EXACT || sizeof(P) == 8, "reference-order stencils are FP64");
     const double f0 = f(0);
     FieldDer<P> r;
-    P up[3];
-    P ko = (P)0;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        AxisDer<P> a;
-        if constexpr (EXACT)
-            a = axis_exact<HESS, KO>(f, off[d], f0, beta[d], B.inv12h[d], B.inv12h2[d], B.kow[d], ko);
-        else
-            a = axis_pairs<HESS, KO, P>(f, off[d], f0, beta[d], B.inv12h[d], B.inv12h2[d], B.kocf[d], ko);
-        r.d[d] = a.d1;
-        up[d] = a.up;
-        if (HESS) r.h[d == 0 ? 0 : (d == 1 ? 3 : 5)] = a.d2;
-    }
     const P b0 = (P)beta[0], b1 = (P)beta[1], b2 = (P)beta[2];
-    const P up_sum = b0 * up[0] + b1 * up[1] + b2 * up[2];
-    const P cen_sum = b0 * r.d[0] + b1 * r.d[1] + b2 * r.d[2];
-    r.adv = w * up_sum + ((P)1 - w) * cen_sum;
-    r.ko = ko;
+    if constexpr (EXACT) {
+        P up[3];
+        P ko = (P)0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const AxisDer<P> a = axis_exact<HESS, KO>(f, off[d], f0, beta[d], B.inv12h[d], B.inv12h2[d], B.kow[d], ko);
+            r.d[d] = a.d1;
+            up[d] = a.up;
+            if (HESS) r.h[d == 0 ? 0 : (d == 1 ? 3 : 5)] = a.d2;
+        }
+        const P up_sum = b0 * up[0] + b1 * up[1] + b2 * up[2];
+        const P cen_sum = b0 * r.d[0] + b1 * r.d[1] + b2 * r.d[2];
+        r.adv = w * up_sum + ((P)1 - w) * cen_sum;
+        r.ko = ko;
+    } else {
+        double upd = 0.0, kod = 0.0;  // sum_d beta_d up_d and the KO sum, FP64
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            P d2;
+            axis_pairs<HESS, KO, P>(f, off[d], beta[d] >= 0.0 ? -off[d] : off[d], f0, beta[d], B.inv12h[d],
+                                    B.inv12h2[d], B.kocf[d], r.d[d], d2, upd, kod);
+            if (HESS) r.h[d == 0 ? 0 : (d == 1 ? 3 : 5)] = d2;
+        }
+        const P cen_sum = b0 * r.d[0] + b1 * r.d[1] + b2 * r.d[2];
+        r.adv = w * (P)upd + ((P)1 - w) * cen_sum;
+        r.ko = (P)kod;
+    }
     if (HESS) {
         r.h[1] = dmix<P, EXACT, L>(f, off[0], off[1], B.inv4hh[0]);
         r.h[2] = dmix<P, EXACT, L>(f, off[0], off[2], B.inv4hh[1]);
