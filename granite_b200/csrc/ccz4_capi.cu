@@ -69,9 +69,10 @@ bool encode_block_tmap(void* map128, const double* base, const DevBlock& d, int 
 namespace {
 
 // Stage configuration per (precision: FP64, MIXED) and block-size class
-// (GRANITE_STAGE_CLASS_EDGES) until a caller sets its own: the winners of the
-// autotuner (granite_b200/tuner.py) on a B200.
-constexpr int DEFAULT_CLASS_CFG[2][GRANITE_STAGE_CLASSES] = {{0, 0, 3, 0, 0, 3}, {4, 0, 4, 3, 4, 3}};
+// (GRANITE_STAGE_CLASS_EDGES) until a caller sets its own: the autotuner's
+// (granite_b200/tuner.py) uniform table on a B200, one configuration per
+// precision, so a level stage stays one launch.
+constexpr int DEFAULT_CLASS_CFG[2][GRANITE_STAGE_CLASSES] = {{0, 0, 0, 0, 0, 0}, {4, 4, 4, 4, 4, 4}};
 
 static_assert(sizeof(CUtensorMap) == 128, "tensor maps are 128 bytes");
 static_assert(alignof(CUtensorMap) >= 64, "tensor maps are 64-byte aligned");

@@ -11,8 +11,11 @@ level of equal cubic blocks of that edge carrying single-puncture data (about
 two million interior points, so a launch takes about a millisecond), with CUDA
 events around every stage launch (the library's profiler), and keeps the
 fastest. The result is a table {"fp64": [cfg per class], "mixed": [...]} that
-Evolver.apply_stage_table applies; the library's built-in default table is the
-one this module produced on a B200.
+Evolver.apply_stage_table applies, and a uniform table (one configuration per
+precision for every class): a level whose blocks use different configurations
+runs one launch per configuration, and on hierarchies of mixed block sizes the
+extra launch tails cost more than the per-class gains, so the library's
+built-in default is the uniform table this module produced on a B200.
 
     python -m granite_b200.tuner [--out table.json] [--classes 16,24] [--steps 3]
 """
@@ -114,7 +117,20 @@ def tune(classes=None, configs=None, precisions=("fp64", "mixed"), steps: int = 
             if 0 in row and row[best] > (1.0 - margin) * row[0]:
                 best = 0
             table[pname][cls] = best
-    return {"classes": list(STAGE_CLASS_EDGES), "table": table, "timings_ns_per_point_stage": timings,
+    # one configuration per precision for every class: a level whose blocks use
+    # different configurations runs one launch per configuration, and every
+    # extra persistent launch adds a tail; the uniform choice minimises the sum
+    # of the per-class times (configuration 0 unless beaten by the margin)
+    uniform = {}
+    for pname in precisions:
+        rows = [timings[pname][str(e)] for e in classes]
+        tot = {cfg: sum(r[str(cfg)] for r in rows) for cfg in configs}
+        best = min(tot, key=tot.get)
+        if 0 in tot and tot[best] > (1.0 - margin) * tot[0]:
+            best = 0
+        uniform[pname] = [best] * len(STAGE_CLASS_EDGES)
+    return {"classes": list(STAGE_CLASS_EDGES), "table": table, "uniform_table": uniform,
+            "timings_ns_per_point_stage": timings,
             "configs": {str(k): stage_config_info(k) for k in configs}, "steps": steps,
             "fp64_chi_threshold": fp64_chi, "target_points": target_points, "margin": margin}
 
