@@ -153,6 +153,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_level_time.argtypes = [vp, C.c_int, dp]
     lib.granite_ccz4_tag_count.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_longlong)]
     lib.granite_ccz4_test_withhold_tile_load.argtypes = [vp, C.c_int]
+    lib.granite_ccz4_set_ghost_push.argtypes = [vp, C.c_int]
     ip_ = C.POINTER(C.c_int)
     lib.granite_ccz4_set_stage_config.argtypes = [vp, C.c_int, C.c_int, C.c_int]
     lib.granite_ccz4_get_stage_config.argtypes = [vp, C.c_int, C.c_int, ip_]
@@ -470,6 +471,10 @@ class Evolver:
         self.committed = False
         if variant is not None:
             self.ctx.check(self.ctx.lib.granite_ccz4_set_kernel_variant(self.ctx.h, variant))
+
+    def set_ghost_push(self, on: bool):
+        """GRANITE_AMR_GHOSTS: stage kernels write the same-level ghost copies (default) or the fills copy them."""
+        self.ctx.check(self.ctx.lib.granite_ccz4_set_ghost_push(self.ctx.h, int(bool(on))))
 
     def set_batching(self, batched: bool):
         self.ctx.check(self.ctx.lib.granite_ccz4_set_batching(self.ctx.h, int(bool(batched))))

@@ -98,6 +98,7 @@ struct LevelLists {
     // stage-kernel tiles: per precision (0 FP64, 1 MIXED) grouped by
     // configuration (groups), each block's tiles contiguous (tile_range)
     Tile* d_tiles = nullptr;
+    std::vector<Tile> h_tiles;       // host copy of d_tiles (push lists are built from it)
     std::vector<StageGroup> groups[2];
     std::vector<int> block_cfg[2];  // per block of the level: its configuration
     int ntiles = 0;
@@ -139,6 +140,19 @@ struct LevelXfer {
     GhostSrc* d_src_stage = nullptr;
     long long nsrc_stage = 0;
     std::vector<std::pair<long long, long long>> src_range_stage;
+    // same-level copies pushed by the stage kernels (push_ok: the level's
+    // interiors do not overlap and its stage kernel is the TMA variant): the
+    // push boxes, per stage tile its range of them, and the ghost sources
+    // without the copies for the fills that follow a pushing stage
+    bool push_ok = false;
+    PushBox* d_push = nullptr;
+    int2* d_tile_push = nullptr;
+    GhostSrc* d_src_nc = nullptr;
+    long long nsrc_nc = 0;
+    std::vector<std::pair<long long, long long>> src_range_nc;
+    GhostSrc* d_src_stage_nc = nullptr;
+    long long nsrc_stage_nc = 0;
+    std::vector<std::pair<long long, long long>> src_range_stage_nc;
 };
 
 // device copy of a host vector (nullptr for an empty one)
@@ -180,6 +194,7 @@ struct Ctx {
     unsigned long long* d_nonfinite = nullptr;
     unsigned int* d_errflag = nullptr;   // set by a TMA stage kernel whose bounded wait gave up
     int test_withhold = 0;               // armed test switch (StageArgs::test_withhold) of the next rk3_step
+    bool ghost_push = true;              // GRANITE_AMR_GHOSTS: stage kernels push same-level ghost copies
     unsigned long long* d_cmp = nullptr; // granite_ccz4_compare_states results (46 words)
     CUtensorMap* d_tmaps = nullptr;      // TMA variant: per box shape, 3 maps per resident block (slots 0-2)
     CUtensorMap* s_tmap = nullptr;       // TMA variant: map of the stateless single-block input
@@ -697,6 +712,16 @@ static int check_errflag(Ctx* c) {
     return GRANITE_OK;
 }
 
+int granite_ccz4_set_ghost_push(void* h, int on) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    c->ghost_push = on != 0;
+    for (auto& kv : c->hgraphs)  // captured steps bake the choice in
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    c->hgraphs.clear();
+    return GRANITE_OK;
+}
+
 int granite_ccz4_test_withhold_tile_load(void* h, int item) {
     Ctx* c = static_cast<Ctx*>(h);
     if (!c) return GRANITE_ERR_INVALID;
@@ -998,6 +1023,10 @@ static void release_lists(Ctx* c) {
             cudaFree(X.d_facemask);
             cudaFree(X.d_src);
             cudaFree(X.d_src_stage);
+            cudaFree(X.d_push);
+            cudaFree(X.d_tile_push);
+            cudaFree(X.d_src_nc);
+            cudaFree(X.d_src_stage_nc);
         }
         c->xfer[m].clear();
         c->xfer_built[m] = false;
@@ -1065,6 +1094,7 @@ static int build_lists(Ctx* c) {
             ll.interior_points += (long long)c->descs[i].ncells[0] * c->descs[i].ncells[1] * c->descs[i].ncells[2];
         }
         CK(upload_vec(tiles, &ll.d_tiles, c->stream), "upload tiles");
+        ll.h_tiles = tiles;
         CK(upload_vec(mtiles, &ll.d_mtiles, c->stream), "upload monitor tiles");
         ll.nmtiles = (int)mtiles.size();
         CK(upload_vec(ghosts, &ll.d_ghost, c->stream), "upload ghost chunks");
@@ -1317,6 +1347,7 @@ static cudaError_t stage_range(Ctx* c, LevelLists& L, int cfg, int precision, co
     StageArgs a = a0;
     if (L.variant == VARIANT_TMA)  // the tensor maps of this configuration's box shape
         a.tmaps = c->d_tmaps + (size_t)tma_shape_of(cfg) * 3 * c->descs.size();
+    if (a.tile_push) a.tile_push += first;  // indexed like the launch's tiles
     // (the TMA kernel keeps a CTA's selected tiles in shared memory: bounded count)
     const bool split = precision == GRANITE_PRECISION_MIXED && c->fp64_chi > 0.0 &&
         (L.variant != VARIANT_TMA || (long long)count <= (long long)tma_grid(cfg) * TMA_SEL_CAP);
@@ -1653,6 +1684,80 @@ int build_ghosts_mode(Ctx* c) {
             X[L].nsrc = (long long)items.size();
             CK(upload_vec(sitems, &X[L].d_src_stage, c->stream), "upload stage ghost sources");
             X[L].nsrc_stage = (long long)sitems.size();
+            // the same lists without the same-level copies (for the fills after a pushing stage)
+            auto nocopy = [](const std::vector<GhostSrc>& all, const std::vector<std::pair<long long, long long>>& rg,
+                             std::vector<GhostSrc>& out, std::vector<std::pair<long long, long long>>& orange) {
+                for (const auto& r : rg) {
+                    const long long f = (long long)out.size();
+                    for (long long q = r.first; q < r.first + r.second; ++q)
+                        if (!(all[q].src_block >= 0 && all[q].src_cell >= 0)) out.push_back(all[q]);
+                    orange.push_back({f, (long long)out.size() - f});
+                }
+            };
+            std::vector<GhostSrc> nc, snc;
+            X[L].src_range_nc.clear();
+            X[L].src_range_stage_nc.clear();
+            nocopy(items, X[L].src_range, nc, X[L].src_range_nc);
+            nocopy(sitems, X[L].src_range_stage, snc, X[L].src_range_stage_nc);
+            CK(upload_vec(nc, &X[L].d_src_nc, c->stream), "upload ghost sources without copies");
+            X[L].nsrc_nc = (long long)nc.size();
+            CK(upload_vec(snc, &X[L].d_src_stage_nc, c->stream), "upload stage ghost sources without copies");
+            X[L].nsrc_stage_nc = (long long)snc.size();
+        }
+        // push boxes: every copy box (a <- b) seen from b's interior, and per
+        // stage tile of the level the boxes of its block that meet the tile.
+        // Only where no two interiors of the level overlap (then every ghost
+        // cell has at most one same-level source, the one the fill would copy).
+        {
+            bool ovl = false;
+            for (size_t p = 0; p < blocks.size() && !ovl; ++p)
+                for (size_t q = p + 1; q < blocks.size() && !ovl; ++q) {
+                    bool all = true;
+                    for (int d = 0; d < 3 && all; ++d)
+                        all = !meet({G[blocks[p]][d], G[blocks[p]][d] + c->descs[blocks[p]].ncells[d]},
+                                    {G[blocks[q]][d], G[blocks[q]][d] + c->descs[blocks[q]].ncells[d]})
+                                   .empty();
+                    ovl = all;
+                }
+            LevelLists& ll = c->levels[L];
+            X[L].push_ok = !ovl && ll.variant == VARIANT_TMA && !ll.h_tiles.empty();
+            if (X[L].push_ok) {
+                std::map<int, std::vector<PushBox>> by_src;
+                for (const XferBox& x : copies) {
+                    PushBox pb{};
+                    pb.dst = x.dst;
+                    for (int d = 0; d < 3; ++d) {
+                        pb.lo[d] = x.s0[d] - NG;
+                        pb.hi[d] = pb.lo[d] + x.n[d];
+                        pb.off[d] = x.d0[d] + NG - x.s0[d];
+                    }
+                    by_src[x.src].push_back(pb);
+                }
+                std::vector<PushBox> plist;
+                std::vector<int2> tp(ll.h_tiles.size(), make_int2(0, 0));
+                for (int pr = 0; pr < 2; ++pr)
+                    for (const StageGroup& g : ll.groups[pr]) {
+                        int TX, TY, TZ;
+                        stage_tile_dims(ll.variant, g.cfg, &TX, &TY, &TZ);
+                        const int tdim[3] = {TX, TY, TZ};
+                        for (int t = g.first; t < g.first + g.count; ++t) {
+                            const Tile& tl = ll.h_tiles[t];
+                            const int t0[3] = {tl.i0, tl.j0, tl.k0};
+                            const int first = (int)plist.size();
+                            auto it = by_src.find(tl.block);
+                            if (it != by_src.end())
+                                for (const PushBox& pb : it->second) {
+                                    bool hit = true;
+                                    for (int d = 0; d < 3 && hit; ++d) hit = pb.lo[d] < t0[d] + tdim[d] && pb.hi[d] > t0[d];
+                                    if (hit) plist.push_back(pb);
+                                }
+                            tp[t] = make_int2(first, (int)plist.size() - first);
+                        }
+                    }
+                CK(upload_vec(plist, &X[L].d_push, c->stream), "upload push boxes");
+                CK(upload_vec(tp, &X[L].d_tile_push, c->stream), "upload tile push ranges");
+                if (!X[L].d_push) X[L].push_ok = false;  // nothing to push on this level
+            }
         }
         // restriction into level L-1 from level L: one launch for the level, or,
         // where fine interiors overlap (a regrid adds blocks beside the old ones),
@@ -1797,7 +1902,7 @@ cudaError_t xfer(Ctx* c, int kind, const XferList& x, int dst_sel, int src_sel) 
 
 // Ghost fill of one level's buffer slot. level_fill: the fill around a step
 // (zero-gradient base); otherwise a stage fill (1/r falloff base).
-cudaError_t fill_level(Ctx* c, int L, int slot, bool level_fill, int mode, long long* n) {
+cudaError_t fill_level(Ctx* c, int L, int slot, bool level_fill, int mode, long long* n, bool pushed = false) {
     LevelLists& ll = c->levels[L];
     const LevelXfer& X = c->xfer[mode][L];
     cudaError_t e;
@@ -1817,17 +1922,21 @@ cudaError_t fill_level(Ctx* c, int L, int slot, bool level_fill, int mode, long 
     // covers it, else from the coarse level, else from the block's own fill. The
     // state (slot 0) gets every ghost cell (finer levels prolong from it, callers
     // read it); an RK stage buffer only the cells the stage stencils read.
+    // after a stage that pushed the same-level copies, the lists without them
     const int local = level_fill ? GHOST_ZERO_GRADIENT : GHOST_SOMMERFELD;
     const bool all = slot == 0;
-    const GhostSrc* src = all ? X.d_src : X.d_src_stage;
-    const auto& ranges = all ? X.src_range : X.src_range_stage;
+    const GhostSrc* src = all ? (pushed ? X.d_src_nc : X.d_src) : (pushed ? X.d_src_stage_nc : X.d_src_stage);
+    const long long nsrc = all ? (pushed ? X.nsrc_nc : X.nsrc) : (pushed ? X.nsrc_stage_nc : X.nsrc_stage);
+    const auto& ranges = all ? (pushed ? X.src_range_nc : X.src_range) : (pushed ? X.src_range_stage_nc : X.src_range_stage);
     if (c->batched) {
+        if (nsrc == 0) return cudaSuccess;
         ++*n;
         return timed(c, GRANITE_KERNEL_GHOST, [&] {
-            return launch_ghost_sources(c->d_blocks, src, all ? X.nsrc : X.nsrc_stage, slot, local, c->stream);
+            return launch_ghost_sources(c->d_blocks, src, nsrc, slot, local, c->stream);
         });
     }
     for (const auto& r : ranges) {
+        if (r.second == 0) continue;
         ++*n;
         if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] {
                  return launch_ghost_sources(c->d_blocks, src + r.first, r.second, slot, local, c->stream);
@@ -1837,10 +1946,19 @@ cudaError_t fill_level(Ctx* c, int L, int slot, bool level_fill, int mode, long 
     return cudaSuccess;
 }
 
+// Whether the stage kernels of level L push the same-level ghost copies in mode.
+bool pushes(const Ctx* c, int L, int mode) {
+    return mode == GRANITE_AMR_GHOSTS && c->ghost_push && c->xfer_built[mode] && c->xfer[mode][L].push_ok;
+}
+
 cudaError_t stage(Ctx* c, int L, int precision, int in, int out, double a1, double a2, double a3dt, int final_stage,
-                  long long* n) {
+                  long long* n, bool push = false) {
     LevelLists& ll = c->levels[L];
     StageArgs a = base_args(c);
+    if (push) {
+        a.push = c->xfer[GRANITE_AMR_GHOSTS][L].d_push;
+        a.tile_push = c->xfer[GRANITE_AMR_GHOSTS][L].d_tile_push;
+    }
     a.in_sel = in;
     a.n_sel = 0;
     a.out_sel = out;
@@ -1888,13 +2006,15 @@ cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long lon
     } else {
         if ((e = fill_level(c, L, 0, true, mode, n))) return e;  // amr.cpp:319
     }
-    // TimeIntegrator::sspRK3Step, main.cpp:673-689
-    if ((e = stage(c, L, precision, 0, 1, 1.0, 0.0, 1.0 * dt, 0, n))) return e;
-    if ((e = fill_level(c, L, 1, false, mode, n))) return e;
-    if ((e = stage(c, L, precision, 1, 2, 0.75, 0.25, 0.25 * dt, 0, n))) return e;
-    if ((e = fill_level(c, L, 2, false, mode, n))) return e;
-    if ((e = stage(c, L, precision, 2, 0, 1.0 / 3.0, 2.0 / 3.0, (2.0 / 3.0) * dt, 1, n))) return e;
-    if ((e = fill_level(c, L, 0, true, mode, n))) return e;  // amr.cpp:329
+    // TimeIntegrator::sspRK3Step, main.cpp:673-689 (in GRANITE_AMR_GHOSTS the
+    // stages write the same-level ghost copies themselves; the fills add the rest)
+    const bool push = pushes(c, L, mode);
+    if ((e = stage(c, L, precision, 0, 1, 1.0, 0.0, 1.0 * dt, 0, n, push))) return e;
+    if ((e = fill_level(c, L, 1, false, mode, n, push))) return e;
+    if ((e = stage(c, L, precision, 1, 2, 0.75, 0.25, 0.25 * dt, 0, n, push))) return e;
+    if ((e = fill_level(c, L, 2, false, mode, n, push))) return e;
+    if ((e = stage(c, L, precision, 2, 0, 1.0 / 3.0, 2.0 / 3.0, (2.0 / 3.0) * dt, 1, n, push))) return e;
+    if ((e = fill_level(c, L, 0, true, mode, n, push))) return e;  // amr.cpp:329
     if (hook) c->level_time[L] += dt;                         // amr.cpp:326
     if (L + 1 < (int)c->levels.size()) {
         for (int r = 0; r < 2; ++r) {  // amr.cpp:334-336, :393-397

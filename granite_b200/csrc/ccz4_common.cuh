@@ -46,6 +46,17 @@ struct Tile {
                      // 128 threads cover w x 128/w points); 0 for fixed-shape kernels
 };
 
+// Interior cells of a source block that are ghost cells of a same-level
+// neighbour (GRANITE_AMR_GHOSTS): the stage kernel that writes such a cell
+// also writes it into the neighbour's ghost cell of the same buffer slot, so
+// the fill after the stage leaves those cells out. Source interior indices
+// [lo, hi) per axis; destination cell (incl. ghosts) = source index + off.
+struct PushBox {
+    int dst;
+    int lo[3], hi[3];
+    int off[3];
+};
+
 // Arguments of one fused RHS launch.
 struct StageArgs {
     int in_sel;      // buffer slot the stencils read
@@ -69,6 +80,10 @@ struct StageArgs {
     // test_withhold - 1, so its bounded wait for that item runs out (no copy is
     // in flight for it) and the launch reports through errflag.
     int test_withhold;
+    // Same-level ghost copies pushed from the RK epilogue (nullable): tile ti of
+    // the launch's list pushes push[tile_push[ti].x .. + tile_push[ti].y).
+    const PushBox* push;
+    const int2* tile_push;
 };
 
 __host__ __device__ inline long long cell_index(const DevBlock& b, int i, int j, int k) {

@@ -495,9 +495,29 @@ __device__ __forceinline__ void point_pm(const DevBlock& B, const double* __rest
 // u_in: the stage input at the point, from global memory, or (tin != nullptr)
 // from a per-thread column of shared memory that the stencil source filled with
 // each field's centre value, field v at tin[v * tin_stride].
+// The new state of interior point (i, j, k) of the tile ti's block into the
+// ghost cells of the same-level neighbours that hold it (A.push), slot
+// out_sel; the boxes are the tile's, the containment test is per point.
+__device__ __forceinline__ void push_copies(const DevBlock* blocks, const StageArgs& A, int ti, int i, int j, int k,
+                                            const double r[NV]) {
+    const int2 pr = A.tile_push[ti];
+    for (int q = pr.x; q < pr.x + pr.y; ++q) {
+        const PushBox P = A.push[q];
+        if (i < P.lo[0] || i >= P.hi[0] || j < P.lo[1] || j >= P.hi[1] || k < P.lo[2] || k >= P.hi[2]) continue;
+        const DevBlock& D = blocks[P.dst];
+        double* o = D.buf[A.out_sel] + cell_index(D, i + P.off[0], j + P.off[1], k + P.off[2]);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) o[(long long)v * D.stride] = r[v];
+    }
+}
+
+// blocks, ti, (i, j, k): the block table, the tile's index in the launch's list
+// and the point's interior indices, for the pushed ghost copies (A.push).
 template <int EPI, typename T>
 __device__ __forceinline__ void stage_epilogue(const DevBlock& B, const StageArgs& A, long long c, const T L[NV],
-                                               const double* tin = nullptr, int tin_stride = 0) {
+                                               const double* tin = nullptr, int tin_stride = 0,
+                                               const DevBlock* blocks = nullptr, int ti = 0, int i = 0, int j = 0,
+                                               int k = 0) {
     const long long st = B.stride;
     if (EPI == EPI_STORE) {
 #pragma unroll
@@ -546,6 +566,7 @@ __device__ __forceinline__ void stage_epilogue(const DevBlock& B, const StageArg
     if (A.final_stage) algebraic_constraints(r);
 #pragma unroll
     for (int v = 0; v < NV; ++v) out[(long long)v * st + c] = r[v];
+    if (A.push && blocks) push_copies(blocks, A, ti, i, j, k, r);
 }
 
 }  // namespace granite_b200

@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         }
         AlgebraT<PM> L[NV];
         point_pm<PM>(B, uin, c, A, S, L);
-        if (valid) stage_epilogue<EPI>(B, A, c, L, tin, C::NT);
+        if (valid) stage_epilogue<EPI>(B, A, c, L, tin, C::NT, blocks, ti, i, j, k);
     }
     // Every issued item was consumed (issue() skips items past this CTA's last
     // tile), so no copy into the ring is in flight when the CTA exits. If

@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(C::NTHR, C::MINB)
         }
         P L[NV];
         ccz4_point<P, false>(B, uin, c, A, S, L);
-        if (valid) stage_epilogue<EPI>(B, A, c, L);
+        if (valid) stage_epilogue<EPI>(B, A, c, L, nullptr, 0, blocks, ti, i, j, k);
     }
 }
 

@@ -436,6 +436,14 @@ GRANITE_API int granite_ccz4_test_withhold_tile_load(void* ctx, int item);
 GRANITE_API int granite_ccz4_set_fp64_chi_threshold(void* ctx, double chi_fp64);
 GRANITE_API int granite_ccz4_get_fp64_chi_threshold(const void* ctx, double* chi_fp64);
 
+/* Same-level ghost copies in GRANITE_AMR_GHOSTS (no counterpart in the
+ * reference): with 1 (the default) the stage kernels write every interior
+ * value a same-level neighbour holds as a ghost cell into that ghost cell of
+ * the same buffer, and the fills after the stages only prolongate and apply
+ * the block-local fills; 0 = the fills copy them (the same values: results are
+ * identical). Levels whose interiors overlap (after a regrid) always copy. */
+GRANITE_API int granite_ccz4_set_ghost_push(void* ctx, int on);
+
 /* Batching (no counterpart in the reference): 1 (default) = one launch per
  * level and RK stage over all blocks, each step replayed as one CUDA graph;
  * 0 = one launch per block and stage, issued eagerly, as a per-block drop-in

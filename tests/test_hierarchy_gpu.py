@@ -184,3 +184,33 @@ def test_finest_prefill_skip_is_exact(gb, oracle_lib, precision):
         ev.close()
     for a, b in zip(*outs):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision,chi", [(0, 0.0), (1, 0.0), (1, 0.5)])
+def test_ghost_push_equals_copy_fills(gb, oracle_lib, precision, chi):
+    # GRANITE_AMR_GHOSTS: the stage kernels write the same-level ghost copies
+    # themselves (both passes of the per-tile precision included) and the fills
+    # after them leave the copies out; the result equals the run whose fills copy
+    # every same-level ghost cell, bit for bit
+    # blocks of 16 to 32 cells, so that every level runs the TMA stage kernel
+    from granite_b200.hierarchy import make_binary_hierarchy
+    h = make_binary_hierarchy(seed=21, levels=3, coarse_n=48, extent=16.0, sizes=(16, 24, 32),
+                              blocks_per_level=(8, 40))
+    geoms = [Geom(b.ncells, b.lo, b.hi) for b in h.blocks]
+    levels = [b.level for b in h.blocks]
+    states = [oracle.add_noise(oracle_lib.init_brill_lindquist(g, h.masses, h.positions, r_floor=0.5 * g.dx[0]),
+                               1e-10, 60 + i) for i, g in enumerate(geoms)]
+    dt = 0.25 * geoms[0].dx[0]
+    outs = []
+    for push in (True, False):
+        ev, blocks = gpu_hierarchy(gb, geoms, levels, states, gb.VARIANT_TMA)
+        ev.set_ghost_push(push)
+        if chi > 0.0:
+            ev.set_fp64_chi_threshold(chi)
+        for _ in range(2):
+            ev.hierarchy_step(dt, precision, gb.AMR_GHOSTS)
+        ev.download()
+        outs.append([b.array.copy() for b in blocks])
+        ev.close()
+    for i, (a, b) in enumerate(zip(*outs)):
+        assert np.array_equal(a, b), f"block {i} level {levels[i]}: pushed ghost copies differ from copied ones"
