@@ -118,11 +118,17 @@ struct XferList {
     BoxChunk* d_chunks = nullptr;
     int nchunks = 0;
     int nboxes = 0;
+    // restriction into a level whose same-level ghost copies are pushed: per
+    // box, the range of push boxes of its destination block that meet it
+    PushBox* d_push = nullptr;
+    int2* d_box_push = nullptr;
 };
 
 void free_xfer(XferList& x) {
     cudaFree(x.d_boxes);
     cudaFree(x.d_chunks);
+    cudaFree(x.d_push);
+    cudaFree(x.d_box_push);
     x = XferList();
 }
 
@@ -145,6 +151,7 @@ struct LevelXfer {
     // push boxes, per stage tile its range of them, and the ghost sources
     // without the copies for the fills that follow a pushing stage
     bool push_ok = false;
+    std::map<int, std::vector<PushBox>> push_by_src;  // host: the push boxes of each source block
     PushBox* d_push = nullptr;
     int2* d_tile_push = nullptr;
     GhostSrc* d_src_nc = nullptr;
@@ -189,12 +196,23 @@ struct Ctx {
     long long matter_cells = 0;
     double fp64_chi = 0.0;         // MIXED: tiles with a point of chi below this run the FP64 algebra
     cudaStream_t stream = nullptr;
+    // second stream of the per-tile precision: the FP64 pass runs beside the
+    // FP32 pass (disjoint tiles), forked from and joined back to `stream`
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string err;
     long long launches = 0;
     unsigned long long* d_nonfinite = nullptr;
     unsigned int* d_errflag = nullptr;   // set by a TMA stage kernel whose bounded wait gave up
     int test_withhold = 0;               // armed test switch (StageArgs::test_withhold) of the next rk3_step
     bool ghost_push = true;              // GRANITE_AMR_GHOSTS: stage kernels push same-level ghost copies
+    // every pushing level's same-level ghost copies of slot 0 equal their
+    // sources (after a GRANITE_AMR_GHOSTS coarse step with pushes; cleared by
+    // anything else that writes the state), and, while a coarse step is being
+    // enqueued, the levels that have pushed in it: their fills before a step
+    // need no copies
+    bool copies_valid = false;
+    std::vector<char> step_pushed;
     unsigned long long* d_cmp = nullptr; // granite_ccz4_compare_states results (46 words)
     CUtensorMap* d_tmaps = nullptr;      // TMA variant: per box shape, 3 maps per resident block (slots 0-2)
     CUtensorMap* s_tmap = nullptr;       // TMA variant: map of the stateless single-block input
@@ -644,6 +662,9 @@ int granite_ccz4_create(const granite_ccz4_params* p, void** out) {
     cudaError_t e = cudaSetDevice(c->device);
     if (e == cudaSuccess) e = configure_stage_kernels();
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_nonfinite, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(c->d_nonfinite, 0, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&c->d_errflag, sizeof(unsigned int));
@@ -687,6 +708,9 @@ int granite_ccz4_destroy(void* h) {
     cudaFree(c->d_cmp);
     cudaFree(c->s_tmap);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream2) cudaStreamDestroy(c->stream2);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     delete c;
     return GRANITE_OK;
 }
@@ -716,6 +740,7 @@ int granite_ccz4_set_ghost_push(void* h, int on) {
     Ctx* c = static_cast<Ctx*>(h);
     if (!c) return GRANITE_ERR_INVALID;
     c->ghost_push = on != 0;
+    c->copies_valid = false;
     for (auto& kv : c->hgraphs)  // captured steps bake the choice in
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     c->hgraphs.clear();
@@ -1186,6 +1211,8 @@ int granite_ccz4_regrid_add(void* h, const granite_block_desc* b, int n) {
     if (!c->committed) return fail(c, GRANITE_ERR_INVALID, "commit before regrid");
     if (n < 0 || (n > 0 && !b)) return fail(c, GRANITE_ERR_INVALID, "bad block list");
     if (n == 0) return GRANITE_OK;
+    c->copies_valid = false;  // new blocks: their neighbours' ghost copies are not current
+    c->step_pushed.clear();
     std::vector<granite_block_desc> descs = c->descs;
     std::vector<int> count(64, 0);
     for (const auto& d : descs) ++count[d.level];
@@ -1282,6 +1309,7 @@ int granite_ccz4_upload_block(void* h, int i, const double* host) {
                        cudaMemcpyHostToDevice, c->stream),
        "H2D block");
     c->level_ghosts_valid[c->descs[i].level] = false;
+    c->copies_valid = false;  // the state changed outside a pushing coarse step
     return GRANITE_OK;
 }
 
@@ -1298,6 +1326,7 @@ int granite_ccz4_upload_all(void* h, const double* const* hosts) {
                            cudaMemcpyHostToDevice, c->stream),
            "H2D block");
     for (size_t L = 0; L < c->level_ghosts_valid.size(); ++L) c->level_ghosts_valid[L] = false;
+    c->copies_valid = false;  // the state changed outside a pushing coarse step
     return GRANITE_OK;
 }
 
@@ -1361,11 +1390,24 @@ static cudaError_t stage_range(Ctx* c, LevelLists& L, int cfg, int precision, co
     if (e != cudaSuccess) return e;
     StageArgs b = a;
     b.tile_prec = flags;
-    b.want_prec = 0;
-    if ((e = launch_stage(L.variant, cfg, PM_MIXED, EPI_RK, c->d_blocks, tiles, count, b, c->stream))) return e;
-    b.want_prec = 1;
     *n += 3;
-    return launch_stage(L.variant, cfg, PM_FP64F, EPI_RK, c->d_blocks, tiles, count, b, c->stream);
+    // The two passes write disjoint tiles: the FP64 pass (few tiles, few CTAs
+    // with work) runs on the second stream beside the FP32 pass and fills the
+    // SMs its tail leaves idle. Under the profiler (every launch bracketed by
+    // events on the main stream) they run one after the other.
+    StageArgs b64 = b;
+    b64.want_prec = 1;
+    b.want_prec = 0;
+    if (c->profiling) {
+        if ((e = launch_stage(L.variant, cfg, PM_MIXED, EPI_RK, c->d_blocks, tiles, count, b, c->stream))) return e;
+        return launch_stage(L.variant, cfg, PM_FP64F, EPI_RK, c->d_blocks, tiles, count, b64, c->stream);
+    }
+    if ((e = cudaEventRecord(c->ev_fork, c->stream))) return e;
+    if ((e = cudaStreamWaitEvent(c->stream2, c->ev_fork, 0))) return e;
+    if ((e = launch_stage(L.variant, cfg, PM_FP64F, EPI_RK, c->d_blocks, tiles, count, b64, c->stream2))) return e;
+    if ((e = launch_stage(L.variant, cfg, PM_MIXED, EPI_RK, c->d_blocks, tiles, count, b, c->stream))) return e;
+    if ((e = cudaEventRecord(c->ev_join, c->stream2))) return e;
+    return cudaStreamWaitEvent(c->stream, c->ev_join, 0);
 }
 
 // The fused stage kernel over one level: the whole work-list at once, or
@@ -1454,6 +1496,7 @@ int granite_ccz4_rk3_step(void* h, int level, double dt, int precision, int bc) 
     if (bc != GRANITE_BC_REFERENCE && bc != GRANITE_BC_PERIODIC) return fail(c, GRANITE_ERR_INVALID, "bad bc");
     if (!std::isfinite(dt)) return fail(c, GRANITE_ERR_INVALID, "dt must be finite");
     CK(cudaSetDevice(c->device), "cudaSetDevice");
+    c->copies_valid = false;  // a level step fills its ghosts block by block
     const bool prefill = !c->level_ghosts_valid[level];
     if (c->profiling || !c->batched || c->test_withhold) {  // (an armed test switch is never captured)
         long long nl = 0;
@@ -1722,7 +1765,8 @@ int build_ghosts_mode(Ctx* c) {
             LevelLists& ll = c->levels[L];
             X[L].push_ok = !ovl && ll.variant == VARIANT_TMA && !ll.h_tiles.empty();
             if (X[L].push_ok) {
-                std::map<int, std::vector<PushBox>> by_src;
+                std::map<int, std::vector<PushBox>>& by_src = X[L].push_by_src;
+                by_src.clear();
                 for (const XferBox& x : copies) {
                     PushBox pb{};
                     pb.dst = x.dst;
@@ -1801,7 +1845,34 @@ int build_ghosts_mode(Ctx* c) {
             }
         for (const auto& res : waves) {
             X[L - 1].restrict_.emplace_back();
-            CK(upload_xfer(res, X[L - 1].restrict_.back(), c->stream), "upload restriction boxes");
+            XferList& rl = X[L - 1].restrict_.back();
+            CK(upload_xfer(res, rl, c->stream), "upload restriction boxes");
+            // the restricted coarse cells that same-level neighbours of level L-1
+            // hold as ghost cells: the restriction writes them there too
+            if (X[L - 1].push_ok && !res.empty()) {
+                std::vector<PushBox> rp;
+                std::vector<int2> bp;
+                for (const XferBox& x : res) {
+                    const int first = (int)rp.size();
+                    auto it = X[L - 1].push_by_src.find(x.dst);
+                    if (it != X[L - 1].push_by_src.end())
+                        for (const PushBox& pb : it->second) {
+                            bool hit = true;
+                            for (int d = 0; d < 3 && hit; ++d) {
+                                const int lo = x.d0[d] - NG, hi = lo + x.n[d];  // coarse interior indices
+                                hit = pb.lo[d] < hi && pb.hi[d] > lo;
+                            }
+                            if (hit) rp.push_back(pb);
+                        }
+                    bp.push_back(make_int2(first, (int)rp.size() - first));
+                }
+                CK(upload_vec(rp, &rl.d_push, c->stream), "upload restriction push boxes");
+                CK(upload_vec(bp, &rl.d_box_push, c->stream), "upload restriction push ranges");
+                if (!rl.d_push) {
+                    cudaFree(rl.d_box_push);
+                    rl.d_box_push = nullptr;
+                }
+            }
         }
     }
     c->xfer_built[GRANITE_AMR_GHOSTS] = true;
@@ -1893,10 +1964,12 @@ int build_reference_mode(Ctx* c) {
     return GRANITE_OK;
 }
 
-cudaError_t xfer(Ctx* c, int kind, const XferList& x, int dst_sel, int src_sel) {
+cudaError_t xfer(Ctx* c, int kind, const XferList& x, int dst_sel, int src_sel, bool push = false) {
     if (x.nchunks == 0) return cudaSuccess;
+    const PushBox* pb = push ? x.d_push : nullptr;
+    const int2* bp = push ? x.d_box_push : nullptr;
     return timed(c, GRANITE_KERNEL_TRANSFER, [&] {
-        return launch_xfer(kind, c->d_blocks, x.d_boxes, x.d_chunks, x.nchunks, dst_sel, src_sel, c->stream);
+        return launch_xfer(kind, c->d_blocks, x.d_boxes, x.d_chunks, x.nchunks, dst_sel, src_sel, c->stream, pb, bp);
     });
 }
 
@@ -2004,7 +2077,11 @@ cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long lon
         ++*n;
         if ((e = level_ghost(c, c->levels[L], GHOST_ZERO_GRADIENT_MASKED, 0, X.d_facemask, n))) return e;
     } else {
-        if ((e = fill_level(c, L, 0, true, mode, n))) return e;  // amr.cpp:319
+        // amr.cpp:319; the same-level copies are current where this level's
+        // stages and the restrictions into it have pushed them
+        const bool fresh = pushes(c, L, mode) && (c->copies_valid || (L < (int)c->step_pushed.size() &&
+                                                                      c->step_pushed[L]));
+        if ((e = fill_level(c, L, 0, true, mode, n, fresh))) return e;
     }
     // TimeIntegrator::sspRK3Step, main.cpp:673-689 (in GRANITE_AMR_GHOSTS the
     // stages write the same-level ghost copies themselves; the fills add the rest)
@@ -2015,6 +2092,7 @@ cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long lon
     if ((e = fill_level(c, L, 2, false, mode, n, push))) return e;
     if ((e = stage(c, L, precision, 2, 0, 1.0 / 3.0, 2.0 / 3.0, (2.0 / 3.0) * dt, 1, n, push))) return e;
     if ((e = fill_level(c, L, 0, true, mode, n, push))) return e;  // amr.cpp:329
+    if (push && L < (int)c->step_pushed.size()) c->step_pushed[L] = 1;
     if (hook) c->level_time[L] += dt;                         // amr.cpp:326
     if (L + 1 < (int)c->levels.size()) {
         for (int r = 0; r < 2; ++r) {  // amr.cpp:334-336, :393-397
@@ -2023,8 +2101,9 @@ cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long lon
             if ((e = subcycle(c, L + 1, dt / 2.0, precision, mode, n, hook, skip))) return e;
         }
         if (hook && (hook->status = ensure_xfer(c, mode))) return cudaErrorInvalidValue;  // a regrid rebuilt them
+        const bool rpush = pushes(c, L, mode);
         for (const XferList& rl : c->xfer[mode][L].restrict_) {                            // amr.cpp:339-341
-            if ((e = xfer(c, XFER_RESTRICT, rl, 0, 0))) return e;
+            if ((e = xfer(c, XFER_RESTRICT, rl, 0, 0, rpush))) return e;
             ++*n;
         }
     }
@@ -2070,17 +2149,24 @@ int granite_ccz4_hierarchy_step(void* h, double dt_coarse, int precision, int am
     int r = check_hierarchy_step(c, dt_coarse, precision, amr_mode);
     if (r) return r;
     for (size_t L = 0; L < c->level_ghosts_valid.size(); ++L) c->level_ghosts_valid[L] = false;
+    const bool valid_at_start = c->copies_valid && amr_mode == GRANITE_AMR_GHOSTS;
+    c->step_pushed.assign(c->levels.size(), 0);
+    auto finish = [&]() {  // after a coarse step in GRANITE_AMR_GHOSTS with pushes, every copy is current
+        c->copies_valid = amr_mode == GRANITE_AMR_GHOSTS && c->ghost_push;
+        c->step_pushed.clear();
+    };
     if (c->profiling || !c->batched) {
         long long n = 0;
         cudaError_t e = subcycle(c, 0, dt_coarse, precision, amr_mode, &n);
         if (e != cudaSuccess) return cuda_fail(c, e, "hierarchy step");
         c->launches += n;
         advance_level_times(c, dt_coarse);
+        finish();
         return GRANITE_OK;
     }
     unsigned long long dtbits;
     std::memcpy(&dtbits, &dt_coarse, sizeof(dt_coarse));
-    auto key = std::make_tuple(precision, amr_mode, dtbits);
+    auto key = std::make_tuple(precision, amr_mode + (valid_at_start ? 2 : 0), dtbits);
     auto it = c->hgraphs.find(key);
     if (it == c->hgraphs.end()) {
         Graph g;
@@ -2100,6 +2186,7 @@ int granite_ccz4_hierarchy_step(void* h, double dt_coarse, int precision, int am
     CK(cudaGraphLaunch(it->second.exec, c->stream), "graph launch");
     c->launches += it->second.launches;
     advance_level_times(c, dt_coarse);
+    finish();
     return GRANITE_OK;
 }
 
@@ -2112,6 +2199,7 @@ int granite_ccz4_hierarchy_step_regrid(void* h, double dt_coarse, int precision,
     int r = check_hierarchy_step(c, dt_coarse, precision, amr_mode);
     if (r) return r;
     for (size_t L = 0; L < c->level_ghosts_valid.size(); ++L) c->level_ghosts_valid[L] = false;
+    c->copies_valid = false;  // the state changed outside a pushing coarse step
     RegridHook hook{regrid_interval, fn, user, 0};
     long long n = 0;
     cudaError_t e = subcycle(c, 0, dt_coarse, precision, amr_mode, &n, &hook);
@@ -2373,6 +2461,7 @@ int granite_ccz4_checkpoint_read(void* hc, const char* path, int* step, double* 
         return r;
     c->level_time = lt;
     for (size_t L = 0; L < c->level_ghosts_valid.size(); ++L) c->level_ghosts_valid[L] = false;
+    c->copies_valid = false;  // the state changed outside a pushing coarse step
     if (step) *step = h.step;
     if (time) *time = h.time;
     return GRANITE_OK;

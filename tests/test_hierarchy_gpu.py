@@ -188,10 +188,10 @@ def test_finest_prefill_skip_is_exact(gb, oracle_lib, precision):
 
 @pytest.mark.parametrize("precision,chi", [(0, 0.0), (1, 0.0), (1, 0.5)])
 def test_ghost_push_equals_copy_fills(gb, oracle_lib, precision, chi):
-    # GRANITE_AMR_GHOSTS: the stage kernels write the same-level ghost copies
-    # themselves (both passes of the per-tile precision included) and the fills
-    # after them leave the copies out; the result equals the run whose fills copy
-    # every same-level ghost cell, bit for bit
+    # GRANITE_AMR_GHOSTS: the stage kernels and the restrictions write the
+    # same-level ghost copies themselves (both passes of the per-tile precision
+    # included) and the fills leave the copies out; the result equals the run
+    # whose fills copy every same-level ghost cell, bit for bit
     # blocks of 16 to 32 cells, so that every level runs the TMA stage kernel
     from granite_b200.hierarchy import make_binary_hierarchy
     h = make_binary_hierarchy(seed=21, levels=3, coarse_n=48, extent=16.0, sizes=(16, 24, 32),
@@ -207,10 +207,17 @@ def test_ghost_push_equals_copy_fills(gb, oracle_lib, precision, chi):
         ev.set_ghost_push(push)
         if chi > 0.0:
             ev.set_fp64_chi_threshold(chi)
-        for _ in range(2):
+        for _ in range(3):  # the second and third steps fill before each level step without copies
             ev.hierarchy_step(dt, precision, gb.AMR_GHOSTS)
         ev.download()
-        outs.append([b.array.copy() for b in blocks])
+        res = [b.array.copy() for b in blocks]
+        # an upload invalidates the pushed copies: the next step fills them again
+        for b, u in zip(blocks, states):
+            b.array[...] = u
+        ev.upload()
+        ev.hierarchy_step(dt, precision, gb.AMR_GHOSTS)
+        ev.download()
+        outs.append(res + [b.array.copy() for b in blocks])
         ev.close()
     for i, (a, b) in enumerate(zip(*outs)):
-        assert np.array_equal(a, b), f"block {i} level {levels[i]}: pushed ghost copies differ from copied ones"
+        assert np.array_equal(a, b), f"array {i}: pushed ghost copies differ from copied ones"
