@@ -118,17 +118,11 @@ struct XferList {
     BoxChunk* d_chunks = nullptr;
     int nchunks = 0;
     int nboxes = 0;
-    // restriction into a level whose same-level ghost copies are pushed: per
-    // box, the range of push boxes of its destination block that meet it
-    PushBox* d_push = nullptr;
-    int2* d_box_push = nullptr;
 };
 
 void free_xfer(XferList& x) {
     cudaFree(x.d_boxes);
     cudaFree(x.d_chunks);
-    cudaFree(x.d_push);
-    cudaFree(x.d_box_push);
     x = XferList();
 }
 
@@ -160,6 +154,11 @@ struct LevelXfer {
     GhostSrc* d_src_stage_nc = nullptr;
     long long nsrc_stage_nc = 0;
     std::vector<std::pair<long long, long long>> src_range_stage_nc;
+    // the fill before a step while the pushed copies are current: no copies but
+    // those of cells a restriction into the level writes
+    GhostSrc* d_src_pre = nullptr;
+    long long nsrc_pre = 0;
+    std::vector<std::pair<long long, long long>> src_range_pre;
 };
 
 // device copy of a host vector (nullptr for an empty one)
@@ -1052,6 +1051,7 @@ static void release_lists(Ctx* c) {
             cudaFree(X.d_tile_push);
             cudaFree(X.d_src_nc);
             cudaFree(X.d_src_stage_nc);
+            cudaFree(X.d_src_pre);
         }
         c->xfer[m].clear();
         c->xfer_built[m] = false;
@@ -1605,6 +1605,8 @@ int build_ghosts_mode(Ctx* c) {
     if (r) return r;
     auto& X = c->xfer[GRANITE_AMR_GHOSTS];
     X.assign(c->levels.size(), LevelXfer());
+    std::vector<std::vector<GhostSrc>> full_src(c->levels.size());    // host copies of the ghost sources
+    std::vector<std::vector<XferBox>> restricted(c->levels.size());   // restriction boxes into each level
     for (size_t L = 0; L < c->levels.size(); ++L) {
         const auto& blocks = c->levels[L].blocks;
         // same-level copies
@@ -1725,6 +1727,7 @@ int build_ghosts_mode(Ctx* c) {
             }
             CK(upload_vec(items, &X[L].d_src, c->stream), "upload ghost sources");
             X[L].nsrc = (long long)items.size();
+            full_src[L] = items;
             CK(upload_vec(sitems, &X[L].d_src_stage, c->stream), "upload stage ghost sources");
             X[L].nsrc_stage = (long long)sitems.size();
             // the same lists without the same-level copies (for the fills after a pushing stage)
@@ -1845,35 +1848,42 @@ int build_ghosts_mode(Ctx* c) {
             }
         for (const auto& res : waves) {
             X[L - 1].restrict_.emplace_back();
-            XferList& rl = X[L - 1].restrict_.back();
-            CK(upload_xfer(res, rl, c->stream), "upload restriction boxes");
-            // the restricted coarse cells that same-level neighbours of level L-1
-            // hold as ghost cells: the restriction writes them there too
-            if (X[L - 1].push_ok && !res.empty()) {
-                std::vector<PushBox> rp;
-                std::vector<int2> bp;
-                for (const XferBox& x : res) {
-                    const int first = (int)rp.size();
-                    auto it = X[L - 1].push_by_src.find(x.dst);
-                    if (it != X[L - 1].push_by_src.end())
-                        for (const PushBox& pb : it->second) {
-                            bool hit = true;
-                            for (int d = 0; d < 3 && hit; ++d) {
-                                const int lo = x.d0[d] - NG, hi = lo + x.n[d];  // coarse interior indices
-                                hit = pb.lo[d] < hi && pb.hi[d] > lo;
-                            }
-                            if (hit) rp.push_back(pb);
-                        }
-                    bp.push_back(make_int2(first, (int)rp.size() - first));
-                }
-                CK(upload_vec(rp, &rl.d_push, c->stream), "upload restriction push boxes");
-                CK(upload_vec(bp, &rl.d_box_push, c->stream), "upload restriction push ranges");
-                if (!rl.d_push) {
-                    cudaFree(rl.d_box_push);
-                    rl.d_box_push = nullptr;
-                }
-            }
+            CK(upload_xfer(res, X[L - 1].restrict_.back(), c->stream), "upload restriction boxes");
+            for (const XferBox& x : res) restricted[L - 1].push_back(x);
         }
+    }
+    // The fill before a level step when the pushed copies are current: the
+    // same-level copies whose source cell a restriction into the level can have
+    // changed since the stage that pushed it, and every non-copy ghost cell.
+    // (The restriction itself does not push: like the reference, it leaves the
+    // neighbours' copies of the cells it writes stale until this fill.)
+    for (size_t L = 0; L < c->levels.size(); ++L) {
+        if (!X[L].push_ok) continue;
+        std::map<int, std::vector<char>> mask;  // per block of the level: cells some restriction writes
+        for (const XferBox& x : restricted[L]) {
+            const auto& d = c->descs[x.dst];
+            const int T0 = d.ncells[0] + 2 * NG, T1 = d.ncells[1] + 2 * NG, T2 = d.ncells[2] + 2 * NG;
+            auto& m = mask[x.dst];
+            if (m.empty()) m.assign((size_t)T0 * T1 * T2, 0);
+            for (int k = 0; k < x.n[2]; ++k)
+                for (int j = 0; j < x.n[1]; ++j)
+                    for (int i = 0; i < x.n[0]; ++i)
+                        m[(size_t)(x.d0[0] + i) + (size_t)T0 * ((x.d0[1] + j) + (size_t)T1 * (x.d0[2] + k))] = 1;
+        }
+        std::vector<GhostSrc> pre;
+        X[L].src_range_pre.clear();
+        for (const auto& r : X[L].src_range) {
+            const long long f = (long long)pre.size();
+            for (long long q = r.first; q < r.first + r.second; ++q) {
+                const GhostSrc& g = full_src[L][q];
+                const bool copy = g.src_block >= 0 && g.src_cell >= 0;
+                auto it = copy ? mask.find(g.src_block) : mask.end();
+                if (!copy || (it != mask.end() && it->second[g.src_cell])) pre.push_back(g);
+            }
+            X[L].src_range_pre.push_back({f, (long long)pre.size() - f});
+        }
+        CK(upload_vec(pre, &X[L].d_src_pre, c->stream), "upload prefill ghost sources");
+        X[L].nsrc_pre = (long long)pre.size();
     }
     c->xfer_built[GRANITE_AMR_GHOSTS] = true;
     return GRANITE_OK;
@@ -1964,18 +1974,20 @@ int build_reference_mode(Ctx* c) {
     return GRANITE_OK;
 }
 
-cudaError_t xfer(Ctx* c, int kind, const XferList& x, int dst_sel, int src_sel, bool push = false) {
+cudaError_t xfer(Ctx* c, int kind, const XferList& x, int dst_sel, int src_sel) {
     if (x.nchunks == 0) return cudaSuccess;
-    const PushBox* pb = push ? x.d_push : nullptr;
-    const int2* bp = push ? x.d_box_push : nullptr;
     return timed(c, GRANITE_KERNEL_TRANSFER, [&] {
-        return launch_xfer(kind, c->d_blocks, x.d_boxes, x.d_chunks, x.nchunks, dst_sel, src_sel, c->stream, pb, bp);
+        return launch_xfer(kind, c->d_blocks, x.d_boxes, x.d_chunks, x.nchunks, dst_sel, src_sel, c->stream);
     });
 }
 
 // Ghost fill of one level's buffer slot. level_fill: the fill around a step
 // (zero-gradient base); otherwise a stage fill (1/r falloff base).
-cudaError_t fill_level(Ctx* c, int L, int slot, bool level_fill, int mode, long long* n, bool pushed = false) {
+// pushed: the fill after a stage that pushed the same-level copies (no copies);
+// prefill_fresh: the fill before a step while the pushed copies are current
+// (only the copies of cells restrictions write).
+cudaError_t fill_level(Ctx* c, int L, int slot, bool level_fill, int mode, long long* n, bool pushed = false,
+                       bool prefill_fresh = false) {
     LevelLists& ll = c->levels[L];
     const LevelXfer& X = c->xfer[mode][L];
     cudaError_t e;
@@ -1998,9 +2010,12 @@ cudaError_t fill_level(Ctx* c, int L, int slot, bool level_fill, int mode, long 
     // after a stage that pushed the same-level copies, the lists without them
     const int local = level_fill ? GHOST_ZERO_GRADIENT : GHOST_SOMMERFELD;
     const bool all = slot == 0;
-    const GhostSrc* src = all ? (pushed ? X.d_src_nc : X.d_src) : (pushed ? X.d_src_stage_nc : X.d_src_stage);
-    const long long nsrc = all ? (pushed ? X.nsrc_nc : X.nsrc) : (pushed ? X.nsrc_stage_nc : X.nsrc_stage);
-    const auto& ranges = all ? (pushed ? X.src_range_nc : X.src_range) : (pushed ? X.src_range_stage_nc : X.src_range_stage);
+    const GhostSrc* src = all ? (prefill_fresh ? X.d_src_pre : pushed ? X.d_src_nc : X.d_src)
+                              : (pushed ? X.d_src_stage_nc : X.d_src_stage);
+    const long long nsrc = all ? (prefill_fresh ? X.nsrc_pre : pushed ? X.nsrc_nc : X.nsrc)
+                               : (pushed ? X.nsrc_stage_nc : X.nsrc_stage);
+    const auto& ranges = all ? (prefill_fresh ? X.src_range_pre : pushed ? X.src_range_nc : X.src_range)
+                             : (pushed ? X.src_range_stage_nc : X.src_range_stage);
     if (c->batched) {
         if (nsrc == 0) return cudaSuccess;
         ++*n;
@@ -2077,11 +2092,11 @@ cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long lon
         ++*n;
         if ((e = level_ghost(c, c->levels[L], GHOST_ZERO_GRADIENT_MASKED, 0, X.d_facemask, n))) return e;
     } else {
-        // amr.cpp:319; the same-level copies are current where this level's
-        // stages and the restrictions into it have pushed them
+        // amr.cpp:319; once this level's stages have pushed its same-level
+        // copies, only those whose source a restriction rewrote are stale
         const bool fresh = pushes(c, L, mode) && (c->copies_valid || (L < (int)c->step_pushed.size() &&
                                                                       c->step_pushed[L]));
-        if ((e = fill_level(c, L, 0, true, mode, n, fresh))) return e;
+        if ((e = fill_level(c, L, 0, true, mode, n, false, fresh))) return e;
     }
     // TimeIntegrator::sspRK3Step, main.cpp:673-689 (in GRANITE_AMR_GHOSTS the
     // stages write the same-level ghost copies themselves; the fills add the rest)
@@ -2101,9 +2116,8 @@ cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long lon
             if ((e = subcycle(c, L + 1, dt / 2.0, precision, mode, n, hook, skip))) return e;
         }
         if (hook && (hook->status = ensure_xfer(c, mode))) return cudaErrorInvalidValue;  // a regrid rebuilt them
-        const bool rpush = pushes(c, L, mode);
         for (const XferList& rl : c->xfer[mode][L].restrict_) {                            // amr.cpp:339-341
-            if ((e = xfer(c, XFER_RESTRICT, rl, 0, 0, rpush))) return e;
+            if ((e = xfer(c, XFER_RESTRICT, rl, 0, 0))) return e;
             ++*n;
         }
     }

@@ -208,8 +208,7 @@ __device__ void prolong_cell(const DevBlock& F, const DevBlock& C, int i, int j,
 }
 
 __global__ void xfer_kernel(int kind, const DevBlock* __restrict__ blocks, const XferBox* __restrict__ boxes,
-                            const BoxChunk* __restrict__ chunks, int dst_sel, int src_sel,
-                            const PushBox* __restrict__ push, const int2* __restrict__ box_push) {
+                            const BoxChunk* __restrict__ chunks, int dst_sel, int src_sel) {
     const BoxChunk ch = chunks[blockIdx.x];
     const XferBox bx = boxes[ch.box];
     const int r = ch.start + threadIdx.x;
@@ -240,19 +239,6 @@ __global__ void xfer_kernel(int kind, const DevBlock* __restrict__ blocks, const
             for (int rj = 0; rj < 2; ++rj)
                 for (int ri = 0; ri < 2; ++ri) s = __dadd_rn(s, __ldg(q + ri * sx + rj * sy + rk * sz));
         db[(long long)v * D.stride + dc] = __ddiv_rn(s, 8.0);
-    }
-    if (push) {
-        // the same values into the same-level neighbours that hold this cell as a ghost
-        const int2 pr = box_push[ch.box];
-        const int ii = i - NG, jj = j - NG, kk = k - NG;
-        for (int q = pr.x; q < pr.x + pr.y; ++q) {
-            const PushBox P = push[q];
-            if (ii < P.lo[0] || ii >= P.hi[0] || jj < P.lo[1] || jj >= P.hi[1] || kk < P.lo[2] || kk >= P.hi[2])
-                continue;
-            const DevBlock& T = blocks[P.dst];
-            double* o = T.buf[dst_sel] + cell_index(T, ii + P.off[0], jj + P.off[1], kk + P.off[2]);
-            for (int v = 0; v < NV; ++v) o[(long long)v * T.stride] = db[(long long)v * D.stride + dc];
-        }
     }
 }
 
@@ -334,10 +320,9 @@ cudaError_t launch_ghost_fill(int mode, const DevBlock* blocks, const GhostItem*
 }
 
 cudaError_t launch_xfer(int kind, const DevBlock* blocks, const XferBox* boxes, const BoxChunk* chunks, int nchunks,
-                        int dst_sel, int src_sel, cudaStream_t stream, const PushBox* push, const int2* box_push) {
+                        int dst_sel, int src_sel, cudaStream_t stream) {
     if (nchunks <= 0) return cudaSuccess;
-    if ((push == nullptr) != (box_push == nullptr) || (push && kind != XFER_RESTRICT)) return cudaErrorInvalidValue;
-    xfer_kernel<<<nchunks, XFER_CHUNK, 0, stream>>>(kind, blocks, boxes, chunks, dst_sel, src_sel, push, box_push);
+    xfer_kernel<<<nchunks, XFER_CHUNK, 0, stream>>>(kind, blocks, boxes, chunks, dst_sel, src_sel);
     return cudaGetLastError();
 }
 

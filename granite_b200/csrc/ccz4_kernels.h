@@ -125,12 +125,8 @@ constexpr int XFER_CHUNK = 256;
 enum XferKind { XFER_COPY = 0, XFER_PROLONG = 1, XFER_RESTRICT = 2 };
 
 // Transfers of slot src_sel of the source blocks into slot dst_sel of the destinations.
-// Restriction with push / box_push set: every restricted cell is also written
-// into the same-level ghost cells of the destination block's push boxes (box b:
-// push[box_push[b].x .. + box_push[b].y)).
 cudaError_t launch_xfer(int kind, const DevBlock* blocks, const XferBox* boxes, const BoxChunk* chunks,
-                        int nchunks, int dst_sel, int src_sel, cudaStream_t stream, const PushBox* push = nullptr,
-                        const int2* box_push = nullptr);
+                        int nchunks, int dst_sel, int src_sel, cudaStream_t stream);
 
 // One ghost cell of a level and where its value comes from (GRANITE_AMR_GHOSTS):
 //   src_block >= 0, src_cell >= 0: copy of that cell of a same-level block
