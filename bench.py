@@ -510,6 +510,11 @@ def main():
                     help="wall-time cap of the accuracy run")
     ap.add_argument("--stage-config", type=int, default=-1,
                     help="one TMA stage-kernel configuration for every block (default: the per-class table)")
+    ap.add_argument("--ghost-push", type=int, default=-1, choices=[-1, 0, 1],
+                    help="GRANITE_AMR_GHOSTS: stage kernels write the same-level ghost copies (1) or the "
+                         "fills copy them (0); -1 = the library default")
+    ap.add_argument("--pass-overlap", type=int, default=-1, choices=[-1, 0, 1],
+                    help="per-tile precision: FP64 pass beside the FP32 pass (1) or after it (0); -1 = default")
     ap.add_argument("--no-amr-reference", action="store_true",
                     help="skip the GRANITE_AMR_REFERENCE hierarchy timing")
     args = ap.parse_args()
@@ -547,6 +552,10 @@ def main():
     run = Runner(gb, args.workload, w, prec, variant, local, args.stage_config)
     if prec == gb.PRECISION_MIXED and args.fp64_chi > 0.0:
         run.ev.set_fp64_chi_threshold(args.fp64_chi)
+    if args.ghost_push >= 0:
+        run.ev.set_ghost_push(bool(args.ghost_push))
+    if args.pass_overlap >= 0:
+        run.ev.set_pass_overlap(bool(args.pass_overlap))
     compare = None
     if prec == gb.PRECISION_MIXED and not args.no_compare:
         compare = Runner(gb, args.workload, w, gb.PRECISION_FP64, variant, local, args.stage_config)

@@ -154,6 +154,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_tag_count.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_longlong)]
     lib.granite_ccz4_test_withhold_tile_load.argtypes = [vp, C.c_int]
     lib.granite_ccz4_set_ghost_push.argtypes = [vp, C.c_int]
+    lib.granite_ccz4_set_pass_overlap.argtypes = [vp, C.c_int]
     ip_ = C.POINTER(C.c_int)
     lib.granite_ccz4_set_stage_config.argtypes = [vp, C.c_int, C.c_int, C.c_int]
     lib.granite_ccz4_get_stage_config.argtypes = [vp, C.c_int, C.c_int, ip_]
@@ -475,6 +476,10 @@ class Evolver:
     def set_ghost_push(self, on: bool):
         """GRANITE_AMR_GHOSTS: stage kernels write the same-level ghost copies (default) or the fills copy them."""
         self.ctx.check(self.ctx.lib.granite_ccz4_set_ghost_push(self.ctx.h, int(bool(on))))
+
+    def set_pass_overlap(self, on: bool):
+        """Per-tile precision: the FP64 pass beside the FP32 pass on a second stream (default) or after it."""
+        self.ctx.check(self.ctx.lib.granite_ccz4_set_pass_overlap(self.ctx.h, int(bool(on))))
 
     def set_batching(self, batched: bool):
         self.ctx.check(self.ctx.lib.granite_ccz4_set_batching(self.ctx.h, int(bool(batched))))

@@ -205,6 +205,7 @@ struct Ctx {
     unsigned int* d_errflag = nullptr;   // set by a TMA stage kernel whose bounded wait gave up
     int test_withhold = 0;               // armed test switch (StageArgs::test_withhold) of the next rk3_step
     bool ghost_push = true;              // GRANITE_AMR_GHOSTS: stage kernels push same-level ghost copies
+    bool overlap_passes = true;          // per-tile precision: FP64 pass beside the FP32 pass (second stream)
     // every pushing level's same-level ghost copies of slot 0 equal their
     // sources (after a GRANITE_AMR_GHOSTS coarse step with pushes; cleared by
     // anything else that writes the state), and, while a coarse step is being
@@ -732,6 +733,19 @@ static int check_errflag(Ctx* c) {
         CK(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
         return fail(c, GRANITE_ERR_CUDA, "stage kernel: a tensor-map tile load did not complete within its wait limit");
     }
+    return GRANITE_OK;
+}
+
+int granite_ccz4_set_pass_overlap(void* h, int on) {
+    Ctx* c = static_cast<Ctx*>(h);
+    if (!c) return GRANITE_ERR_INVALID;
+    c->overlap_passes = on != 0;
+    for (auto& kv : c->hgraphs)  // captured steps bake the choice in
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    c->hgraphs.clear();
+    for (auto& kv : c->graphs)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    c->graphs.clear();
     return GRANITE_OK;
 }
 
@@ -1398,7 +1412,7 @@ static cudaError_t stage_range(Ctx* c, LevelLists& L, int cfg, int precision, co
     StageArgs b64 = b;
     b64.want_prec = 1;
     b.want_prec = 0;
-    if (c->profiling) {
+    if (c->profiling || !c->overlap_passes) {
         if ((e = launch_stage(L.variant, cfg, PM_MIXED, EPI_RK, c->d_blocks, tiles, count, b, c->stream))) return e;
         return launch_stage(L.variant, cfg, PM_FP64F, EPI_RK, c->d_blocks, tiles, count, b64, c->stream);
     }

@@ -434,6 +434,9 @@ GRANITE_API int granite_ccz4_test_withhold_tile_load(void* ctx, int item);
  * FP64 algebra on every tile. Changing it drops the cached step graphs. The
  * stateless operators (granite_ccz4_compute_rhs_*) are not affected. */
 GRANITE_API int granite_ccz4_set_fp64_chi_threshold(void* ctx, double chi_fp64);
+/* 1 (default): the FP64 pass of the per-tile precision runs on a second stream
+ * of the context beside the FP32 pass (they write disjoint tiles); 0: after it. */
+GRANITE_API int granite_ccz4_set_pass_overlap(void* ctx, int on);
 GRANITE_API int granite_ccz4_get_fp64_chi_threshold(const void* ctx, double* chi_fp64);
 
 /* Same-level ghost copies in GRANITE_AMR_GHOSTS (no counterpart in the
