@@ -205,7 +205,7 @@ struct Ctx {
     unsigned int* d_errflag = nullptr;   // set by a TMA stage kernel whose bounded wait gave up
     int test_withhold = 0;               // armed test switch (StageArgs::test_withhold) of the next rk3_step
     bool ghost_push = true;              // GRANITE_AMR_GHOSTS: stage kernels push same-level ghost copies
-    bool overlap_passes = true;          // per-tile precision: FP64 pass beside the FP32 pass (second stream)
+    bool overlap_passes = false;         // per-tile precision: FP64 pass beside the FP32 pass (second stream)
     // every pushing level's same-level ghost copies of slot 0 equal their
     // sources (after a GRANITE_AMR_GHOSTS coarse step with pushes; cleared by
     // anything else that writes the state), and, while a coarse step is being
@@ -1785,13 +1785,19 @@ int build_ghosts_mode(Ctx* c) {
                 std::map<int, std::vector<PushBox>>& by_src = X[L].push_by_src;
                 by_src.clear();
                 for (const XferBox& x : copies) {
+                    const DevBlock& D = c->hblocks[x.dst];
                     PushBox pb{};
-                    pb.dst = x.dst;
+                    for (int sl = 0; sl < 3; ++sl) pb.buf[sl] = D.buf[sl];
+                    pb.stride = D.stride;
+                    pb.tx = D.tx;
+                    pb.txy = D.tx * D.ty;
+                    int off[3];
                     for (int d = 0; d < 3; ++d) {
                         pb.lo[d] = x.s0[d] - NG;
                         pb.hi[d] = pb.lo[d] + x.n[d];
-                        pb.off[d] = x.d0[d] + NG - x.s0[d];
+                        off[d] = x.d0[d] + NG - x.s0[d];  // destination cell index - source interior index
                     }
+                    pb.base = off[0] + (long long)pb.tx * off[1] + (long long)pb.txy * off[2];
                     by_src[x.src].push_back(pb);
                 }
                 std::vector<PushBox> plist;

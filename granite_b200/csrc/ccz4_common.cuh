@@ -50,12 +50,20 @@ struct Tile {
 // neighbour (GRANITE_AMR_GHOSTS): the stage kernel that writes such a cell
 // also writes it into the neighbour's ghost cell of the same buffer slot, so
 // the fill after the stage leaves those cells out. Source interior indices
-// [lo, hi) per axis; destination cell (incl. ghosts) = source index + off.
+// [lo, hi) per axis; the destination cell of source interior index (i, j, k)
+// is base + i + tx j + txy k in the neighbour's buffers (its pointers, field
+// stride and row / plane lengths are carried here, so a push needs no lookup
+// of the neighbour's descriptor).
 struct PushBox {
-    int dst;
+    double* buf[3];
+    long long stride;
+    long long base;
+    int tx, txy;
     int lo[3], hi[3];
-    int off[3];
 };
+// Push boxes of one tile staged in shared memory by the TMA stage kernel
+// (more than this many: read from global memory).
+constexpr int PUSH_STAGE_MAX = 16;
 
 // Arguments of one fused RHS launch.
 struct StageArgs {

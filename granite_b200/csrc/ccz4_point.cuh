@@ -495,28 +495,26 @@ __device__ __forceinline__ void point_pm(const DevBlock& B, const double* __rest
 // u_in: the stage input at the point, from global memory, or (tin != nullptr)
 // from a per-thread column of shared memory that the stencil source filled with
 // each field's centre value, field v at tin[v * tin_stride].
-// The new state of interior point (i, j, k) of the tile ti's block into the
-// ghost cells of the same-level neighbours that hold it (A.push), slot
-// out_sel; the boxes are the tile's, the containment test is per point.
-__device__ __forceinline__ void push_copies(const DevBlock* blocks, const StageArgs& A, int ti, int i, int j, int k,
+// The new state of interior point (i, j, k) into the ghost cells of the
+// same-level neighbours that hold it (the tile's npush boxes, slot out_sel);
+// the containment test is per point.
+__device__ __forceinline__ void push_copies(const PushBox* boxes, int npush, int out_sel, int i, int j, int k,
                                             const double r[NV]) {
-    const int2 pr = A.tile_push[ti];
-    for (int q = pr.x; q < pr.x + pr.y; ++q) {
-        const PushBox P = A.push[q];
+    for (int q = 0; q < npush; ++q) {
+        const PushBox& P = boxes[q];
         if (i < P.lo[0] || i >= P.hi[0] || j < P.lo[1] || j >= P.hi[1] || k < P.lo[2] || k >= P.hi[2]) continue;
-        const DevBlock& D = blocks[P.dst];
-        double* o = D.buf[A.out_sel] + cell_index(D, i + P.off[0], j + P.off[1], k + P.off[2]);
+        double* o = P.buf[out_sel] + (P.base + i + (long long)P.tx * j + (long long)P.txy * k);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) o[(long long)v * D.stride] = r[v];
+        for (int v = 0; v < NV; ++v) o[(long long)v * P.stride] = r[v];
     }
 }
 
-// blocks, ti, (i, j, k): the block table, the tile's index in the launch's list
-// and the point's interior indices, for the pushed ghost copies (A.push).
+// pushes, npush, (i, j, k): the tile's push boxes (A.push set) and the point's
+// interior indices, for the pushed ghost copies.
 template <int EPI, typename T>
 __device__ __forceinline__ void stage_epilogue(const DevBlock& B, const StageArgs& A, long long c, const T L[NV],
                                                const double* tin = nullptr, int tin_stride = 0,
-                                               const DevBlock* blocks = nullptr, int ti = 0, int i = 0, int j = 0,
+                                               const PushBox* pushes = nullptr, int npush = 0, int i = 0, int j = 0,
                                                int k = 0) {
     const long long st = B.stride;
     if (EPI == EPI_STORE) {
@@ -566,7 +564,7 @@ __device__ __forceinline__ void stage_epilogue(const DevBlock& B, const StageArg
     if (A.final_stage) algebraic_constraints(r);
 #pragma unroll
     for (int v = 0; v < NV; ++v) out[(long long)v * st + c] = r[v];
-    if (A.push && blocks) push_copies(blocks, A, ti, i, j, k, r);
+    if (npush > 0) push_copies(pushes, npush, A.out_sel, i, j, k, r);
 }
 
 }  // namespace granite_b200

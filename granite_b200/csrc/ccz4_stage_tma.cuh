@@ -238,6 +238,10 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         if (tid == 0) g_sel_list[TMA_SEL_CAP] = nsel < TMA_SEL_CAP ? nsel : TMA_SEL_CAP;  // (host keeps it below)
     }
     __syncthreads();
+    // push boxes of the current tile, double-buffered by tile round: staged when
+    // the round starts, read in its epilogue (the round's first field barrier
+    // lies between), overwritten two rounds later
+    __shared__ PushBox s_push[2][PUSH_STAGE_MAX];
     const int lx = tid % C::TX, ly = (tid / C::TX) % C::TY, lz = tid / (C::TX * C::TY);
     double* tin = C::TIN ? reinterpret_cast<double*>(base + C::OFF_TIN) + tid : nullptr;
     void* hs = C::HS ? static_cast<void*>(reinterpret_cast<P*>(base + C::OFF_HS) + tid) : nullptr;
@@ -258,6 +262,18 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         const int ic = min(i, B.n[0] - 1), jc = min(j, B.n[1] - 1), kc = min(k, B.n[2] - 1);
         const long long c = cell_index(B, ic + NG, jc + NG, kc + NG);
         const double* __restrict__ uin = B.buf[A.in_sel];
+        const PushBox* pushes = nullptr;
+        int npush = 0;
+        if (A.push) {
+            const int2 pr = A.tile_push[ti];
+            npush = pr.y;
+            if (npush <= PUSH_STAGE_MAX) {
+                if (tid < npush) s_push[r & 1][tid] = A.push[pr.x + tid];
+                pushes = s_push[r & 1];
+            } else {
+                pushes = A.push + pr.x;
+            }
+        }
         if constexpr (C::TIN) {
             // L2 prefetches: this tile's u^n (read by the epilogue; stage 1 takes
             // it from the ring) and the next tile's pointwise cells
@@ -279,7 +295,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         }
         AlgebraT<PM> L[NV];
         point_pm<PM>(B, uin, c, A, S, L);
-        if (valid) stage_epilogue<EPI>(B, A, c, L, tin, C::NT, blocks, ti, i, j, k);
+        if (valid) stage_epilogue<EPI>(B, A, c, L, tin, C::NT, pushes, npush, i, j, k);
     }
     // Every issued item was consumed (issue() skips items past this CTA's last
     // tile), so no copy into the ring is in flight when the CTA exits. If

@@ -283,7 +283,9 @@ __global__ void __launch_bounds__(C::NTHR, C::MINB)
         }
         P L[NV];
         ccz4_point<P, false>(B, uin, c, A, S, L);
-        if (valid) stage_epilogue<EPI>(B, A, c, L, nullptr, 0, blocks, ti, i, j, k);
+        // (the consumers have no tile barrier to stage the push boxes behind: global reads)
+        const int2 pr = A.push ? A.tile_push[ti] : make_int2(0, 0);
+        if (valid) stage_epilogue<EPI>(B, A, c, L, nullptr, 0, A.push ? A.push + pr.x : nullptr, pr.y, i, j, k);
     }
 }
 

@@ -434,8 +434,10 @@ GRANITE_API int granite_ccz4_test_withhold_tile_load(void* ctx, int item);
  * FP64 algebra on every tile. Changing it drops the cached step graphs. The
  * stateless operators (granite_ccz4_compute_rhs_*) are not affected. */
 GRANITE_API int granite_ccz4_set_fp64_chi_threshold(void* ctx, double chi_fp64);
-/* 1 (default): the FP64 pass of the per-tile precision runs on a second stream
- * of the context beside the FP32 pass (they write disjoint tiles); 0: after it. */
+/* 1: the FP64 pass of the per-tile precision runs on a second stream of the
+ * context beside the FP32 pass (they write disjoint tiles); 0 (default): after
+ * it. Measured on the binary hierarchy: 67.9 vs 67.2 ms per coarse step, the
+ * concurrent FP64 CTAs take SM slots the persistent FP32 pass needs. */
 GRANITE_API int granite_ccz4_set_pass_overlap(void* ctx, int on);
 GRANITE_API int granite_ccz4_get_fp64_chi_threshold(const void* ctx, double* chi_fp64);
 
