@@ -24,7 +24,9 @@ Extra objects on the JSON line:
                 profiling pass with CUDA events around every stage launch.
   e2e           the same metric through the C ABI with host buffers: every
                 step uploads every block from pinned memory, steps, and
-                downloads every block.
+                downloads every block; two contexts take the steps in turn so
+                one's copies overlap the other's step ("serial": one context,
+                copies and step in series).
   cpu_baseline  the compiled reference (oracle/_ref, Release flags, OpenMP on
                 all host cores) on a bounded sample of the workload's blocks.
 """
@@ -98,12 +100,16 @@ def ncu_traffic(workload: str, kernel: str):
 class Runner:
     """One workload on one device through the library's resident-block API."""
 
-    def __init__(self, gb, name, w, precision, variant, device, stage_config=-1):
+    def __init__(self, gb, name, w, precision, variant, device, stage_config=-1, like=None):
+        """like: another Runner of the same workload whose host blocks (the
+        initial state) this one shares instead of building its own."""
         self.gb, self.w, self.prec = gb, w, precision
         self.ev = gb.Evolver(gb.CCZ4Params(device=device), variant)
         if stage_config >= 0:
             self.ev.force_stage_config(stage_config)
-        if w["kind"] == "hier":
+        if like is not None:
+            self.h, self.blocks, self.points_per_step, self.dt = like.h, like.blocks, like.points_per_step, like.dt
+        elif w["kind"] == "hier":
             self.h = hierarchy_of(gb, w)
             self.blocks = gb.block_states(self.h, noise=1e-10, seed=12345)
             self.points_per_step = self.h.point_updates_per_coarse_step()
@@ -549,13 +555,16 @@ def main():
     kname = {gb.VARIANT_SMEM: "ccz4_stage_smem_kernel", gb.VARIANT_TMA: "ccz4_stage_tma_kernel"}.get(
         variant, "ccz4_stage_kernel")
     prec = gb.PRECISION_MIXED if precision == "mixed" else gb.PRECISION_FP64
+    def configure(r):
+        if prec == gb.PRECISION_MIXED and args.fp64_chi > 0.0:
+            r.ev.set_fp64_chi_threshold(args.fp64_chi)
+        if args.ghost_push >= 0:
+            r.ev.set_ghost_push(bool(args.ghost_push))
+        if args.pass_overlap >= 0:
+            r.ev.set_pass_overlap(bool(args.pass_overlap))
+
     run = Runner(gb, args.workload, w, prec, variant, local, args.stage_config)
-    if prec == gb.PRECISION_MIXED and args.fp64_chi > 0.0:
-        run.ev.set_fp64_chi_threshold(args.fp64_chi)
-    if args.ghost_push >= 0:
-        run.ev.set_ghost_push(bool(args.ghost_push))
-    if args.pass_overlap >= 0:
-        run.ev.set_pass_overlap(bool(args.pass_overlap))
+    configure(run)
     compare = None
     if prec == gb.PRECISION_MIXED and not args.no_compare:
         compare = Runner(gb, args.workload, w, gb.PRECISION_FP64, variant, local, args.stage_config)
@@ -587,29 +596,57 @@ def main():
 
     # e2e through the C ABI with host buffers (pinned), copies inside the timed
     # region: every step uploads its input state (the workload's initial state)
-    # from pinned host memory, steps, and downloads the result into another
-    # pinned buffer
-    hosts_in, hosts_out = [], []
-    for b in run.blocks:
-        for lst in (hosts_in, hosts_out):
-            t = torch.empty(b.array.size, dtype=torch.float64, pin_memory=True)
-            v = t.numpy().reshape(b.array.shape)
-            lst.append((t, v))
-        hosts_in[-1][1][...] = b.array
-    e2e_steps = max(1, min(args.steps, 3 if hier else 20))
+    # from pinned host memory, steps, and downloads the result into a pinned
+    # buffer. Two contexts hold the workload and take the steps in turn, so the
+    # copies of one (copy engines) run while the other steps (SMs); before a
+    # context takes its next step the host waits for its previous result. The
+    # same round trip on one context, copies and step in series, is reported
+    # beside it.
+    def pinned_like(a):
+        t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+        return t, t.numpy().reshape(a.shape)
+
+    hosts_in = [pinned_like(b.array) for b in run.blocks]
+    for (_, v), b in zip(hosts_in, run.blocks):
+        v[...] = b.array
+    hosts_out = [[pinned_like(b.array) for b in run.blocks] for _ in range(2)]
+    vin = [v for _, v in hosts_in]
+    vouts = [[v for _, v in ho] for ho in hosts_out]
+
+    serial_steps = max(1, min(args.steps, 3 if hier else 20))
     run.ev.sync()
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
-    vin = [v for _, v in hosts_in]
-    vout = [v for _, v in hosts_out]
-    for _ in range(e2e_steps):
+    for _ in range(serial_steps):
         run.ev.upload(None, vin)
         run.step()
-        run.ev.download(None, vout)
+        run.ev.download(None, vouts[0])
     run.ev.sync()
+    serial_ms = max_over_ranks(torch, dist, world, (time.perf_counter() - t0) * 1000.0, f"cuda:{local}")
+    serial_val = whole_job_rate(run.points_per_step, serial_steps, world, serial_ms)
+
+    run2 = Runner(gb, args.workload, w, prec, variant, local, args.stage_config, like=run)
+    configure(run2)
+    run2.step()  # builds its step graph
+    run2.ev.sync()
+    pair = (run, run2)
+    e2e_steps = max(4, min(args.steps, 16 if hier else 40))
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for s in range(e2e_steps):
+        r = pair[s % 2]
+        r.ev.sync()  # its previous result is on the host before the buffers are reused
+        r.ev.upload(None, vin)
+        r.step()
+        r.ev.download(None, vouts[s % 2], wait=False)
+    for r in pair:
+        r.ev.sync()
     e2e_ms = max_over_ranks(torch, dist, world, (time.perf_counter() - t0) * 1000.0, f"cuda:{local}")
     e2e_val = whole_job_rate(run.points_per_step, e2e_steps, world, e2e_ms)
+    run2.ev.close()
+    del run2, pair
 
     # after the headline measurements: the same mixed steps with the FP32 algebra on
     # every tile, then the FP64 comparison runs (these drop and rebuild cached graphs)
@@ -693,7 +730,8 @@ def main():
                 "dtype": "f32+f64" if prec == gb.PRECISION_MIXED else "f64", "data": "synthetic",
                 "config": cfg, "roofline": rl,
                 "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": run.state_bytes,
-                        "d2h_bytes_per_step": run.state_bytes, "steps": e2e_steps},
+                        "d2h_bytes_per_step": run.state_bytes, "steps": e2e_steps, "contexts": 2,
+                        "serial": {"value": serial_val, "steps": serial_steps, "contexts": 1}},
                 "cpu_baseline": cb, "clocks": clocks, "gpu_launches": launches}
         if cmp_line:
             line["fp64_plain"] = cmp_line

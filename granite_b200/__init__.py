@@ -34,7 +34,7 @@ KERNEL_STAGE, KERNEL_GHOST, KERNEL_TRANSFER, KERNEL_CONSTRAINTS = 0, 1, 2, 3
 VARIANT_GLOBAL, VARIANT_SMEM, VARIANT_GLOBAL_R168, VARIANT_GLOBAL_R128, VARIANT_TMA = 0, 1, 2, 3, 4
 VARIANT_NAMES = {"global": 0, "smem": 1, "global_r168": 2, "global_r128": 3, "tma": 4}
 # configurations of the TMA stage kernel and the block-size classes they are tuned for
-STAGE_CONFIGS = 6
+STAGE_CONFIGS = 8
 STAGE_CLASS_EDGES = (16, 24, 32, 48, 64, 96)
 
 _ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "no sm_100 device", -4: "out of memory",
@@ -128,6 +128,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_regrid_add.argtypes = [vp, C.POINTER(_BlockDesc), C.c_int]
     lib.granite_ccz4_upload_all.argtypes = [vp, C.POINTER(dp)]
     lib.granite_ccz4_download_all.argtypes = [vp, C.POINTER(dp)]
+    lib.granite_ccz4_download_all_async.argtypes = [vp, C.POINTER(dp)]
     ip = C.POINTER(C.c_int)
     hp = C.POINTER(_HorizonParams)
     lib.granite_ccz4_default_horizon_params.argtypes = [hp]
@@ -160,6 +161,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_get_stage_config.argtypes = [vp, C.c_int, C.c_int, ip_]
     lib.granite_ccz4_force_stage_config.argtypes = [vp, C.c_int]
     lib.granite_ccz4_stage_config_info.argtypes = [C.c_int, ip_, ip_, ip_, ip_]
+    lib.granite_ccz4_stage_config_schedule.argtypes = [C.c_int, ip_, ip_]
     lib.granite_ccz4_block_stage_class.argtypes = [C.POINTER(_BlockDesc), ip_]
     lib.granite_ccz4_compare_states.argtypes = [vp, vp, dp, dp, C.POINTER(C.c_longlong)]
     _LIB = lib
@@ -177,14 +179,16 @@ def _dp(a):
 # ---------------------------------------------------------------------------
 
 def stage_config_info(cfg: int) -> dict:
-    """Tile depth, ring slots and shared-memory options of a TMA configuration."""
+    """Tile depth, ring slots, shared-memory options and schedule of a TMA configuration."""
     lib = load_library()
     v = [C.c_int() for _ in range(4)]
     rc = lib.granite_ccz4_stage_config_info(int(cfg), *[C.byref(x) for x in v])
     if rc != GRANITE_OK:
         raise GraniteError(rc, f"unknown stage configuration {cfg}")
+    w = [C.c_int() for _ in range(2)]
+    lib.granite_ccz4_stage_config_schedule(int(cfg), *[C.byref(x) for x in w])
     return {"tile": (16, 4, v[0].value), "ring_slots": v[1].value, "shared_input": bool(v[2].value),
-            "shared_hessian": bool(v[3].value)}
+            "shared_hessian": bool(v[3].value), "warp_specialized": bool(w[0].value), "ctas_per_sm": w[1].value}
 
 
 def block_stage_class(ncells) -> int:
@@ -557,13 +561,20 @@ class Evolver:
         a = self.blocks[idx].array if array is None else _f64(array)
         self.ctx.check(self.ctx.lib.granite_ccz4_upload_block(self.ctx.h, idx, _dp(a)))
 
-    def download(self, idx: int | None = None, out=None):
-        """Block idx (all blocks when None, one synchronisation) into its host array or ``out``."""
+    def download(self, idx: int | None = None, out=None, wait: bool = True):
+        """Block idx (all blocks when None, one synchronisation) into its host array or ``out``.
+        For all blocks, ``wait=False`` queues the copies on the context's stream and
+        returns at once (granite_ccz4_download_all_async): the arrays hold the state
+        after the next sync()."""
         if idx is None:
             arrs = [b.array for b in self.blocks] if out is None else [_f64(a) for a in out]
             ptrs = (C.POINTER(C.c_double) * len(arrs))(*[_dp(a) for a in arrs])
-            self.ctx.check(self.ctx.lib.granite_ccz4_download_all(self.ctx.h, ptrs))
+            fn = self.ctx.lib.granite_ccz4_download_all if wait else self.ctx.lib.granite_ccz4_download_all_async
+            self.ctx.check(fn(self.ctx.h, ptrs))
+            if not wait:
+                self._keep_out = arrs
             return
+        assert wait, "single-block downloads wait"
         a = self.blocks[idx].array if out is None else _f64(out)
         self.ctx.check(self.ctx.lib.granite_ccz4_download_block(self.ctx.h, idx, _dp(a)))
 

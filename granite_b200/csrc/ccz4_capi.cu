@@ -204,7 +204,7 @@ struct Ctx {
     unsigned long long* d_nonfinite = nullptr;
     unsigned int* d_errflag = nullptr;   // set by a TMA stage kernel whose bounded wait gave up
     int test_withhold = 0;               // armed test switch (StageArgs::test_withhold) of the next rk3_step
-    bool ghost_push = true;              // GRANITE_AMR_GHOSTS: stage kernels push same-level ghost copies
+    bool ghost_push = false;             // GRANITE_AMR_GHOSTS: stage kernels push same-level ghost copies
     bool overlap_passes = false;         // per-tile precision: FP64 pass beside the FP32 pass (second stream)
     // every pushing level's same-level ghost copies of slot 0 equal their
     // sources (after a GRANITE_AMR_GHOSTS coarse step with pushes; cleared by
@@ -579,6 +579,14 @@ int granite_ccz4_stage_config_info(int cfg, int* tile_z, int* ring_slots, int* s
     if (shared_hessian) *shared_hessian = TMA_CFGS[cfg].hs;
     return GRANITE_OK;
 }
+
+int granite_ccz4_stage_config_schedule(int cfg, int* warp_specialized, int* ctas_per_sm) {
+    if (cfg < 0 || cfg >= NUM_TMA_CFGS) return GRANITE_ERR_INVALID;
+    if (warp_specialized) *warp_specialized = TMA_CFGS[cfg].ws;
+    if (ctas_per_sm) *ctas_per_sm = TMA_CFGS[cfg].minb;
+    return GRANITE_OK;
+}
+static_assert(GRANITE_STAGE_CONFIGS == NUM_TMA_CFGS, "the header's configuration count");
 
 int granite_ccz4_block_stage_class(const granite_block_desc* b, int* cls) {
     if (!b || !cls) return GRANITE_ERR_INVALID;
@@ -1344,7 +1352,7 @@ int granite_ccz4_upload_all(void* h, const double* const* hosts) {
     return GRANITE_OK;
 }
 
-int granite_ccz4_download_all(void* h, double* const* hosts) {
+int granite_ccz4_download_all_async(void* h, double* const* hosts) {
     Ctx* c = static_cast<Ctx*>(h);
     if (!c) return GRANITE_ERR_INVALID;
     if (!c->committed) return fail(c, GRANITE_ERR_INVALID, "commit before upload/download");
@@ -1356,6 +1364,13 @@ int granite_ccz4_download_all(void* h, double* const* hosts) {
         CK(cudaMemcpyAsync(hosts[i], c->hblocks[i].buf[0], (size_t)c->hblocks[i].stride * NV * sizeof(double),
                            cudaMemcpyDeviceToHost, c->stream),
            "D2H block");
+    return GRANITE_OK;
+}
+
+int granite_ccz4_download_all(void* h, double* const* hosts) {
+    int r = granite_ccz4_download_all_async(h, hosts);
+    if (r) return r;
+    Ctx* c = static_cast<Ctx*>(h);
     CK(cudaStreamSynchronize(c->stream), "sync");
     return check_errflag(c);  // a stage whose tile wait gave up has left no valid state
 }

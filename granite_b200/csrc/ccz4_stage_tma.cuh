@@ -19,7 +19,11 @@
 //        epilogue's u^n cells and the next tile's pointwise cells are
 //        prefetched into L2 at the start of each tile;
 //   HS   the 36 values of the Hessian-field loop live in a per-thread column of
-//        shared memory instead of local memory.
+//        shared memory instead of local memory;
+//   MINB resident CTAs per SM that the register allocation is sized for
+//        (__launch_bounds__): 3 CTAs of 128 threads cap a thread at 168
+//        registers, and the ring (with or without TIN) still fits three times in
+//        an SM's shared memory.
 #pragma once
 
 #include <cstdint>
@@ -31,12 +35,12 @@ namespace granite_b200 {
 
 namespace {
 
-template <int TZ_, int NBUF_, bool TIN_, bool HS_>
+template <int TZ_, int NBUF_, bool TIN_, bool HS_, int MINB_>
 struct TmaCfgT {
     static constexpr int TZ = TZ_, NBUF = NBUF_;
     static constexpr bool TIN = TIN_, HS = HS_;
     static constexpr int TX = 16, TY = 4, NT = TX * TY * TZ;
-    static constexpr int MINB = TZ == 2 ? 2 : 1;  // resident CTAs per SM asked of the register allocator
+    static constexpr int MINB = MINB_;  // resident CTAs per SM asked of the register allocator
     static constexpr int BX = TX + 8, BY = TY + 8, BZ = TZ + 8;
     static constexpr int BOX = BX * BY * BZ;
     static constexpr unsigned BYTES = BOX * sizeof(double);  // complete_tx count of one item
@@ -374,7 +378,8 @@ struct TmaConfigOps {
 // One translation unit per configuration k of TMA_CFGS defines its entry points.
 #define GRANITE_TMA_CFG_UNIT(K, STORE)                                                                               \
     namespace granite_b200 {                                                                                         \
-    using TmaCfg##K = TmaCfgT<TMA_CFGS[K].tz, TMA_CFGS[K].nbuf, TMA_CFGS[K].tin != 0, TMA_CFGS[K].hs != 0>;           \
+    using TmaCfg##K =                                                                                                \
+        TmaCfgT<TMA_CFGS[K].tz, TMA_CFGS[K].nbuf, TMA_CFGS[K].tin != 0, TMA_CFGS[K].hs != 0, TMA_CFGS[K].minb>;      \
     cudaError_t configure_tma_cfg##K(int nsm, int grids[3][2][2]) {                                                  \
         return TmaConfigOps<TmaCfg##K>::configure<STORE>(nsm, grids);                                                \
     }                                                                                                                \

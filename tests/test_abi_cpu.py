@@ -139,6 +139,7 @@ def test_null_context_is_an_error_everywhere(lib):
         lib.granite_ccz4_checkpoint_read(None, b"x", None, None),
         lib.granite_ccz4_upload_all(None, None),
         lib.granite_ccz4_download_all(None, None),
+        lib.granite_ccz4_download_all_async(None, None),
     ]
     assert calls == [-1] * len(calls)
     n = C.c_int()
@@ -243,6 +244,16 @@ def test_stage_configs_and_classes_without_a_device():
         info = gb.stage_config_info(k)
         assert info["tile"][:2] == (16, 4) and info["tile"][2] in (2, 4)
         assert info["ring_slots"] in (2, 3, 4)
+        assert info["ctas_per_sm"] in (1, 2, 3)
+        if info["ctas_per_sm"] == 3:
+            # the ring and the stage-input column of one CTA fit three times in
+            # an SM's 228 KB of shared memory (with 7.5 KB per CTA for static
+            # buffers and the per-CTA reservation)
+            nt = 64 * info["tile"][2]
+            dyn = info["ring_slots"] * 24 * 12 * (info["tile"][2] + 8) * 8 + 256
+            dyn += 22 * nt * 8 if info["shared_input"] else 0
+            assert not info["shared_hessian"] and 3 * (dyn + 7680) <= 228 * 1024, (k, info)
+    assert [gb.stage_config_info(k)["ctas_per_sm"] for k in (6, 7)] == [3, 3]
     with pytest.raises(gb.GraniteError):
         gb.stage_config_info(gb.STAGE_CONFIGS)
     assert [gb.block_stage_class((e, e, e)) for e in gb.STAGE_CLASS_EDGES] == list(range(6))

@@ -188,10 +188,12 @@ def test_finest_prefill_skip_is_exact(gb, oracle_lib, precision):
 
 @pytest.mark.parametrize("precision,chi", [(0, 0.0), (1, 0.0), (1, 0.5)])
 def test_ghost_push_equals_copy_fills(gb, oracle_lib, precision, chi):
-    # GRANITE_AMR_GHOSTS: the stage kernels and the restrictions write the
-    # same-level ghost copies themselves (both passes of the per-tile precision
-    # included) and the fills leave the copies out; the result equals the run
-    # whose fills copy every same-level ghost cell, bit for bit
+    # GRANITE_AMR_GHOSTS with pushes on: the stage kernels write the same-level
+    # ghost copies themselves (both passes of the per-tile precision included),
+    # the fills after the stages leave the copies out, and the fill before a
+    # level step refreshes only the copies of cells a restriction rewrote; the
+    # result equals the run whose fills copy every same-level ghost cell (the
+    # default), bit for bit
     # blocks of 16 to 32 cells, so that every level runs the TMA stage kernel
     from granite_b200.hierarchy import make_binary_hierarchy
     h = make_binary_hierarchy(seed=21, levels=3, coarse_n=48, extent=16.0, sizes=(16, 24, 32),
@@ -221,3 +223,52 @@ def test_ghost_push_equals_copy_fills(gb, oracle_lib, precision, chi):
         ev.close()
     for i, (a, b) in enumerate(zip(*outs)):
         assert np.array_equal(a, b), f"array {i}: pushed ghost copies differ from copied ones"
+
+
+def test_two_contexts_pipelined_host_round_trips(gb, oracle_lib):
+    """The host round trip of bench.py's e2e: two contexts alternate, each step
+    uploads the input from pinned memory, steps, and queues the download
+    (granite_ccz4_download_all_async) while the other context works; every
+    result equals the same step taken alone, bit for bit."""
+    import torch
+    h, geoms, levels = small_hierarchy(seed=4, levels=3)
+    states = [oracle_lib.init_brill_lindquist(g, h.masses, h.positions, r_floor=0.5 * g.dx[0]) for g in geoms]
+    dt = 0.25 * geoms[0].dx[0]
+    ev, blocks = gpu_hierarchy(gb, geoms, levels, states)
+    ev.hierarchy_step(dt, gb.PRECISION_MIXED, gb.AMR_GHOSTS)
+    ev.download()
+    want = [b.array.copy() for b in blocks]
+    ev.close()
+
+    def pinned(a):
+        t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+        v = t.numpy().reshape(a.shape)
+        v[...] = a
+        return t, v
+
+    pin_in = [pinned(s) for s in states]
+    vin = [v for _, v in pin_in]
+    evs, outs = [], []
+    for _ in range(2):
+        e, _b = gpu_hierarchy(gb, geoms, levels, states)
+        evs.append(e)
+        outs.append([pinned(np.zeros_like(s)) for s in states])
+    try:
+        for s in range(6):
+            e, o = evs[s % 2], outs[s % 2]
+            e.sync()
+            if s >= 2:  # the result of step s - 2, read before its buffers are reused
+                for a, b in zip(want, o):
+                    assert np.array_equal(a, b[1])
+                for _, v in o:
+                    v[...] = 0.0
+            e.upload(None, vin)
+            e.hierarchy_step(dt, gb.PRECISION_MIXED, gb.AMR_GHOSTS)
+            e.download(None, [v for _, v in o], wait=False)
+        for e, o in zip(evs, outs):
+            e.sync()
+            for a, b in zip(want, o):
+                assert np.array_equal(a, b[1])
+    finally:
+        for e in evs:
+            e.close()

@@ -25,7 +25,7 @@ from test_parity_gpu import parity
 
 pytestmark = pytest.mark.gpu
 
-CONFIGS = [0, 1, 2, 3, 4, 5]
+CONFIGS = [0, 1, 2, 3, 4, 5, 6, 7]
 
 
 @pytest.fixture(scope="module")
@@ -121,7 +121,7 @@ def test_per_class_table_on_a_hierarchy(gb, oracle_lib):
 
     classes = [gb.block_stage_class(g.n) for g in geoms]
     assert len(set(classes)) == 3
-    mixed_table = [2, 5, 3, 4, 1, 2]
+    mixed_table = [6, 5, 3, 7, 1, 2]
     table = {"fp64": mixed_table, "mixed": mixed_table}
     a = run(None, gb.PRECISION_FP64)
     b = run(table, gb.PRECISION_FP64)
