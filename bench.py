@@ -24,9 +24,9 @@ Extra objects on the JSON line:
                 profiling pass with CUDA events around every stage launch.
   e2e           the same metric through the C ABI with host buffers: every
                 step uploads every block from pinned memory, steps, and
-                downloads every block; two contexts take the steps in turn so
-                one's copies overlap the other's step ("serial": one context,
-                copies and step in series).
+                downloads every block; three contexts take the steps in turn so
+                that one's upload and another's download overlap the third's
+                step ("serial": one context, copies and step in series).
   cpu_baseline  the compiled reference (oracle/_ref, Release flags, OpenMP on
                 all host cores) on a bounded sample of the workload's blocks.
 """
@@ -49,6 +49,7 @@ sys.path.insert(0, ROOT)
 METRIC = "CCZ4 RK3 point-updates/s on 1 B200: mixed/batched vs FP64 plain, equal accuracy"
 UNIT = "point-updates/s"
 BYTES_PER_POINT_UPDATE = 1408  # 3 stages: (2 + 3 + 3) x 22 fields x 8 B
+E2E_CONTEXTS = 3  # contexts of the e2e pipeline: upload, step and download in flight at once
 # reference-equivalent flops per point-update: 3 RHS + KO evaluations as ccz4.cpp
 # is written (10,395 each, op-counted) + the RK combine (22 fields x 3 stages x 4)
 FLOPS_PER_POINT_UPDATE = 3 * 10395 + 22 * 3 * 4
@@ -418,7 +419,10 @@ def roofline(gb, run: Runner, workload, prof_steps, kernel):
             "traffic": traffic, "peak_source": peak_kind, "kernel": kernel,
             "avg_launch_ms": st_ms / max(st_n, 1), "launches_per_step": st_n / prof_steps,
             "algorithmic_bytes_per_launch": per_launch,
-            "stage_share_of_step": st_ms / max(st_ms + gh_ms + xf_ms, 1e-12), "compute": compute}
+            "stage_share_of_step": st_ms / max(st_ms + gh_ms + xf_ms, 1e-12),
+            "device_ms_per_step": {"stage": st_ms / prof_steps, "ghost": gh_ms / prof_steps,
+                                   "transfer": xf_ms / prof_steps},
+            "compute": compute}
 
 
 def accuracy(gb, a: Runner, b: Runner, steps: int):
@@ -597,8 +601,12 @@ def main():
     # e2e through the C ABI with host buffers (pinned), copies inside the timed
     # region: every step uploads its input state (the workload's initial state)
     # from pinned host memory, steps, and downloads the result into a pinned
-    # buffer. Two contexts hold the workload and take the steps in turn, so the
-    # copies of one (copy engines) run while the other steps (SMs); before a
+    # buffer. E2E_CONTEXTS contexts hold the workload and take the steps in
+    # turn, a three-stage pipeline: while one context steps (SMs), the next
+    # one's upload and the previous one's download run (copy engines, one
+    # direction each). Uploads, and downloads, are ordered across the contexts
+    # by events on the contexts' streams, so each copy runs at the full PCIe
+    # rate instead of sharing it with the other contexts' copies; before a
     # context takes its next step the host waits for its previous result. The
     # same round trip on one context, copies and step in series, is reported
     # beside it.
@@ -609,7 +617,7 @@ def main():
     hosts_in = [pinned_like(b.array) for b in run.blocks]
     for (_, v), b in zip(hosts_in, run.blocks):
         v[...] = b.array
-    hosts_out = [[pinned_like(b.array) for b in run.blocks] for _ in range(2)]
+    hosts_out = [[pinned_like(b.array) for b in run.blocks] for _ in range(E2E_CONTEXTS)]
     vin = [v for _, v in hosts_in]
     vouts = [[v for _, v in ho] for ho in hosts_out]
 
@@ -626,27 +634,40 @@ def main():
     serial_ms = max_over_ranks(torch, dist, world, (time.perf_counter() - t0) * 1000.0, f"cuda:{local}")
     serial_val = whole_job_rate(run.points_per_step, serial_steps, world, serial_ms)
 
-    run2 = Runner(gb, args.workload, w, prec, variant, local, args.stage_config, like=run)
-    configure(run2)
-    run2.step()  # builds its step graph
-    run2.ev.sync()
-    pair = (run, run2)
-    e2e_steps = max(4, min(args.steps, 16 if hier else 40))
+    ring = [run]
+    for _ in range(E2E_CONTEXTS - 1):
+        r = Runner(gb, args.workload, w, prec, variant, local, args.stage_config, like=run)
+        configure(r)
+        r.step()  # builds its step graph
+        r.ev.sync()
+        ring.append(r)
+    streams = [torch.cuda.ExternalStream(r.ev.stream_handle(), device=f"cuda:{local}") for r in ring]
+    e2e_steps = max(2 * E2E_CONTEXTS, min(args.steps, 16 if hier else 40))
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
+    last_up = last_down = None
     for s in range(e2e_steps):
-        r = pair[s % 2]
+        r, st = ring[s % E2E_CONTEXTS], streams[s % E2E_CONTEXTS]
         r.ev.sync()  # its previous result is on the host before the buffers are reused
+        if last_up is not None:
+            st.wait_event(last_up)
         r.ev.upload(None, vin)
+        last_up = torch.cuda.Event()
+        last_up.record(st)
         r.step()
-        r.ev.download(None, vouts[s % 2], wait=False)
-    for r in pair:
+        if last_down is not None:
+            st.wait_event(last_down)
+        r.ev.download(None, vouts[s % E2E_CONTEXTS], wait=False)
+        last_down = torch.cuda.Event()
+        last_down.record(st)
+    for r in ring:
         r.ev.sync()
     e2e_ms = max_over_ranks(torch, dist, world, (time.perf_counter() - t0) * 1000.0, f"cuda:{local}")
     e2e_val = whole_job_rate(run.points_per_step, e2e_steps, world, e2e_ms)
-    run2.ev.close()
-    del run2, pair
+    for r in ring[1:]:
+        r.ev.close()
+    del ring, streams
 
     # after the headline measurements: the same mixed steps with the FP32 algebra on
     # every tile, then the FP64 comparison runs (these drop and rebuild cached graphs)
@@ -730,7 +751,7 @@ def main():
                 "dtype": "f32+f64" if prec == gb.PRECISION_MIXED else "f64", "data": "synthetic",
                 "config": cfg, "roofline": rl,
                 "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": run.state_bytes,
-                        "d2h_bytes_per_step": run.state_bytes, "steps": e2e_steps, "contexts": 2,
+                        "d2h_bytes_per_step": run.state_bytes, "steps": e2e_steps, "contexts": E2E_CONTEXTS,
                         "serial": {"value": serial_val, "steps": serial_steps, "contexts": 1}},
                 "cpu_baseline": cb, "clocks": clocks, "gpu_launches": launches}
         if cmp_line:

@@ -226,9 +226,10 @@ def test_ghost_push_equals_copy_fills(gb, oracle_lib, precision, chi):
 
 
 def test_two_contexts_pipelined_host_round_trips(gb, oracle_lib):
-    """The host round trip of bench.py's e2e: two contexts alternate, each step
-    uploads the input from pinned memory, steps, and queues the download
-    (granite_ccz4_download_all_async) while the other context works; every
+    """The host round trip of bench.py's e2e: three contexts take the steps in
+    turn, each step uploads the input from pinned memory, steps, and queues the
+    download (granite_ccz4_download_all_async) while the other contexts work,
+    uploads and downloads ordered across the contexts' streams by events; every
     result equals the same step taken alone, bit for bit."""
     import torch
     h, geoms, levels = small_hierarchy(seed=4, levels=3)
@@ -248,23 +249,34 @@ def test_two_contexts_pipelined_host_round_trips(gb, oracle_lib):
 
     pin_in = [pinned(s) for s in states]
     vin = [v for _, v in pin_in]
+    nctx = 3
     evs, outs = [], []
-    for _ in range(2):
+    for _ in range(nctx):
         e, _b = gpu_hierarchy(gb, geoms, levels, states)
         evs.append(e)
         outs.append([pinned(np.zeros_like(s)) for s in states])
+    streams = [torch.cuda.ExternalStream(e.stream_handle(), device="cuda:0") for e in evs]
     try:
-        for s in range(6):
-            e, o = evs[s % 2], outs[s % 2]
+        last_up = last_down = None
+        for s in range(9):
+            e, o, st = evs[s % nctx], outs[s % nctx], streams[s % nctx]
             e.sync()
-            if s >= 2:  # the result of step s - 2, read before its buffers are reused
+            if s >= nctx:  # the result of step s - nctx, read before its buffers are reused
                 for a, b in zip(want, o):
                     assert np.array_equal(a, b[1])
                 for _, v in o:
                     v[...] = 0.0
+            if last_up is not None:
+                st.wait_event(last_up)
             e.upload(None, vin)
+            last_up = torch.cuda.Event()
+            last_up.record(st)
             e.hierarchy_step(dt, gb.PRECISION_MIXED, gb.AMR_GHOSTS)
+            if last_down is not None:
+                st.wait_event(last_down)
             e.download(None, [v for _, v in o], wait=False)
+            last_down = torch.cuda.Event()
+            last_down.record(st)
         for e, o in zip(evs, outs):
             e.sync()
             for a, b in zip(want, o):
