@@ -162,7 +162,7 @@ __global__ void ghost_fill_kernel(int mode, const DevBlock* __restrict__ blocks,
 // amr.cpp:496-561: nearest coarse centre by rounding, one-sided neighbour by
 // the sign of the fractional offset, indices clamped to the coarse block.
 __device__ void prolong_cell(const DevBlock& F, const DevBlock& C, int i, int j, int k, double* __restrict__ fb,
-                             const double* __restrict__ cb, int v0 = 0, int v1 = NV) {
+                             const double* __restrict__ cb) {
     const int fi[3] = {i, j, k};
     const int ct[3] = {C.tx, C.ty, C.tz};
     int c0[3], c1[3];
@@ -195,7 +195,7 @@ __device__ void prolong_cell(const DevBlock& F, const DevBlock& C, int i, int j,
     const int o011 = (int)cell_index(C, c0[0], c1[1], c1[2]), o111 = (int)cell_index(C, c1[0], c1[1], c1[2]);
     const long long fc = cell_index(F, i, j, k);
 #pragma unroll 2
-    for (int v = v0; v < v1; ++v) {
+    for (int v = 0; v < NV; ++v) {
         const double* q = cb + (long long)v * C.stride;
         double val = __dmul_rn(w000, __ldg(q + o000));
         val = __dadd_rn(val, __dmul_rn(w100, __ldg(q + o100)));
@@ -244,23 +244,17 @@ __global__ void xfer_kernel(int kind, const DevBlock* __restrict__ blocks, const
     }
 }
 
-// Two threads per listed ghost cell: thread t and t + 128 of a CTA move fields
-// [0, 11) and [11, 22) of cell 128 blockIdx.x + t, so each thread has all of its
-// 11 loads in flight at once (one thread per cell moved the 22 fields in two
-// passes of 11 loads to stay within 64 registers); 4 CTAs of 256 threads per
-// SM. Each cell is written exactly once. The cells a launch reads
-// (interior cells of this level, coarse slot 0) are never written by it, so
-// every value of a cell is loaded before any is stored.
-constexpr int GHOST_CELLS_PER_CTA = 128;
-
-__global__ void __launch_bounds__(2 * GHOST_CELLS_PER_CTA, 4)
-    ghost_sources_kernel(const DevBlock* __restrict__ blocks, const GhostSrc* __restrict__ items, long long n, int sel,
-                         int local_mode) {
-    const int half = threadIdx.x / GHOST_CELLS_PER_CTA;
-    const long long t = (long long)blockIdx.x * GHOST_CELLS_PER_CTA + (threadIdx.x % GHOST_CELLS_PER_CTA);
+// One thread per listed ghost cell; each cell is written exactly once. The
+// cells a launch reads (interior cells of this level, coarse slot 0) are never
+// written by it, so every value of a cell is loaded before any is stored.
+// 4 CTAs of 256 threads per SM (64 registers): the fields of a cell are moved in
+// two halves and the prolongation keeps 32-bit offsets, so the paths fit without
+// the 127 registers (16 warps per SM) of a one-pass version; about 5 % faster on
+// the hierarchy's fills.
+__global__ void __launch_bounds__(256, 4) ghost_sources_kernel(const DevBlock* __restrict__ blocks, const GhostSrc* __restrict__ items,
+                                     long long n, int sel, int local_mode) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    constexpr int NH = NV / 2;
-    const int v0 = half * NH;
     const GhostSrc it = items[t];
     const DevBlock& D = blocks[it.dst_block];
     double* db = D.buf[sel];
@@ -268,7 +262,7 @@ __global__ void __launch_bounds__(2 * GHOST_CELLS_PER_CTA, 4)
     const int i = it.dst_cell % D.tx, j = (it.dst_cell / D.tx) % D.ty, k = it.dst_cell / (D.tx * D.ty);
     if (it.src_block >= 0 && it.src_cell < 0) {  // coarse level
         const DevBlock& C = blocks[it.src_block];
-        prolong_cell(D, C, i, j, k, db, C.buf[0], v0, v0 + NH);
+        prolong_cell(D, C, i, j, k, db, C.buf[0]);
         return;
     }
     const double* src;
@@ -279,17 +273,20 @@ __global__ void __launch_bounds__(2 * GHOST_CELLS_PER_CTA, 4)
         sstr = S.stride;
     } else if (local_mode == GHOST_SOMMERFELD) {
         const FalloffChain ch = falloff_chain(D, i, j, k);
-        double v_[NH];
 #pragma unroll
-        for (int v = 0; v < NH; ++v) v_[v] = __ldg(db + (v0 + v) * dstr + ch.src);
+        for (int h = 0; h < 2; ++h) {
+            double v_[NV / 2];
 #pragma unroll
-        for (int v = 0; v < NH; ++v) {
-            const double fi = f_inf(v0 + v);
-            double val = v_[v];
+            for (int v = 0; v < NV / 2; ++v) v_[v] = __ldg(db + (h * (NV / 2) + v) * dstr + ch.src);
 #pragma unroll
+            for (int v = 0; v < NV / 2; ++v) {
+                const double fi = f_inf(h * (NV / 2) + v);
+                double val = v_[v];
+    #pragma unroll
             for (int p = 0; p < 3; ++p)  // unrolled with a guard: the radii stay in registers
                 if (p < ch.npass) val = falloff(fi, val, ch.ri[p], ch.rg[p]);
-            db[(v0 + v) * dstr + dst] = val;
+                db[(h * (NV / 2) + v) * dstr + dst] = val;
+            }
         }
         return;
     } else {  // zero gradient
@@ -297,11 +294,14 @@ __global__ void __launch_bounds__(2 * GHOST_CELLS_PER_CTA, 4)
                               clampi(k, NG, NG + D.n[2] - 1));
         sstr = dstr;
     }
-    double v_[NH];
 #pragma unroll
-    for (int v = 0; v < NH; ++v) v_[v] = __ldg(src + (v0 + v) * sstr);
+    for (int h = 0; h < 2; ++h) {
+        double v_[NV / 2];
 #pragma unroll
-    for (int v = 0; v < NH; ++v) db[(v0 + v) * dstr + dst] = v_[v];
+        for (int v = 0; v < NV / 2; ++v) v_[v] = __ldg(src + (h * (NV / 2) + v) * sstr);
+#pragma unroll
+        for (int v = 0; v < NV / 2; ++v) db[(h * (NV / 2) + v) * dstr + dst] = v_[v];
+    }
 }
 
 }  // namespace
@@ -309,8 +309,8 @@ __global__ void __launch_bounds__(2 * GHOST_CELLS_PER_CTA, 4)
 cudaError_t launch_ghost_sources(const DevBlock* blocks, const GhostSrc* items, long long nitems, int sel,
                                  int local_mode, cudaStream_t stream) {
     if (nitems <= 0) return cudaSuccess;
-    ghost_sources_kernel<<<(unsigned)((nitems + GHOST_CELLS_PER_CTA - 1) / GHOST_CELLS_PER_CTA),
-                           2 * GHOST_CELLS_PER_CTA, 0, stream>>>(blocks, items, nitems, sel, local_mode);
+    ghost_sources_kernel<<<(unsigned)((nitems + 255) / 256), 256, 0, stream>>>(blocks, items, nitems, sel,
+                                                                            local_mode);
     return cudaGetLastError();
 }
 
