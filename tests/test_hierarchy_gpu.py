@@ -225,7 +225,7 @@ def test_ghost_push_equals_copy_fills(gb, oracle_lib, precision, chi):
         assert np.array_equal(a, b), f"array {i}: pushed ghost copies differ from copied ones"
 
 
-def test_two_contexts_pipelined_host_round_trips(gb, oracle_lib):
+def test_three_context_pipeline_host_round_trips(gb, oracle_lib):
     """The host round trip of bench.py's e2e: three contexts take the steps in
     turn, each step uploads the input from pinned memory, steps, and queues the
     download (granite_ccz4_download_all_async) while the other contexts work,
