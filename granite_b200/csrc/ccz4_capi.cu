@@ -159,15 +159,6 @@ struct LevelXfer {
     GhostSrc* d_src_pre = nullptr;
     long long nsrc_pre = 0;
     std::vector<std::pair<long long, long long>> src_range_pre;
-    // the same-level copies of d_src / d_src_stage with resolved addresses (offsets
-    // from cp_arena, the arena the lists were built for): a batched fill runs
-    // them as one launch and the rest of the cells (d_src_nc / d_src_stage_nc) as
-    // another
-    GhostCopy* d_cp = nullptr;
-    long long ncp = 0;
-    GhostCopy* d_cp_stage = nullptr;
-    long long ncp_stage = 0;
-    const char* cp_arena = nullptr;
 };
 
 // device copy of a host vector (nullptr for an empty one)
@@ -1083,8 +1074,6 @@ static void release_lists(Ctx* c) {
             cudaFree(X.d_src_nc);
             cudaFree(X.d_src_stage_nc);
             cudaFree(X.d_src_pre);
-            cudaFree(X.d_cp);
-            cudaFree(X.d_cp_stage);
         }
         c->xfer[m].clear();
         c->xfer_built[m] = false;
@@ -1789,26 +1778,6 @@ int build_ghosts_mode(Ctx* c) {
             X[L].nsrc_nc = (long long)nc.size();
             CK(upload_vec(snc, &X[L].d_src_stage_nc, c->stream), "upload stage ghost sources without copies");
             X[L].nsrc_stage_nc = (long long)snc.size();
-            // the copies of both lists with their addresses resolved against the arena
-            auto resolve = [&](const std::vector<GhostSrc>& all, std::vector<GhostCopy>& out) {
-                const double* a0 = reinterpret_cast<const double*>(c->arena);
-                for (const auto& g : all) {
-                    if (!(g.src_block >= 0 && g.src_cell >= 0)) continue;
-                    const DevBlock& D = c->hblocks[g.dst_block];
-                    const DevBlock& S = c->hblocks[g.src_block];
-                    out.push_back(GhostCopy{(long long)(D.buf[0] - a0) + g.dst_cell, (long long)(S.buf[0] - a0) + g.src_cell,
-                                            (int)(D.buf[1] - D.buf[0]), (int)D.stride, (int)(S.buf[1] - S.buf[0]),
-                                            (int)S.stride});
-                }
-            };
-            std::vector<GhostCopy> cp, scp;
-            resolve(items, cp);
-            resolve(sitems, scp);
-            CK(upload_vec(cp, &X[L].d_cp, c->stream), "upload ghost copies");
-            X[L].ncp = (long long)cp.size();
-            CK(upload_vec(scp, &X[L].d_cp_stage, c->stream), "upload stage ghost copies");
-            X[L].ncp_stage = (long long)scp.size();
-            X[L].cp_arena = c->arena;
         }
         // push boxes: every copy box (a <- b) seen from b's interior, and per
         // stage tile of the level the boxes of its block that meet the tile.
@@ -2083,25 +2052,6 @@ cudaError_t fill_level(Ctx* c, int L, int slot, bool level_fill, int mode, long 
     const auto& ranges = all ? (prefill_fresh ? X.src_range_pre : pushed ? X.src_range_nc : X.src_range)
                              : (pushed ? X.src_range_stage_nc : X.src_range_stage);
     if (c->batched) {
-        if (!pushed && !prefill_fresh && X.cp_arena == c->arena) {
-            // the copies (resolved addresses) and the other cells as two launches
-            const GhostCopy* cp = all ? X.d_cp : X.d_cp_stage;
-            const long long ncp = all ? X.ncp : X.ncp_stage;
-            const GhostSrc* rest = all ? X.d_src_nc : X.d_src_stage_nc;
-            const long long nrest = all ? X.nsrc_nc : X.nsrc_stage_nc;
-            if (ncp > 0) {
-                ++*n;
-                if ((e = timed(c, GRANITE_KERNEL_GHOST, [&] {
-                         return launch_ghost_copies(reinterpret_cast<double*>(c->arena), cp, ncp, slot, c->stream);
-                     })))
-                    return e;
-            }
-            if (nrest == 0) return cudaSuccess;
-            ++*n;
-            return timed(c, GRANITE_KERNEL_GHOST, [&] {
-                return launch_ghost_sources(c->d_blocks, rest, nrest, slot, local, c->stream);
-            });
-        }
         if (nsrc == 0) return cudaSuccess;
         ++*n;
         return timed(c, GRANITE_KERNEL_GHOST, [&] {

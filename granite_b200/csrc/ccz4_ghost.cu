@@ -304,30 +304,7 @@ __global__ void __launch_bounds__(256, 4) ghost_sources_kernel(const DevBlock* _
     }
 }
 
-// One thread per listed copy, all 22 loads in flight before the stores; the
-// addresses come from the item alone (no block descriptor, no cell
-// coordinates). Sources are interior cells, destinations ghost cells.
-__global__ void __launch_bounds__(256) ghost_copy_kernel(double* __restrict__ arena, const GhostCopy* __restrict__ items,
-                                                         long long n, int sel) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const GhostCopy it = items[t];
-    const double* __restrict__ s = arena + it.src + (long long)sel * it.spitch;
-    double* __restrict__ d = arena + it.dst + (long long)sel * it.dpitch;
-    double v_[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) v_[v] = __ldg(s + (long long)v * it.sstride);
-#pragma unroll
-    for (int v = 0; v < NV; ++v) d[(long long)v * it.dstride] = v_[v];
-}
-
 }  // namespace
-
-cudaError_t launch_ghost_copies(double* arena, const GhostCopy* items, long long nitems, int sel, cudaStream_t stream) {
-    if (nitems <= 0) return cudaSuccess;
-    ghost_copy_kernel<<<(unsigned)((nitems + 255) / 256), 256, 0, stream>>>(arena, items, nitems, sel);
-    return cudaGetLastError();
-}
 
 cudaError_t launch_ghost_sources(const DevBlock* blocks, const GhostSrc* items, long long nitems, int sel,
                                  int local_mode, cudaStream_t stream) {

@@ -144,17 +144,6 @@ struct GhostSrc {
 cudaError_t launch_ghost_sources(const DevBlock* blocks, const GhostSrc* items, long long nitems, int sel,
                                  int local_mode, cudaStream_t stream);
 
-// A same-level ghost copy with its addresses resolved: dst / src are the
-// element offsets, from the context's arena base, of the cell in slot 0 field
-// 0 of the destination / source block; slot s field v of it lies at
-// + s * pitch + v * stride (elements).
-struct GhostCopy {
-    long long dst, src;
-    int dpitch, dstride, spitch, sstride;
-};
-// Every listed copy (slot `sel` of the source into slot `sel` of the destination).
-cudaError_t launch_ghost_copies(double* arena, const GhostCopy* items, long long nitems, int sel, cudaStream_t stream);
-
 // Constraint monitor (ccz4.cpp:941-1159) over a tile work-list. Writes ham /
 // mom (single-block drop-in; may be null) and per-CTA partial sums of H^2 and
 // |M|^2 to partials[2 * tile] (may be null).
