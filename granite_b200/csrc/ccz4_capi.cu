@@ -206,11 +206,12 @@ struct Ctx {
     int test_withhold = 0;               // armed test switch (StageArgs::test_withhold) of the next rk3_step
     bool ghost_push = false;             // GRANITE_AMR_GHOSTS: stage kernels push same-level ghost copies
     bool overlap_passes = false;         // per-tile precision: FP64 pass beside the FP32 pass (second stream)
-    // every pushing level's same-level ghost copies of slot 0 equal their
-    // sources (after a GRANITE_AMR_GHOSTS coarse step with pushes; cleared by
-    // anything else that writes the state), and, while a coarse step is being
-    // enqueued, the levels that have pushed in it: their fills before a step
-    // need no copies
+    // every level's same-level ghost copies of slot 0 equal their sources except
+    // where a restriction has rewritten a source cell since (after a
+    // GRANITE_AMR_GHOSTS coarse step; cleared by anything else that writes the
+    // state), and, while a coarse step is being enqueued, the levels whose
+    // fill after a step (or whose pushing stages) made them so in it: their
+    // fills before a step copy only the cells of restricted sources
     bool copies_valid = false;
     std::vector<char> step_pushed;
     unsigned long long* d_cmp = nullptr; // granite_ccz4_compare_states results (46 words)
@@ -2127,10 +2128,12 @@ cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long lon
         ++*n;
         if ((e = level_ghost(c, c->levels[L], GHOST_ZERO_GRADIENT_MASKED, 0, X.d_facemask, n))) return e;
     } else {
-        // amr.cpp:319; once this level's stages have pushed its same-level
-        // copies, only those whose source a restriction rewrote are stale
-        const bool fresh = pushes(c, L, mode) && (c->copies_valid || (L < (int)c->step_pushed.size() &&
-                                                                      c->step_pushed[L]));
+        // amr.cpp:319; once the fill after this level's last step (or its pushing
+        // stages) made the same-level copies current, only those whose source a
+        // restriction rewrote since are stale: between that fill and this one
+        // the level's state changed only by restrictions into it
+        const bool fresh = mode == GRANITE_AMR_GHOSTS &&
+                           (c->copies_valid || (L < (int)c->step_pushed.size() && c->step_pushed[L]));
         if ((e = fill_level(c, L, 0, true, mode, n, false, fresh))) return e;
     }
     // TimeIntegrator::sspRK3Step, main.cpp:673-689 (in GRANITE_AMR_GHOSTS the
@@ -2142,7 +2145,7 @@ cudaError_t subcycle(Ctx* c, int L, double dt, int precision, int mode, long lon
     if ((e = fill_level(c, L, 2, false, mode, n, push))) return e;
     if ((e = stage(c, L, precision, 2, 0, 1.0 / 3.0, 2.0 / 3.0, (2.0 / 3.0) * dt, 1, n, push))) return e;
     if ((e = fill_level(c, L, 0, true, mode, n, push))) return e;  // amr.cpp:329
-    if (push && L < (int)c->step_pushed.size()) c->step_pushed[L] = 1;
+    if (mode == GRANITE_AMR_GHOSTS && L < (int)c->step_pushed.size()) c->step_pushed[L] = 1;
     if (hook) c->level_time[L] += dt;                         // amr.cpp:326
     if (L + 1 < (int)c->levels.size()) {
         for (int r = 0; r < 2; ++r) {  // amr.cpp:334-336, :393-397
@@ -2200,8 +2203,8 @@ int granite_ccz4_hierarchy_step(void* h, double dt_coarse, int precision, int am
     for (size_t L = 0; L < c->level_ghosts_valid.size(); ++L) c->level_ghosts_valid[L] = false;
     const bool valid_at_start = c->copies_valid && amr_mode == GRANITE_AMR_GHOSTS;
     c->step_pushed.assign(c->levels.size(), 0);
-    auto finish = [&]() {  // after a coarse step in GRANITE_AMR_GHOSTS with pushes, every copy is current
-        c->copies_valid = amr_mode == GRANITE_AMR_GHOSTS && c->ghost_push;
+    auto finish = [&]() {  // after a GRANITE_AMR_GHOSTS coarse step only copies of restricted cells are stale
+        c->copies_valid = amr_mode == GRANITE_AMR_GHOSTS;
         c->step_pushed.clear();
     };
     if (c->profiling || !c->batched) {

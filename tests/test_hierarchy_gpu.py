@@ -160,13 +160,23 @@ def test_hierarchy_mixed_close_to_fp64(gb, oracle_lib):
         parity(b, a, rtol=1e-5, what="mixed vs fp64")
 
 
-@pytest.mark.parametrize("precision", [0, 1])
-def test_finest_prefill_skip_is_exact(gb, oracle_lib, precision):
+@pytest.mark.parametrize("precision,layout", [(0, "small"), (1, "small"), (0, "tma"), (1, "tma")])
+def test_finest_prefill_skip_is_exact(gb, oracle_lib, precision, layout):
     # the graph-captured step leaves out the fill before the finest level's second
-    # substep (its inputs are those of the fill that ended the first one); the
+    # substep (its inputs are those of the fill that ended the first one), and
+    # once the fill after a level's step has made its same-level copies current,
+    # its fill before the next step copies only cells whose source a restriction
+    # rewrote in between (within a coarse step and across coarse steps); the
     # uncaptured step with the regrid hook (interval 0: no regrid) performs every
-    # fill, as amr.cpp does: the two agree bit for bit
-    h, geoms, levels = small_hierarchy(seed=17, levels=3)
+    # fill in full, as amr.cpp does: the two agree bit for bit
+    if layout == "small":
+        h, geoms, levels = small_hierarchy(seed=17, levels=3)
+    else:  # blocks of 16 to 32 cells (the TMA stage kernel on every level)
+        from granite_b200.hierarchy import make_binary_hierarchy
+        h = make_binary_hierarchy(seed=23, levels=3, coarse_n=48, extent=16.0, sizes=(16, 24, 32),
+                                  blocks_per_level=(8, 40))
+        geoms = [Geom(b.ncells, b.lo, b.hi) for b in h.blocks]
+        levels = [b.level for b in h.blocks]
     states = [oracle.add_noise(oracle_lib.init_brill_lindquist(g, h.masses, h.positions, r_floor=0.5 * g.dx[0]),
                                1e-10, 90 + i) for i, g in enumerate(geoms)]
     dt = 0.25 * geoms[0].dx[0]
@@ -174,7 +184,7 @@ def test_finest_prefill_skip_is_exact(gb, oracle_lib, precision):
     for hooked in (False, True):
         ev, blocks = gpu_hierarchy(gb, geoms, levels, states)
         ev.set_fp64_chi_threshold(0.5)
-        for _ in range(2):
+        for _ in range(3):
             if hooked:
                 ev.hierarchy_step_regrid(dt, None, 0, precision=precision, amr_mode=gb.AMR_GHOSTS)
             else:
