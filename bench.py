@@ -84,18 +84,21 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(workload: str, kernel: str):
-    """dram bytes per stage launch from the committed ncu summary, if any."""
+def ncu_traffic(workload: str, kernel: str, precision: str):
+    """dram bytes per stage launch from the committed ncu summary, if any: the
+    line `traffic_bytes_per_launch_<precision>:`, else `traffic_bytes_per_launch:`."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
     if not os.path.exists(path):
         return None
+    found = {}
     for line in open(path):
-        if line.strip().startswith("traffic_bytes_per_launch:"):
+        key, _, val = line.strip().partition(":")
+        if key.startswith("traffic_bytes_per_launch") and val:
             try:
-                return float(line.split(":", 1)[1].split()[0])
+                found[key] = float(val.split()[0])
             except ValueError:
-                return None
-    return None
+                pass
+    return found.get(f"traffic_bytes_per_launch_{precision}", found.get("traffic_bytes_per_launch"))
 
 
 class Runner:
@@ -406,7 +409,7 @@ def roofline(gb, run: Runner, workload, prof_steps, kernel):
     total_bytes = BYTES_PER_POINT_UPDATE * run.points_per_step * prof_steps
     achieved = total_bytes / (st_ms / 1000.0) / 1e9
     per_launch = total_bytes / max(st_n, 1)
-    traffic = ncu_traffic(workload, kernel)
+    traffic = ncu_traffic(workload, kernel, "mixed" if run.prec == gb.PRECISION_MIXED else "fp64")
     # the bound that applies to this kernel: its FP64 / FP32 pipes (HBM is ~10 % busy)
     fp64_peak = gb.measure_fma_rate(run.ev.params.device, 0)
     fp32_peak = gb.measure_fma_rate(run.ev.params.device, 1)

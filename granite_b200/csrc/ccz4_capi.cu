@@ -1888,13 +1888,13 @@ int build_ghosts_mode(Ctx* c) {
             for (const XferBox& x : res) restricted[L - 1].push_back(x);
         }
     }
-    // The fill before a level step when the pushed copies are current: the
-    // same-level copies whose source cell a restriction into the level can have
-    // changed since the stage that pushed it, and every non-copy ghost cell.
-    // (The restriction itself does not push: like the reference, it leaves the
-    // neighbours' copies of the cells it writes stale until this fill.)
+    // The fill before a level step when the same-level copies are current (the
+    // fill after the level's previous step, or its pushing stages, made them
+    // so): the copies whose source cell a restriction into the level can have
+    // changed since, and every non-copy ghost cell. (The restriction itself
+    // does not push: like the reference, it leaves the neighbours' copies of
+    // the cells it writes stale until this fill.) Built for every level.
     for (size_t L = 0; L < c->levels.size(); ++L) {
-        if (!X[L].push_ok) continue;
         std::map<int, std::vector<char>> mask;  // per block of the level: cells some restriction writes
         for (const XferBox& x : restricted[L]) {
             const auto& d = c->descs[x.dst];
