@@ -455,14 +455,16 @@ def accuracy_run(gb, a: Runner, b: Runner, steps: int, every: int, seconds: floa
     long-term stable) or `seconds` of wall time pass. Reports the comparison
     at the last step where the FP64 state was finite, the largest deviation up
     to there and while ||H||_2 of the FP64 state stayed within 10x of its
-    initial value (the solution still bounded), and a thinned history
-    [step, max_rel_dev, h_l2_ratio, h_l2_fp64]."""
+    initial value (the solution still bounded, with the field and step of that
+    largest deviation), and a thinned history [step, max_rel_dev, field,
+    h_l2_ratio, h_l2_fp64]."""
     for r in (a, b):
         r.ev.upload()
         r.ev.sync()
     h0 = a.ev.constraint_norms(-1)[0]
     last, worst, hist, stop = None, 0.0, [], "steps"
     worst_bounded, bounded_until, still_bounded = 0.0, 0, True
+    worst_bounded_at = (None, None)  # (field, step)
     t0 = time.perf_counter()
     for s in range(1, steps + 1):
         a.step()
@@ -477,11 +479,12 @@ def accuracy_run(gb, a: Runner, b: Runner, steps: int, every: int, seconds: floa
         last = r
         worst = max(worst, r["max_rel_dev"])
         if still_bounded and r["h_l2_fp64"] <= 10.0 * h0:
-            worst_bounded = max(worst_bounded, r["max_rel_dev"])
+            if r["max_rel_dev"] >= worst_bounded:
+                worst_bounded, worst_bounded_at = r["max_rel_dev"], (r["max_rel_dev_field"], s)
             bounded_until = s
         else:
             still_bounded = False
-        hist.append([s, r["max_rel_dev"], r["h_l2_ratio"], r["h_l2_fp64"]])
+        hist.append([s, r["max_rel_dev"], r["max_rel_dev_field"], r["h_l2_ratio"], r["h_l2_fp64"]])
         if time.perf_counter() - t0 > seconds:
             stop = "time cap"
             break
@@ -489,6 +492,8 @@ def accuracy_run(gb, a: Runner, b: Runner, steps: int, every: int, seconds: floa
     out.update({"steps_requested": steps, "check_every": every, "stopped_by": stop,
                 "max_rel_dev_over_run": worst, "h_l2_fp64_initial": h0,
                 "bounded_until_step": bounded_until, "max_rel_dev_while_bounded": worst_bounded,
+                "max_rel_dev_while_bounded_field": worst_bounded_at[0],
+                "max_rel_dev_while_bounded_step": worst_bounded_at[1],
                 "wall_s": time.perf_counter() - t0,
                 "history": hist[:: max(1, len(hist) // 20)] + ([hist[-1]] if hist else [])})
     if stop == "fp64 state non-finite":
