@@ -53,8 +53,10 @@ constexpr int tma_shape_of(int cfg) { return TMA_CFGS[cfg].tz == 4 ? 0 : 1; }
 // Per-tile precision launches of the TMA kernel keep each CTA's selected tiles
 // in shared memory: at most TMA_SEL_CAP per CTA, i.e. ntiles <= grid x TMA_SEL_CAP.
 constexpr int TMA_SEL_CAP = 1024;
-// The persistent grid of a TMA configuration's MIXED RK kernel on the current
-// device (0 before configure_stage_kernels).
+// Grid of the FP64 pass of the per-tile precision, in resident grids.
+constexpr int TMA_FP64_SPREAD = 4;
+// The resident grid of a TMA configuration's per-tile precision passes on the
+// current device, the smaller of the two (0 before configure_stage_kernels).
 int tma_grid(int cfg);
 // Tensor map of one 22-field block buffer (dims x, y, z, field; cells incl.
 // ghosts) with the box of tile depth tz. Returns false when the buffer cannot

@@ -283,7 +283,10 @@ int tma_grid(int cfg) {
     int dev = 0;
     if (cfg < 0 || cfg >= NUM_TMA_CFGS) return 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return 0;
-    return g_tma_grid[dev][cfg][PM_MIXED][EPI_RK][1];
+    // the smaller of the two per-tile passes' resident grids (the FP64 pass may
+    // fit fewer CTAs per SM)
+    const int a = g_tma_grid[dev][cfg][PM_MIXED][EPI_RK][1], b = g_tma_grid[dev][cfg][PM_FP64F][EPI_RK][1];
+    return a < b ? a : b;
 }
 
 static cudaError_t launch_tma(int cfg, int pm, int epi, const DevBlock* blocks, const Tile* tiles, int ntiles,
@@ -294,8 +297,13 @@ static cudaError_t launch_tma(int cfg, int pm, int epi, const DevBlock* blocks, 
     if (e != cudaSuccess) return e;
     const bool sel = args.tile_prec != nullptr;  // per-tile precision passes (RK epilogue)
     if (sel && epi != EPI_RK) return cudaErrorInvalidValue;
-    const int cap = (dev >= 0 && dev < MAX_DEVICES) ? g_tma_grid[dev][cfg][pm][epi][sel ? 1 : 0] : 0;
+    int cap = (dev >= 0 && dev < MAX_DEVICES) ? g_tma_grid[dev][cfg][pm][epi][sel ? 1 : 0] : 0;
     if (cap <= 0) return cudaErrorInvalidConfiguration;  // not instantiated, or configure_stage_kernels() not run
+    // The FP64 pass of the per-tile precision takes few tiles, clustered near the
+    // punctures: TMA_FP64_SPREAD times the resident grid spreads them over more
+    // CTAs (a CTA without selected tiles exits after its scan), so fewer CTAs run
+    // two or more of them one after the other.
+    if (pm == PM_FP64F && sel) cap *= TMA_FP64_SPREAD;
     return g_tma_launch[cfg](pm, epi, sel, blocks, tiles, ntiles, args, stream, ntiles < cap ? ntiles : cap);
 }
 
