@@ -581,10 +581,11 @@ int granite_ccz4_stage_config_info(int cfg, int* tile_z, int* ring_slots, int* s
     return GRANITE_OK;
 }
 
-int granite_ccz4_stage_config_schedule(int cfg, int* warp_specialized, int* ctas_per_sm) {
+int granite_ccz4_stage_config_schedule(int cfg, int* warp_specialized, int* ctas_per_sm, int* items_per_barrier) {
     if (cfg < 0 || cfg >= NUM_TMA_CFGS) return GRANITE_ERR_INVALID;
     if (warp_specialized) *warp_specialized = TMA_CFGS[cfg].ws;
     if (ctas_per_sm) *ctas_per_sm = TMA_CFGS[cfg].minb;
+    if (items_per_barrier) *items_per_barrier = TMA_CFGS[cfg].bar;
     return GRANITE_OK;
 }
 static_assert(GRANITE_STAGE_CONFIGS == NUM_TMA_CFGS, "the header's configuration count");

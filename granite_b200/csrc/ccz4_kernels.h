@@ -38,11 +38,13 @@ int stage_tile_dims(int variant, int cfg, int* tx, int* ty, int* tz);
 struct TmaCfg {
     int tz, nbuf, tin, hs, ws;
     int minb;  // resident CTAs per SM the register allocation is sized for (__launch_bounds__)
+    int bar;   // ring items per CTA barrier (1 or 2; the barrier frees that many slots)
 };
-constexpr int NUM_TMA_CFGS = 8;
-constexpr TmaCfg TMA_CFGS[NUM_TMA_CFGS] = {{4, 3, 0, 0, 0, 1}, {4, 3, 1, 1, 0, 1}, {2, 3, 1, 1, 0, 2},
-                                           {2, 2, 1, 1, 0, 2}, {2, 3, 1, 0, 0, 2}, {2, 3, 0, 0, 1, 2},
-                                           {2, 3, 0, 0, 0, 3}, {2, 2, 1, 0, 0, 3}};
+constexpr int NUM_TMA_CFGS = 11;
+constexpr TmaCfg TMA_CFGS[NUM_TMA_CFGS] = {
+    {4, 3, 0, 0, 0, 1, 1}, {4, 3, 1, 1, 0, 1, 1}, {2, 3, 1, 1, 0, 2, 1}, {2, 2, 1, 1, 0, 2, 1},
+    {2, 3, 1, 0, 0, 2, 1}, {2, 3, 0, 0, 1, 2, 1}, {2, 3, 0, 0, 0, 3, 1}, {2, 2, 1, 0, 0, 3, 1},
+    {2, 3, 1, 0, 0, 2, 2}, {2, 4, 0, 0, 0, 2, 2}, {4, 4, 0, 0, 0, 1, 2}};
 // The box (cells incl. the 4-cell halo) one tensor-map load brings in per
 // field: 24 x 12 x (tz + 8). Tensor maps exist per box shape: shape 0 (tz = 4)
 // and shape 1 (tz = 2).

@@ -7,10 +7,12 @@
 // a stream of items q = (tile round q / NV, field FIELD_ORDER[q % NV]). Item q
 // is one (16 + 8) x (4 + 8) x (TZ + 8)-cell box (the 16 x 4 x TZ tile and its
 // 4-cell halo) of one field, brought into ring slot q % NBUF by a single
-// cp.async.bulk.tensor load that completes on that slot's mbarrier. Thread 0
-// issues item q + NBUF - 1 when the CTA starts on item q, so loads run NBUF - 1
-// fields ahead and across tile boundaries. Rows of 24 doubles put the 16-wide x
-// rows of a warp in distinct shared-memory banks for every stencil offset.
+// cp.async.bulk.tensor load that completes on that slot's mbarrier. Every BAR
+// items (BAR = 1 or 2) the CTA meets at a barrier, after which the slots of
+// the last BAR items are free and thread 0 issues items q + NBUF - BAR ..
+// q + NBUF - 1 into them: loads run NBUF - BAR to NBUF - 1 fields ahead, across
+// tile boundaries. Rows of 24 doubles put the 16-wide x rows of a warp in
+// distinct shared-memory banks for every stencil offset.
 //
 // Options of a configuration:
 //   TIN  every field's centre value is copied from the ring into a per-thread
@@ -23,7 +25,9 @@
 //   MINB resident CTAs per SM that the register allocation is sized for
 //        (__launch_bounds__): 3 CTAs of 128 threads cap a thread at 168
 //        registers, and the ring (with or without TIN) still fits three times in
-//        an SM's shared memory.
+//        an SM's shared memory;
+//   BAR  ring items per CTA barrier: 2 halves the barriers of a tile (22 fields)
+//        at the price of a shallower look-ahead on every other item.
 #pragma once
 
 #include <cstdint>
@@ -35,9 +39,12 @@ namespace granite_b200 {
 
 namespace {
 
-template <int TZ_, int NBUF_, bool TIN_, bool HS_, int MINB_>
+template <int TZ_, int NBUF_, bool TIN_, bool HS_, int MINB_, int BAR_ = 1>
 struct TmaCfgT {
-    static constexpr int TZ = TZ_, NBUF = NBUF_;
+    static constexpr int TZ = TZ_, NBUF = NBUF_, BAR = BAR_;
+    // a tile round's first item starts a barrier group (the round's shared push
+    // boxes rely on it), and at least one item is loaded ahead
+    static_assert((BAR == 1 || BAR == 2) && NV % BAR == 0 && NBUF > BAR, "barrier grouping");
     static constexpr bool TIN = TIN_, HS = HS_;
     static constexpr int TX = 16, TY = 4, NT = TX * TY * TZ;
     static constexpr int MINB = MINB_;  // resident CTAs per SM asked of the register allocator
@@ -177,12 +184,17 @@ struct TmaSource {
             }
         }
     }
-    // Every thread of the CTA calls der() for every item in order (the call
-    // carries the CTA barrier that frees the slot the next load overwrites).
+    // Every thread of the CTA calls der() for every item in order (every BAR-th
+    // call carries the CTA barrier that frees the slots of the last BAR items,
+    // which the next BAR loads overwrite).
     template <bool HESS, bool EXACT, typename P>
     __device__ __forceinline__ FieldDer<P> der(int v, const double beta[3], P w) {
-        __syncthreads();
-        if (threadIdx.x == 0 && !failed) issue(next + C::NBUF - 1);
+        if (next % C::BAR == 0) {
+            __syncthreads();
+            if (threadIdx.x == 0 && !failed)
+#pragma unroll
+                for (int j = C::NBUF - C::BAR; j < C::NBUF; ++j) issue(next + j);
+        }
         wait(next);
         const double* box = ring + (size_t)(next % C::NBUF) * C::BOX + lin;
         if constexpr (C::TIN) tin[v * NT] = box[0];
@@ -253,7 +265,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
                         tin, hs, nullptr, (lx + 4) + C::BX * ((ly + 4) + C::BY * (lz + 4)), 0, false,
                         A.errflag, 0, A.test_withhold};
     if (tid == 0)
-        for (int q = 0; q < C::NBUF - 1; ++q) S.issue(q);
+        for (int q = 0; q < C::NBUF - C::BAR; ++q) S.issue(q);
     for (int r = 0;; ++r) {
         const int ti = S.round_tile(r);
         if (ti >= ntiles) break;
@@ -304,12 +316,13 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     // Every issued item was consumed (issue() skips items past this CTA's last
     // tile), so no copy into the ring is in flight when the CTA exits. If
     // thread 0 gave up waiting at item f (which already had its full wait), it
-    // had issued items up to f + NBUF - 1 and nothing after: each of
-    // f + 1 .. f + NBUF - 1 that was issued gets its own bounded wait, whatever
-    // the others do, so no copy into this CTA's shared memory outlives it.
+    // had issued items up to f0 + NBUF - 1 (f0 = f rounded down to its barrier
+    // group) and nothing after: each of f + 1 .. f0 + NBUF - 1 that was issued
+    // gets its own bounded wait, whatever the others do, so no copy into this
+    // CTA's shared memory outlives it.
     if (S.failed && tid == 0) {
         const int f = S.fail_q;
-        for (int q = f + 1; q < f + C::NBUF; ++q) {
+        for (int q = f + 1; q < f - f % C::BAR + C::NBUF; ++q) {
             if (S.round_tile(q / NV) >= ntiles) continue;
             S.failed = false;
             S.wait(q);
@@ -379,7 +392,8 @@ struct TmaConfigOps {
 #define GRANITE_TMA_CFG_UNIT(K, STORE)                                                                               \
     namespace granite_b200 {                                                                                         \
     using TmaCfg##K =                                                                                                \
-        TmaCfgT<TMA_CFGS[K].tz, TMA_CFGS[K].nbuf, TMA_CFGS[K].tin != 0, TMA_CFGS[K].hs != 0, TMA_CFGS[K].minb>;      \
+        TmaCfgT<TMA_CFGS[K].tz, TMA_CFGS[K].nbuf, TMA_CFGS[K].tin != 0, TMA_CFGS[K].hs != 0, TMA_CFGS[K].minb,      \
+                TMA_CFGS[K].bar>;                                                                                    \
     cudaError_t configure_tma_cfg##K(int nsm, int grids[3][2][2]) {                                                  \
         return TmaConfigOps<TmaCfg##K>::configure<STORE>(nsm, grids);                                                \
     }                                                                                                                \

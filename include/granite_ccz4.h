@@ -405,7 +405,7 @@ GRANITE_API int granite_ccz4_get_kernel_variant(const void* ctx, int* variant);
  * writes a table a caller can apply). A level's blocks of different
  * configurations run as one launch per configuration. Set before commit.
  * All configurations compute identical FP64 results. */
-#define GRANITE_STAGE_CONFIGS 8
+#define GRANITE_STAGE_CONFIGS 11
 #define GRANITE_STAGE_CLASSES 6
 #define GRANITE_STAGE_CLASS_EDGES 16, 24, 32, 48, 64, 96
 /* cls: class index (0 .. GRANITE_STAGE_CLASSES - 1) or -1 for every class;
@@ -418,8 +418,11 @@ GRANITE_API int granite_ccz4_stage_config_info(int cfg, int* tile_z, int* ring_s
                                                int* shared_hessian);
 /* The schedule of a configuration: warp_specialized = 1 when the mixed RK
  * kernels split stencil and algebra warps; ctas_per_sm = the resident CTAs per
- * SM its register allocation is sized for (3: at most 168 registers a thread). */
-GRANITE_API int granite_ccz4_stage_config_schedule(int cfg, int* warp_specialized, int* ctas_per_sm);
+ * SM its register allocation is sized for (3: at most 168 registers a thread);
+ * items_per_barrier = field boxes consumed per CTA barrier (1 or 2). Null
+ * outputs are skipped. */
+GRANITE_API int granite_ccz4_stage_config_schedule(int cfg, int* warp_specialized, int* ctas_per_sm,
+                                                   int* items_per_barrier);
 GRANITE_API int granite_ccz4_block_stage_class(const granite_block_desc* b, int* cls);
 
 /* Test switch of the wait limit above (no counterpart in the reference, which

@@ -245,6 +245,7 @@ def test_stage_configs_and_classes_without_a_device():
         assert info["tile"][:2] == (16, 4) and info["tile"][2] in (2, 4)
         assert info["ring_slots"] in (2, 3, 4)
         assert info["ctas_per_sm"] in (1, 2, 3)
+        assert info["items_per_barrier"] in (1, 2) and info["ring_slots"] > info["items_per_barrier"]
         if info["ctas_per_sm"] == 3:
             # the ring and the stage-input column of one CTA fit three times in
             # an SM's 228 KB of shared memory (with 7.5 KB per CTA for static
@@ -254,6 +255,7 @@ def test_stage_configs_and_classes_without_a_device():
             dyn += 22 * nt * 8 if info["shared_input"] else 0
             assert not info["shared_hessian"] and 3 * (dyn + 7680) <= 228 * 1024, (k, info)
     assert [gb.stage_config_info(k)["ctas_per_sm"] for k in (6, 7)] == [3, 3]
+    assert [gb.stage_config_info(k)["items_per_barrier"] for k in range(gb.STAGE_CONFIGS)] == [1] * 8 + [2] * 3
     with pytest.raises(gb.GraniteError):
         gb.stage_config_info(gb.STAGE_CONFIGS)
     assert [gb.block_stage_class((e, e, e)) for e in gb.STAGE_CLASS_EDGES] == list(range(6))

@@ -25,7 +25,7 @@ from test_parity_gpu import parity
 
 pytestmark = pytest.mark.gpu
 
-CONFIGS = [0, 1, 2, 3, 4, 5, 6, 7]
+CONFIGS = list(range(11))
 
 
 @pytest.fixture(scope="module")
