@@ -17,7 +17,8 @@ runs one launch per configuration, and on hierarchies of mixed block sizes the
 extra launch tails cost more than the per-class gains, so the library's
 built-in default is the uniform table this module produced on a B200.
 
-    python -m granite_b200.tuner [--out table.json] [--classes 16,24] [--steps 3]
+    python -m granite_b200.tuner [--out table.json] [--classes 16,24] [--configs 0,4] [--precisions mixed]
+                                 [--steps 3]
 """
 from __future__ import annotations
 
@@ -139,13 +140,17 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--out", default=None, help="write the result (JSON) here")
     ap.add_argument("--classes", default=None, help="comma-separated class edges (default: all)")
+    ap.add_argument("--configs", default=None, help="comma-separated configurations (default: all)")
+    ap.add_argument("--precisions", default="fp64,mixed", help="comma-separated: fp64, mixed")
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--fp64-chi", type=float, default=0.5)
     ap.add_argument("--device", type=int, default=0)
     args = ap.parse_args(argv)
     classes = [int(x) for x in args.classes.split(",")] if args.classes else None
-    res = tune(classes=classes, steps=args.steps, fp64_chi=args.fp64_chi, device=args.device,
-               log=lambda m: print(m, file=sys.stderr, flush=True))
+    configs = [int(x) for x in args.configs.split(",")] if args.configs else None
+    precisions = tuple(x for x in args.precisions.split(",") if x)
+    res = tune(classes=classes, configs=configs, precisions=precisions, steps=args.steps, fp64_chi=args.fp64_chi,
+               device=args.device, log=lambda m: print(m, file=sys.stderr, flush=True))
     try:
         import torch
         res["device_name"] = torch.cuda.get_device_name(args.device)
