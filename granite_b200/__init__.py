@@ -34,7 +34,7 @@ KERNEL_STAGE, KERNEL_GHOST, KERNEL_TRANSFER, KERNEL_CONSTRAINTS = 0, 1, 2, 3
 VARIANT_GLOBAL, VARIANT_SMEM, VARIANT_GLOBAL_R168, VARIANT_GLOBAL_R128, VARIANT_TMA = 0, 1, 2, 3, 4
 VARIANT_NAMES = {"global": 0, "smem": 1, "global_r168": 2, "global_r128": 3, "tma": 4}
 # configurations of the TMA stage kernel and the block-size classes they are tuned for
-STAGE_CONFIGS = 11
+STAGE_CONFIGS = 12
 STAGE_CLASS_EDGES = (16, 24, 32, 48, 64, 96)
 
 _ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "no sm_100 device", -4: "out of memory",
@@ -161,7 +161,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
     lib.granite_ccz4_get_stage_config.argtypes = [vp, C.c_int, C.c_int, ip_]
     lib.granite_ccz4_force_stage_config.argtypes = [vp, C.c_int]
     lib.granite_ccz4_stage_config_info.argtypes = [C.c_int, ip_, ip_, ip_, ip_]
-    lib.granite_ccz4_stage_config_schedule.argtypes = [C.c_int, ip_, ip_, ip_]
+    lib.granite_ccz4_stage_config_schedule.argtypes = [C.c_int, ip_, ip_, ip_, ip_]
     lib.granite_ccz4_block_stage_class.argtypes = [C.POINTER(_BlockDesc), ip_]
     lib.granite_ccz4_compare_states.argtypes = [vp, vp, dp, dp, C.POINTER(C.c_longlong)]
     _LIB = lib
@@ -185,11 +185,11 @@ def stage_config_info(cfg: int) -> dict:
     rc = lib.granite_ccz4_stage_config_info(int(cfg), *[C.byref(x) for x in v])
     if rc != GRANITE_OK:
         raise GraniteError(rc, f"unknown stage configuration {cfg}")
-    w = [C.c_int() for _ in range(3)]
+    w = [C.c_int() for _ in range(4)]
     lib.granite_ccz4_stage_config_schedule(int(cfg), *[C.byref(x) for x in w])
     return {"tile": (16, 4, v[0].value), "ring_slots": v[1].value, "shared_input": bool(v[2].value),
             "shared_hessian": bool(v[3].value), "warp_specialized": bool(w[0].value), "ctas_per_sm": w[1].value,
-            "items_per_barrier": w[2].value}
+            "items_per_barrier": w[2].value, "x_remainder_tiles": bool(w[3].value)}
 
 
 def block_stage_class(ncells) -> int:

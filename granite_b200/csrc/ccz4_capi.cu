@@ -341,9 +341,17 @@ void tiles_of(int block, const granite_block_desc& b, std::vector<Tile>& out, in
         TY = 128 / w;
         TZ = 1;
     }
+    // TMA x-remainder tiles: a block whose x extent is TMA_REM_X more than a
+    // multiple of 16 covers its last TMA_REM_X columns with TMA_REM_X x TY x 2 TZ
+    // tiles (Tile::w = -TMA_REM_X), each after the full tiles of its rows
+    const bool rem = variant == VARIANT_TMA && !adaptive && cfg >= 0 && cfg < NUM_TMA_CFGS && TMA_CFGS[cfg].rem &&
+                     b.ncells[0] % TX == TMA_REM_X;
+    const int nx = rem ? b.ncells[0] - TMA_REM_X : b.ncells[0];
     for (int k = 0; k < b.ncells[2]; k += TZ)
-        for (int j = 0; j < b.ncells[1]; j += TY)
-            for (int i = 0; i < b.ncells[0]; i += TX) out.push_back(Tile{block, i, j, k, w});
+        for (int j = 0; j < b.ncells[1]; j += TY) {
+            for (int i = 0; i < nx; i += TX) out.push_back(Tile{block, i, j, k, w});
+            if (rem && k % (2 * TZ) == 0) out.push_back(Tile{block, nx, j, k, -TMA_REM_X});
+        }
 }
 
 // Block-size class of a block for the per-class stage configuration: the class
@@ -581,11 +589,13 @@ int granite_ccz4_stage_config_info(int cfg, int* tile_z, int* ring_slots, int* s
     return GRANITE_OK;
 }
 
-int granite_ccz4_stage_config_schedule(int cfg, int* warp_specialized, int* ctas_per_sm, int* items_per_barrier) {
+int granite_ccz4_stage_config_schedule(int cfg, int* warp_specialized, int* ctas_per_sm, int* items_per_barrier,
+                                       int* x_remainder_tiles) {
     if (cfg < 0 || cfg >= NUM_TMA_CFGS) return GRANITE_ERR_INVALID;
     if (warp_specialized) *warp_specialized = TMA_CFGS[cfg].ws;
     if (ctas_per_sm) *ctas_per_sm = TMA_CFGS[cfg].minb;
     if (items_per_barrier) *items_per_barrier = TMA_CFGS[cfg].bar;
+    if (x_remainder_tiles) *x_remainder_tiles = TMA_CFGS[cfg].rem;
     return GRANITE_OK;
 }
 static_assert(GRANITE_STAGE_CONFIGS == NUM_TMA_CFGS, "the header's configuration count");
@@ -1405,8 +1415,10 @@ static cudaError_t stage_range(Ctx* c, LevelLists& L, int cfg, int precision, co
                                int count, long long* n) {
     const Tile* tiles = L.d_tiles + first;
     StageArgs a = a0;
-    if (L.variant == VARIANT_TMA)  // the tensor maps of this configuration's box shape
+    if (L.variant == VARIANT_TMA) {  // the tensor maps of this configuration's box shape(s)
         a.tmaps = c->d_tmaps + (size_t)tma_shape_of(cfg) * 3 * c->descs.size();
+        a.tmaps_rem = TMA_CFGS[cfg].rem ? c->d_tmaps + (size_t)TMA_REM_SHAPE * 3 * c->descs.size() : nullptr;
+    }
     if (a.tile_push) a.tile_push += first;  // indexed like the launch's tiles
     // (the TMA kernel keeps a CTA's selected tiles in shared memory: bounded count)
     const bool split = precision == GRANITE_PRECISION_MIXED && c->fp64_chi > 0.0 &&
@@ -1827,12 +1839,14 @@ int build_ghosts_mode(Ctx* c) {
                         for (int t = g.first; t < g.first + g.count; ++t) {
                             const Tile& tl = ll.h_tiles[t];
                             const int t0[3] = {tl.i0, tl.j0, tl.k0};
+                            const int rdim[3] = {TMA_REM_X, TY, 2 * TZ};  // x-remainder tiles
+                            const int* tdim_t = tl.w < 0 ? rdim : tdim;
                             const int first = (int)plist.size();
                             auto it = by_src.find(tl.block);
                             if (it != by_src.end())
                                 for (const PushBox& pb : it->second) {
                                     bool hit = true;
-                                    for (int d = 0; d < 3 && hit; ++d) hit = pb.lo[d] < t0[d] + tdim[d] && pb.hi[d] > t0[d];
+                                    for (int d = 0; d < 3 && hit; ++d) hit = pb.lo[d] < t0[d] + tdim_t[d] && pb.hi[d] > t0[d];
                                     if (hit) plist.push_back(pb);
                                 }
                             tp[t] = make_int2(first, (int)plist.size() - first);

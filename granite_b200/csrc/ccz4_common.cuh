@@ -43,7 +43,8 @@ struct Tile {
     int block;
     int i0, j0, k0;  // interior-relative origin of the tile
     int w;           // tile width along x for the global-load stage kernels (32, 16 or 8;
-                     // 128 threads cover w x 128/w points); 0 for fixed-shape kernels
+                     // 128 threads cover w x 128/w points); 0 for fixed-shape kernels;
+                     // -8 for an x-remainder tile of the TMA kernel (8 x 4 x 2 tz points)
 };
 
 // Interior cells of a source block that are ghost cells of a same-level
@@ -80,6 +81,7 @@ struct StageArgs {
     const double* rho; const double* Si; const double* Sij; const double* S;
     unsigned long long* nonfinite;  // floor hits on non-finite chi/alpha (nullable)
     const void* tmaps;     // TMA variant: CUtensorMap of (block b, slot s) at tmaps[3 b + s]
+    const void* tmaps_rem; // TMA variant with x-remainder tiles: the same for their box shape
     unsigned int* errflag; // TMA variant: set to 1 when a bounded mbarrier wait gives up (nullable)
     // Per-tile precision (nullable): the launch covers only tiles ti with tile_prec[ti] == want_prec.
     const unsigned char* tile_prec;

@@ -39,12 +39,20 @@ struct TmaCfg {
     int tz, nbuf, tin, hs, ws;
     int minb;  // resident CTAs per SM the register allocation is sized for (__launch_bounds__)
     int bar;   // ring items per CTA barrier (1 or 2; the barrier frees that many slots)
+    // x-remainder tiles (tz = 2 only): a block whose x extent leaves 8 cells
+    // after its 16-wide tiles covers them with 8 x 4 x 4 tiles (Tile::w = -8,
+    // the 128 threads all on points) loaded with the 24 x 12 x 12 box shape,
+    // instead of 16-wide tiles half outside the block
+    int rem;
 };
-constexpr int NUM_TMA_CFGS = 11;
+constexpr int NUM_TMA_CFGS = 12;
 constexpr TmaCfg TMA_CFGS[NUM_TMA_CFGS] = {
-    {4, 3, 0, 0, 0, 1, 1}, {4, 3, 1, 1, 0, 1, 1}, {2, 3, 1, 1, 0, 2, 1}, {2, 2, 1, 1, 0, 2, 1},
-    {2, 3, 1, 0, 0, 2, 1}, {2, 3, 0, 0, 1, 2, 1}, {2, 3, 0, 0, 0, 3, 1}, {2, 2, 1, 0, 0, 3, 1},
-    {2, 3, 1, 0, 0, 2, 2}, {2, 4, 0, 0, 0, 2, 2}, {4, 4, 0, 0, 0, 1, 2}};
+    {4, 3, 0, 0, 0, 1, 1, 0}, {4, 3, 1, 1, 0, 1, 1, 0}, {2, 3, 1, 1, 0, 2, 1, 0}, {2, 2, 1, 1, 0, 2, 1, 0},
+    {2, 3, 1, 0, 0, 2, 1, 0}, {2, 3, 0, 0, 1, 2, 1, 0}, {2, 3, 0, 0, 0, 3, 1, 0}, {2, 2, 1, 0, 0, 3, 1, 0},
+    {2, 3, 1, 0, 0, 2, 2, 0}, {2, 4, 0, 0, 0, 2, 2, 0}, {4, 4, 0, 0, 0, 1, 2, 0}, {2, 3, 1, 0, 0, 2, 1, 1}};
+// Points of an x-remainder tile along x, and the box shape that loads it.
+constexpr int TMA_REM_X = 8;
+constexpr int TMA_REM_SHAPE = 0;
 // The box (cells incl. the 4-cell halo) one tensor-map load brings in per
 // field: 24 x 12 x (tz + 8). Tensor maps exist per box shape: shape 0 (tz = 4)
 // and shape 1 (tz = 2).

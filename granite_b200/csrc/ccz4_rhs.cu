@@ -194,7 +194,9 @@ __global__ void __launch_bounds__(128)
     const int ti = first + blockIdx.x;
     const Tile t = tiles[ti];
     const DevBlock& B = blocks[t.block];
-    const int w = t.w > 0 ? t.w : tx, h = t.w > 0 ? 128 / t.w : ty, d = t.w > 0 ? 1 : tz;
+    // global-load tiles: w x 128/w x 1; TMA x-remainder tiles (w < 0): -w x ty x 2 tz
+    const int w = t.w > 0 ? t.w : (t.w < 0 ? -t.w : tx), h = t.w > 0 ? 128 / t.w : ty,
+              d = t.w > 0 ? 1 : (t.w < 0 ? 2 * tz : tz);
     const double* chi = B.buf[sel] + (long long)CHI * B.stride;
     bool low = false;
     for (int p = threadIdx.x; p < w * h * d; p += blockDim.x) {
@@ -263,6 +265,7 @@ cudaError_t configure_tma_cfg7(int, int[3][2][2]);
 cudaError_t configure_tma_cfg8(int, int[3][2][2]);
 cudaError_t configure_tma_cfg9(int, int[3][2][2]);
 cudaError_t configure_tma_cfg10(int, int[3][2][2]);
+cudaError_t configure_tma_cfg11(int, int[3][2][2]);
 cudaError_t launch_tma_cfg0(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
 cudaError_t launch_tma_cfg1(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
 cudaError_t launch_tma_cfg2(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
@@ -274,13 +277,15 @@ cudaError_t launch_tma_cfg7(int, int, bool, const DevBlock*, const Tile*, int, c
 cudaError_t launch_tma_cfg8(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
 cudaError_t launch_tma_cfg9(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
 cudaError_t launch_tma_cfg10(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
-static_assert(NUM_TMA_CFGS == 11, "one configure / launch pair per TMA configuration");
+cudaError_t launch_tma_cfg11(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
+static_assert(NUM_TMA_CFGS == 12, "one configure / launch pair per TMA configuration");
 static const TmaConfigure g_tma_configure[NUM_TMA_CFGS] = {
     configure_tma_cfg0, configure_tma_cfg1, configure_tma_cfg2, configure_tma_cfg3, configure_tma_cfg4, configure_tma_cfg5,
-    configure_tma_cfg6, configure_tma_cfg7, configure_tma_cfg8, configure_tma_cfg9, configure_tma_cfg10};
+    configure_tma_cfg6, configure_tma_cfg7, configure_tma_cfg8, configure_tma_cfg9, configure_tma_cfg10,
+    configure_tma_cfg11};
 static const TmaLaunch g_tma_launch[NUM_TMA_CFGS] = {
     launch_tma_cfg0, launch_tma_cfg1, launch_tma_cfg2, launch_tma_cfg3, launch_tma_cfg4, launch_tma_cfg5,
-    launch_tma_cfg6, launch_tma_cfg7, launch_tma_cfg8, launch_tma_cfg9, launch_tma_cfg10};
+    launch_tma_cfg6, launch_tma_cfg7, launch_tma_cfg8, launch_tma_cfg9, launch_tma_cfg10, launch_tma_cfg11};
 
 // Persistent grid of each TMA configuration on each device: SMs x resident CTAs.
 constexpr int MAX_DEVICES = 64;
@@ -299,6 +304,7 @@ int tma_grid(int cfg) {
 static cudaError_t launch_tma(int cfg, int pm, int epi, const DevBlock* blocks, const Tile* tiles, int ntiles,
                               const StageArgs& args, cudaStream_t stream) {
     if (!args.tmaps || cfg < 0 || cfg >= NUM_TMA_CFGS || pm < 0 || pm > 2) return cudaErrorInvalidValue;
+    if (TMA_CFGS[cfg].rem && !args.tmaps_rem) return cudaErrorInvalidValue;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;

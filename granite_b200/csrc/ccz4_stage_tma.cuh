@@ -39,22 +39,29 @@ namespace granite_b200 {
 
 namespace {
 
-template <int TZ_, int NBUF_, bool TIN_, bool HS_, int MINB_, int BAR_ = 1>
+template <int TZ_, int NBUF_, bool TIN_, bool HS_, int MINB_, int BAR_ = 1, bool REM_ = false>
 struct TmaCfgT {
     static constexpr int TZ = TZ_, NBUF = NBUF_, BAR = BAR_;
     // a tile round's first item starts a barrier group (the round's shared push
     // boxes rely on it), and at least one item is loaded ahead
     static_assert((BAR == 1 || BAR == 2) && NV % BAR == 0 && NBUF > BAR, "barrier grouping");
-    static constexpr bool TIN = TIN_, HS = HS_;
+    static constexpr bool TIN = TIN_, HS = HS_, REM = REM_;
     static constexpr int TX = 16, TY = 4, NT = TX * TY * TZ;
     static constexpr int MINB = MINB_;  // resident CTAs per SM asked of the register allocator
     static constexpr int BX = TX + 8, BY = TY + 8, BZ = TZ + 8;
     static constexpr int BOX = BX * BY * BZ;
     static constexpr unsigned BYTES = BOX * sizeof(double);  // complete_tx count of one item
-    static_assert(BYTES % 128 == 0, "slots stay 128-byte aligned");
+    // x-remainder tiles: TMA_REM_X x TY x 2 TZ points, the same rows (BX, BY) and
+    // 2 TZ + 8 planes per box, so the stencil offsets stay those of the full tiles
+    static_assert(!REM || (TZ == 2 && TMA_SHAPE_TZ[TMA_REM_SHAPE] == 2 * TZ && TMA_REM_X * TY * 2 * TZ == NT),
+                  "remainder tiles: 8 x 4 x 4 points in the tz = 4 box shape");
+    static constexpr int BOX_REM = BX * BY * (2 * TZ + 8);
+    static constexpr unsigned BYTES_REM = BOX_REM * sizeof(double);
+    static constexpr int SLOT = REM ? BOX_REM : BOX;  // doubles per ring slot
+    static_assert(BYTES % 128 == 0 && (SLOT * sizeof(double)) % 128 == 0, "slots stay 128-byte aligned");
     static_assert(BX == TMA_BOX_X && BY == TMA_BOX_Y, "box = tile + halo");
     // dynamic shared memory: ring | mbarriers | stage-input column | Hessian slots
-    static constexpr size_t OFF_BAR = (size_t)NBUF * BYTES;
+    static constexpr size_t OFF_BAR = (size_t)NBUF * SLOT * sizeof(double);
     static constexpr size_t OFF_TIN = (OFF_BAR + NBUF * sizeof(unsigned long long) + 127) / 128 * 128;
     static constexpr size_t OFF_HS = OFF_TIN + (TIN ? (size_t)NV * NT * sizeof(double) : 0);
     template <typename P>
@@ -131,8 +138,9 @@ struct TmaSource {
     const DevBlock* blocks;
     const Tile* tiles;
     const unsigned char* maps;  // CUtensorMap array of this box shape, 128 bytes each
+    const unsigned char* maps_rem;  // REM: the same for the remainder tiles' box shape
     int ntiles, in_sel;
-    double* ring;      // NBUF slots of C::BOX doubles
+    double* ring;      // NBUF slots of C::SLOT doubles
     unsigned bar0;     // shared address of the slot mbarriers (8 bytes apart)
     double* tin;       // TIN: this thread's stage-input column (field v at tin[v * NT])
     void* hs;          // HS: this thread's Hessian-loop column (slot q at hs[q * NT])
@@ -162,12 +170,13 @@ struct TmaSource {
         if (ti >= ntiles) return;
         if (withhold != 0 && q == withhold - 1 && blockIdx.x == 0) return;  // test switch: never issued
         const Tile t = tiles[ti];
+        const bool rem = C::REM && t.w < 0;
         const int s = q % C::NBUF;
         const unsigned bar = bar0 + 8u * s;
-        mbar_expect_tx(bar, C::BYTES);
+        mbar_expect_tx(bar, rem ? C::BYTES_REM : C::BYTES);
         // box origin = tile origin - 4 cells = interior index (cells incl. ghosts start 4 lower)
-        tma_load_box(smem_addr(ring + (size_t)s * C::BOX), maps + (size_t)(3 * t.block + in_sel) * 128, t.i0,
-                     t.j0, t.k0, FIELD_ORDER[q % NV], bar);
+        tma_load_box(smem_addr(ring + (size_t)s * C::SLOT), (rem ? maps_rem : maps) + (size_t)(3 * t.block + in_sel) * 128,
+                     t.i0, t.j0, t.k0, FIELD_ORDER[q % NV], bar);
     }
     __device__ __forceinline__ void wait(int q) {
         if (failed) return;
@@ -196,7 +205,7 @@ struct TmaSource {
                 for (int j = C::NBUF - C::BAR; j < C::NBUF; ++j) issue(next + j);
         }
         wait(next);
-        const double* box = ring + (size_t)(next % C::NBUF) * C::BOX + lin;
+        const double* box = ring + (size_t)(next % C::NBUF) * C::SLOT + lin;
         if constexpr (C::TIN) tin[v * NT] = box[0];
         const SharedLoad L{box};
         ++next;
@@ -258,12 +267,24 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     // the round starts, read in its epilogue (the round's first field barrier
     // lies between), overwritten two rounds later
     __shared__ PushBox s_push[2][PUSH_STAGE_MAX];
-    const int lx = tid % C::TX, ly = (tid / C::TX) % C::TY, lz = tid / (C::TX * C::TY);
+    // this thread's point within a tile: 16 x 4 x TZ, or TMA_REM_X x 4 x 2 TZ
+    // for an x-remainder tile (the box rows are the same, so is the stencil code)
+    auto local = [&](const Tile& t, int& px, int& py, int& pz) {
+        if (C::REM && t.w < 0) {
+            px = tid % TMA_REM_X;
+            py = (tid / TMA_REM_X) % C::TY;
+            pz = tid / (TMA_REM_X * C::TY);
+        } else {
+            px = tid % C::TX;
+            py = (tid / C::TX) % C::TY;
+            pz = tid / (C::TX * C::TY);
+        }
+    };
     double* tin = C::TIN ? reinterpret_cast<double*>(base + C::OFF_TIN) + tid : nullptr;
     void* hs = C::HS ? static_cast<void*>(reinterpret_cast<P*>(base + C::OFF_HS) + tid) : nullptr;
-    TmaSource<C, SEL> S{blocks, tiles, static_cast<const unsigned char*>(A.tmaps), ntiles, A.in_sel, ring, bar0,
-                        tin, hs, nullptr, (lx + 4) + C::BX * ((ly + 4) + C::BY * (lz + 4)), 0, false,
-                        A.errflag, 0, A.test_withhold};
+    TmaSource<C, SEL> S{blocks, tiles, static_cast<const unsigned char*>(A.tmaps),
+                        static_cast<const unsigned char*>(A.tmaps_rem), ntiles, A.in_sel, ring, bar0,
+                        tin, hs, nullptr, 0, 0, false, A.errflag, 0, A.test_withhold};
     if (tid == 0)
         for (int q = 0; q < C::NBUF - C::BAR; ++q) S.issue(q);
     for (int r = 0;; ++r) {
@@ -272,6 +293,9 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         const Tile t = tiles[ti];
         const DevBlock& B = blocks[t.block];
         S.B = &B;
+        int lx, ly, lz;
+        local(t, lx, ly, lz);
+        S.lin = (lx + 4) + C::BX * ((ly + 4) + C::BY * (lz + 4));
         const int i = t.i0 + lx, j = t.j0 + ly, k = t.k0 + lz;
         const bool valid = i < B.n[0] && j < B.n[1] && k < B.n[2];
         // pointwise loads of threads outside the block use a valid cell; their results are dropped
@@ -302,8 +326,10 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
             if (tn < ntiles) {
                 const Tile t2 = tiles[tn];
                 const DevBlock& B2 = blocks[t2.block];
-                const long long c2 = cell_index(B2, min(t2.i0 + lx, B2.n[0] - 1) + NG, min(t2.j0 + ly, B2.n[1] - 1) + NG,
-                                                min(t2.k0 + lz, B2.n[2] - 1) + NG);
+                int x2, y2, z2;
+                local(t2, x2, y2, z2);
+                const long long c2 = cell_index(B2, min(t2.i0 + x2, B2.n[0] - 1) + NG, min(t2.j0 + y2, B2.n[1] - 1) + NG,
+                                                min(t2.k0 + z2, B2.n[2] - 1) + NG);
                 const double* u2 = B2.buf[A.in_sel] + c2;
 #pragma unroll
                 for (int v = 0; v < NV; ++v) prefetch_l2(u2 + (long long)v * B2.stride);
@@ -393,7 +419,7 @@ struct TmaConfigOps {
     namespace granite_b200 {                                                                                         \
     using TmaCfg##K =                                                                                                \
         TmaCfgT<TMA_CFGS[K].tz, TMA_CFGS[K].nbuf, TMA_CFGS[K].tin != 0, TMA_CFGS[K].hs != 0, TMA_CFGS[K].minb,      \
-                TMA_CFGS[K].bar>;                                                                                    \
+                TMA_CFGS[K].bar, TMA_CFGS[K].rem != 0>;                                                              \
     cudaError_t configure_tma_cfg##K(int nsm, int grids[3][2][2]) {                                                  \
         return TmaConfigOps<TmaCfg##K>::configure<STORE>(nsm, grids);                                                \
     }                                                                                                                \

@@ -405,7 +405,7 @@ GRANITE_API int granite_ccz4_get_kernel_variant(const void* ctx, int* variant);
  * writes a table a caller can apply). A level's blocks of different
  * configurations run as one launch per configuration. Set before commit.
  * All configurations compute identical FP64 results. */
-#define GRANITE_STAGE_CONFIGS 11
+#define GRANITE_STAGE_CONFIGS 12
 #define GRANITE_STAGE_CLASSES 6
 #define GRANITE_STAGE_CLASS_EDGES 16, 24, 32, 48, 64, 96
 /* cls: class index (0 .. GRANITE_STAGE_CLASSES - 1) or -1 for every class;
@@ -419,10 +419,12 @@ GRANITE_API int granite_ccz4_stage_config_info(int cfg, int* tile_z, int* ring_s
 /* The schedule of a configuration: warp_specialized = 1 when the mixed RK
  * kernels split stencil and algebra warps; ctas_per_sm = the resident CTAs per
  * SM its register allocation is sized for (3: at most 168 registers a thread);
- * items_per_barrier = field boxes consumed per CTA barrier (1 or 2). Null
- * outputs are skipped. */
+ * items_per_barrier = field boxes consumed per CTA barrier (1 or 2);
+ * x_remainder_tiles = 1 when a block whose x extent is 8 more than a multiple
+ * of 16 covers its last 8 columns with 8 x 4 x 4 tiles instead of 16-wide tiles
+ * half outside the block. Null outputs are skipped. */
 GRANITE_API int granite_ccz4_stage_config_schedule(int cfg, int* warp_specialized, int* ctas_per_sm,
-                                                   int* items_per_barrier);
+                                                   int* items_per_barrier, int* x_remainder_tiles);
 GRANITE_API int granite_ccz4_block_stage_class(const granite_block_desc* b, int* cls);
 
 /* Test switch of the wait limit above (no counterpart in the reference, which

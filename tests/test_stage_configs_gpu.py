@@ -25,7 +25,7 @@ from test_parity_gpu import parity
 
 pytestmark = pytest.mark.gpu
 
-CONFIGS = list(range(11))
+CONFIGS = list(range(12))
 
 
 @pytest.fixture(scope="module")
@@ -36,7 +36,8 @@ def gb():
 
 @pytest.fixture(scope="module")
 def case(oracle_lib):
-    # partial tiles in x (40 = 16 + 16 + 8), y (22) and z (18 = 4 x 4 + 2 / 9 x 2)
+    # partial tiles in x (40 = 16 + 16 + 8: configuration 11 covers the last 8 columns with 8 x 4 x 4
+    # remainder tiles), y (22) and z (18 = 4 x 4 + 2 / 9 x 2)
     g = Geom((40, 22, 18), (-5.0, -2.75, -2.25), (5.0, 2.75, 2.25))
     u = oracle_lib.init_brill_lindquist(g, [1.0], [[0.12, -0.1, 0.05]], r_floor=0.5 * g.dx[0])
     u = oracle.add_noise(u, 1e-10, 99)
@@ -89,7 +90,7 @@ def test_per_class_table_on_a_hierarchy(gb, oracle_lib):
     # blocks of three size classes on two levels; each class gets another
     # configuration, so a level stage runs as several launches
     geoms = [Geom((16, 16, 16), (-4.0, -4.0, -4.0), (0.0, 0.0, 0.0)),
-             Geom((32, 32, 16), (0.0, -4.0, -4.0), (8.0, 4.0, 0.0)),
+             Geom((40, 32, 16), (0.0, -4.0, -4.0), (10.0, 4.0, 0.0)),
              Geom((16, 16, 16), (-4.0, 0.0, -4.0), (0.0, 4.0, 0.0)),
              Geom((48, 48, 48), (-3.0, -3.0, -3.0), (3.0, 3.0, 3.0))]
     levels = [0, 0, 0, 1]
@@ -121,7 +122,7 @@ def test_per_class_table_on_a_hierarchy(gb, oracle_lib):
 
     classes = [gb.block_stage_class(g.n) for g in geoms]
     assert len(set(classes)) == 3
-    mixed_table = [6, 5, 3, 7, 1, 2]
+    mixed_table = [6, 11, 3, 5, 1, 2]  # the 40-wide block (class 1) gets x-remainder tiles
     table = {"fp64": mixed_table, "mixed": mixed_table}
     a = run(None, gb.PRECISION_FP64)
     b = run(table, gb.PRECISION_FP64)
