@@ -45,11 +45,12 @@ struct TmaCfg {
     // instead of 16-wide tiles half outside the block
     int rem;
 };
-constexpr int NUM_TMA_CFGS = 12;
+constexpr int NUM_TMA_CFGS = 14;
 constexpr TmaCfg TMA_CFGS[NUM_TMA_CFGS] = {
     {4, 3, 0, 0, 0, 1, 1, 0}, {4, 3, 1, 1, 0, 1, 1, 0}, {2, 3, 1, 1, 0, 2, 1, 0}, {2, 2, 1, 1, 0, 2, 1, 0},
     {2, 3, 1, 0, 0, 2, 1, 0}, {2, 3, 0, 0, 1, 2, 1, 0}, {2, 3, 0, 0, 0, 3, 1, 0}, {2, 2, 1, 0, 0, 3, 1, 0},
-    {2, 3, 1, 0, 0, 2, 2, 0}, {2, 4, 0, 0, 0, 2, 2, 0}, {4, 4, 0, 0, 0, 1, 2, 0}, {2, 3, 1, 0, 0, 2, 1, 1}};
+    {2, 3, 1, 0, 0, 2, 2, 0}, {2, 4, 0, 0, 0, 2, 2, 0}, {4, 4, 0, 0, 0, 1, 2, 0}, {2, 3, 1, 0, 0, 2, 1, 1},
+    {2, 3, 0, 0, 0, 2, 1, 1}, {2, 2, 1, 0, 0, 2, 1, 1}};
 // Points of an x-remainder tile along x, and the box shape that loads it.
 constexpr int TMA_REM_X = 8;
 constexpr int TMA_REM_SHAPE = 0;
