@@ -44,13 +44,15 @@ struct TmaCfg {
     // the 128 threads all on points) loaded with the 24 x 12 x 12 box shape,
     // instead of 16-wide tiles half outside the block
     int rem;
+    int pf;  // L2 prefetches of u^n and the next tile's pointwise cells without tin (tin implies them)
 };
-constexpr int NUM_TMA_CFGS = 14;
+constexpr int NUM_TMA_CFGS = 15;
 constexpr TmaCfg TMA_CFGS[NUM_TMA_CFGS] = {
-    {4, 3, 0, 0, 0, 1, 1, 0}, {4, 3, 1, 1, 0, 1, 1, 0}, {2, 3, 1, 1, 0, 2, 1, 0}, {2, 2, 1, 1, 0, 2, 1, 0},
-    {2, 3, 1, 0, 0, 2, 1, 0}, {2, 3, 0, 0, 1, 2, 1, 0}, {2, 3, 0, 0, 0, 3, 1, 0}, {2, 2, 1, 0, 0, 3, 1, 0},
-    {2, 3, 1, 0, 0, 2, 2, 0}, {2, 4, 0, 0, 0, 2, 2, 0}, {4, 4, 0, 0, 0, 1, 2, 0}, {2, 3, 1, 0, 0, 2, 1, 1},
-    {2, 3, 0, 0, 0, 2, 1, 1}, {2, 2, 1, 0, 0, 2, 1, 1}};
+    {4, 3, 0, 0, 0, 1, 1, 0, 0}, {4, 3, 1, 1, 0, 1, 1, 0, 0}, {2, 3, 1, 1, 0, 2, 1, 0, 0},
+    {2, 2, 1, 1, 0, 2, 1, 0, 0}, {2, 3, 1, 0, 0, 2, 1, 0, 0}, {2, 3, 0, 0, 1, 2, 1, 0, 0},
+    {2, 3, 0, 0, 0, 3, 1, 0, 0}, {2, 2, 1, 0, 0, 3, 1, 0, 0}, {2, 3, 1, 0, 0, 2, 2, 0, 0},
+    {2, 4, 0, 0, 0, 2, 2, 0, 0}, {4, 4, 0, 0, 0, 1, 2, 0, 0}, {2, 3, 1, 0, 0, 2, 1, 1, 0},
+    {2, 3, 0, 0, 0, 2, 1, 1, 0}, {2, 2, 1, 0, 0, 2, 1, 1, 0}, {2, 3, 0, 0, 0, 2, 1, 1, 1}};
 // Points of an x-remainder tile along x, and the box shape that loads it.
 constexpr int TMA_REM_X = 8;
 constexpr int TMA_REM_SHAPE = 0;

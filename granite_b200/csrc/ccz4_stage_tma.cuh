@@ -17,9 +17,9 @@
 // Options of a configuration:
 //   TIN  every field's centre value is copied from the ring into a per-thread
 //        column of shared memory as it streams through, and the RK epilogue
-//        reads the stage input there instead of from global memory; the
-//        epilogue's u^n cells and the next tile's pointwise cells are
-//        prefetched into L2 at the start of each tile;
+//        reads the stage input there instead of from global memory;
+//   PF   the epilogue's u^n cells and the next tile's pointwise cells are
+//        prefetched into L2 at the start of each tile (always with TIN);
 //   HS   the 36 values of the Hessian-field loop live in a per-thread column of
 //        shared memory instead of local memory;
 //   MINB resident CTAs per SM that the register allocation is sized for
@@ -39,13 +39,14 @@ namespace granite_b200 {
 
 namespace {
 
-template <int TZ_, int NBUF_, bool TIN_, bool HS_, int MINB_, int BAR_ = 1, bool REM_ = false>
+template <int TZ_, int NBUF_, bool TIN_, bool HS_, int MINB_, int BAR_ = 1, bool REM_ = false, bool PF_ = false>
 struct TmaCfgT {
     static constexpr int TZ = TZ_, NBUF = NBUF_, BAR = BAR_;
     // a tile round's first item starts a barrier group (the round's shared push
     // boxes rely on it), and at least one item is loaded ahead
     static_assert((BAR == 1 || BAR == 2) && NV % BAR == 0 && NBUF > BAR, "barrier grouping");
     static constexpr bool TIN = TIN_, HS = HS_, REM = REM_;
+    static constexpr bool PF = TIN || PF_;  // the L2 prefetches at the start of each tile
     static constexpr int TX = 16, TY = 4, NT = TX * TY * TZ;
     static constexpr int MINB = MINB_;  // resident CTAs per SM asked of the register allocator
     static constexpr int BX = TX + 8, BY = TY + 8, BZ = TZ + 8;
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
                 pushes = A.push + pr.x;
             }
         }
-        if constexpr (C::TIN) {
+        if constexpr (C::PF) {
             // L2 prefetches: this tile's u^n (read by the epilogue; stage 1 takes
             // it from the ring) and the next tile's pointwise cells
             if (EPI == EPI_RK && A.n_sel != A.in_sel) {
@@ -419,7 +420,7 @@ struct TmaConfigOps {
     namespace granite_b200 {                                                                                         \
     using TmaCfg##K =                                                                                                \
         TmaCfgT<TMA_CFGS[K].tz, TMA_CFGS[K].nbuf, TMA_CFGS[K].tin != 0, TMA_CFGS[K].hs != 0, TMA_CFGS[K].minb,      \
-                TMA_CFGS[K].bar, TMA_CFGS[K].rem != 0>;                                                              \
+                TMA_CFGS[K].bar, TMA_CFGS[K].rem != 0, TMA_CFGS[K].pf != 0>;                                         \
     cudaError_t configure_tma_cfg##K(int nsm, int grids[3][2][2]) {                                                  \
         return TmaConfigOps<TmaCfg##K>::configure<STORE>(nsm, grids);                                                \
     }                                                                                                                \
