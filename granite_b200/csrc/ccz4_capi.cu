@@ -323,8 +323,9 @@ DevBlock make_devblock(const granite_block_desc& b, double sigma) {
 // Tiles of one block. adaptive (global-load stage kernels only): pick the tile
 // width w in {32, 16, 8} (128 / w rows) that leaves the fewest idle threads on
 // this block's x-y face, preferring the wider tile on ties (longer coalesced rows).
+// rem_mapped: the block has tensor maps of its configuration's remainder box.
 void tiles_of(int block, const granite_block_desc& b, std::vector<Tile>& out, int variant, bool adaptive = false,
-              int cfg = 0) {
+              int cfg = 0, bool rem_mapped = false) {
     int TX, TY, TZ;
     stage_tile_dims(variant, cfg, &TX, &TY, &TZ);
     int w = 0;
@@ -347,7 +348,7 @@ void tiles_of(int block, const granite_block_desc& b, std::vector<Tile>& out, in
     // multiple of 16 covers its last TMA_REM_X columns with TMA_REM_X x TY x 2 TZ
     // tiles (Tile::w = -TMA_REM_X), each after the full tiles of its rows
     const bool rem = variant == VARIANT_TMA && !adaptive && cfg >= 0 && cfg < NUM_TMA_CFGS && TMA_CFGS[cfg].rem &&
-                     b.ncells[0] % TX == TMA_REM_X;
+                     rem_mapped && b.ncells[0] % TX == TMA_REM_X;
     const int nx = rem ? b.ncells[0] - TMA_REM_X : b.ncells[0];
     for (int k = 0; k < b.ncells[2]; k += TZ)
         for (int j = 0; j < b.ncells[1]; j += TY) {
@@ -1104,18 +1105,23 @@ static int build_lists(Ctx* c) {
     int maxlev = 0;
     for (const auto& d : c->descs) maxlev = std::max(maxlev, d.level);
     // TMA variant: one tensor map per (box shape, block, slot); a block that
-    // cannot be mapped sends its whole level to the global-load kernel
+    // cannot be mapped in the tile shapes (tz = 4 and 2) sends its whole level
+    // to the global-load kernel; a block without the tz = 8 shape (less than 8
+    // cells deep) only goes without the remainder tiles of tz = 4 configurations
     const size_t nb = c->descs.size();
     std::vector<char> mapped(nb, 0);
+    std::vector<std::array<char, TMA_SHAPES>> shape_ok(nb);
     if (c->variant == VARIANT_TMA) {
         std::vector<CUtensorMap> maps(TMA_SHAPES * 3 * nb);
         for (size_t i = 0; i < nb; ++i) {
-            bool ok = true;
-            for (int sh = 0; sh < TMA_SHAPES; ++sh)
+            for (int sh = 0; sh < TMA_SHAPES; ++sh) {
+                bool ok = true;
                 for (int sl = 0; sl < 3; ++sl)
                     ok = ok && encode_block_tmap(&maps[(sh * nb + i) * 3 + sl], c->hblocks[i].buf[sl], c->hblocks[i],
                                                  TMA_SHAPE_TZ[sh]);
-            mapped[i] = ok;
+                shape_ok[i][sh] = ok;
+            }
+            mapped[i] = shape_ok[i][tma_shape_for_tz(4)] && shape_ok[i][tma_shape_for_tz(2)];
         }
         CK(upload_vec(maps, &c->d_tmaps, c->stream), "upload tensor maps");
     }
@@ -1140,7 +1146,9 @@ static int build_lists(Ctx* c) {
                 for (size_t q = 0; q < ll.blocks.size(); ++q) {
                     if (ll.block_cfg[pr][q] != cfg) continue;
                     const int t0 = (int)tiles.size();
-                    tiles_of(ll.blocks[q], c->descs[ll.blocks[q]], tiles, ll.variant, adaptive_tiles(ll.variant), cfg);
+                    const int rs = ll.variant == VARIANT_TMA ? tma_rem_shape_of(cfg) : -1;
+                    tiles_of(ll.blocks[q], c->descs[ll.blocks[q]], tiles, ll.variant, adaptive_tiles(ll.variant), cfg,
+                             rs >= 0 && shape_ok[ll.blocks[q]][rs]);
                     ll.tile_range[pr][q] = {t0, (int)tiles.size() - t0};
                 }
                 if ((int)tiles.size() > g0) ll.groups[pr].push_back({cfg, g0, (int)tiles.size() - g0});
@@ -1419,7 +1427,7 @@ static cudaError_t stage_range(Ctx* c, LevelLists& L, int cfg, int precision, co
     StageArgs a = a0;
     if (L.variant == VARIANT_TMA) {  // the tensor maps of this configuration's box shape(s)
         a.tmaps = c->d_tmaps + (size_t)tma_shape_of(cfg) * 3 * c->descs.size();
-        a.tmaps_rem = TMA_CFGS[cfg].rem ? c->d_tmaps + (size_t)TMA_REM_SHAPE * 3 * c->descs.size() : nullptr;
+        a.tmaps_rem = TMA_CFGS[cfg].rem ? c->d_tmaps + (size_t)tma_rem_shape_of(cfg) * 3 * c->descs.size() : nullptr;
     }
     if (a.tile_push) a.tile_push += first;  // indexed like the launch's tiles
     // (the TMA kernel keeps a CTA's selected tiles in shared memory: bounded count)

@@ -54,8 +54,8 @@ struct TmaCfgT {
     static constexpr unsigned BYTES = BOX * sizeof(double);  // complete_tx count of one item
     // x-remainder tiles: TMA_REM_X x TY x 2 TZ points, the same rows (BX, BY) and
     // 2 TZ + 8 planes per box, so the stencil offsets stay those of the full tiles
-    static_assert(!REM || (TZ == 2 && TMA_SHAPE_TZ[TMA_REM_SHAPE] == 2 * TZ && TMA_REM_X * TY * 2 * TZ == NT),
-                  "remainder tiles: 8 x 4 x 4 points in the tz = 4 box shape");
+    static_assert(!REM || (tma_shape_for_tz(2 * TZ) >= 0 && TMA_REM_X * TY * 2 * TZ == NT),
+                  "remainder tiles: one point per thread, loaded with the 2 TZ box shape");
     static constexpr int BOX_REM = BX * BY * (2 * TZ + 8);
     static constexpr unsigned BYTES_REM = BOX_REM * sizeof(double);
     static constexpr int SLOT = REM ? BOX_REM : BOX;  // doubles per ring slot

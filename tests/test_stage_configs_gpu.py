@@ -25,7 +25,7 @@ from test_parity_gpu import parity
 
 pytestmark = pytest.mark.gpu
 
-CONFIGS = list(range(15))
+CONFIGS = list(range(16))
 
 
 @pytest.fixture(scope="module")
