@@ -609,7 +609,7 @@ def main():
     # e2e through the C ABI with host buffers (pinned), copies inside the timed
     # region: every step uploads its input state (the workload's initial state)
     # from pinned host memory, steps, and downloads the result into a pinned
-    # buffer. E2E_CONTEXTS contexts hold the workload and take the steps in
+    # buffer. Up to E2E_CONTEXTS contexts hold the workload and take the steps in
     # turn, a three-stage pipeline: while one context steps (SMs), the next
     # one's upload and the previous one's download run (copy engines, one
     # direction each). Uploads, and downloads, are ordered across the contexts
@@ -625,7 +625,7 @@ def main():
     hosts_in = [pinned_like(b.array) for b in run.blocks]
     for (_, v), b in zip(hosts_in, run.blocks):
         v[...] = b.array
-    hosts_out = [[pinned_like(b.array) for b in run.blocks] for _ in range(E2E_CONTEXTS)]
+    hosts_out = [[pinned_like(b.array) for b in run.blocks]]  # one per context (more below)
     vin = [v for _, v in hosts_in]
     vouts = [[v for _, v in ho] for ho in hosts_out]
 
@@ -642,21 +642,28 @@ def main():
     serial_ms = max_over_ranks(torch, dist, world, (time.perf_counter() - t0) * 1000.0, f"cuda:{local}")
     serial_val = whole_job_rate(run.points_per_step, serial_steps, world, serial_ms)
 
+    # as many more contexts as the device's free memory holds (a 60 GB hierarchy
+    # fits one more at most), keeping 2 GB for graphs and scratch
+    free_bytes = torch.cuda.mem_get_info(local)[0]
+    extra = max(0, min(E2E_CONTEXTS - 1, int((free_bytes - (2 << 30)) // max(run.ev.arena_bytes(), 1))))
     ring = [run]
-    for _ in range(E2E_CONTEXTS - 1):
+    for _ in range(extra):
         r = Runner(gb, args.workload, w, prec, variant, local, args.stage_config, like=run)
         configure(r)
         r.step()  # builds its step graph
         r.ev.sync()
         ring.append(r)
+    nctx = len(ring)
+    hosts_out += [[pinned_like(b.array) for b in run.blocks] for _ in range(nctx - 1)]
+    vouts = [[v for _, v in ho] for ho in hosts_out]
     streams = [torch.cuda.ExternalStream(r.ev.stream_handle(), device=f"cuda:{local}") for r in ring]
-    e2e_steps = max(2 * E2E_CONTEXTS, min(args.steps, 16 if hier else 40))
+    e2e_steps = max(2 * nctx, min(args.steps, 16 if hier else 40))
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
     last_up = last_down = None
     for s in range(e2e_steps):
-        r, st = ring[s % E2E_CONTEXTS], streams[s % E2E_CONTEXTS]
+        r, st = ring[s % nctx], streams[s % nctx]
         r.ev.sync()  # its previous result is on the host before the buffers are reused
         if last_up is not None:
             st.wait_event(last_up)
@@ -666,7 +673,7 @@ def main():
         r.step()
         if last_down is not None:
             st.wait_event(last_down)
-        r.ev.download(None, vouts[s % E2E_CONTEXTS], wait=False)
+        r.ev.download(None, vouts[s % nctx], wait=False)
         last_down = torch.cuda.Event()
         last_down.record(st)
     for r in ring:
@@ -759,7 +766,7 @@ def main():
                 "dtype": "f32+f64" if prec == gb.PRECISION_MIXED else "f64", "data": "synthetic",
                 "config": cfg, "roofline": rl,
                 "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": run.state_bytes,
-                        "d2h_bytes_per_step": run.state_bytes, "steps": e2e_steps, "contexts": E2E_CONTEXTS,
+                        "d2h_bytes_per_step": run.state_bytes, "steps": e2e_steps, "contexts": nctx,
                         "serial": {"value": serial_val, "steps": serial_steps, "contexts": 1}},
                 "cpu_baseline": cb, "clocks": clocks, "gpu_launches": launches}
         if cmp_line:
