@@ -33,8 +33,9 @@ int stage_tile_dims(int variant, int cfg, int* tx, int* ty, int* tz);
 // loop's 36 values live in shared memory instead of local memory.
 // ws: the mixed RK kernels are warp-specialized (stencil warps feed algebra
 // warps through shared memory; ccz4_stage_ws.cuh), the FP64 ones those of
-// configuration 4. Configuration 0 is the untuned default and the only one
-// with the store (drop-in RHS) epilogue.
+// configuration 4. Configuration 0 is the only one with the store (drop-in
+// RHS) epilogue; the defaults per precision and block-size class are in
+// ccz4_capi.cu (DEFAULT_CLASS_CFG).
 struct TmaCfg {
     int tz, nbuf, tin, hs, ws;
     int minb;  // resident CTAs per SM the register allocation is sized for (__launch_bounds__)
