@@ -188,10 +188,16 @@ __global__ void __launch_bounds__(TX* TY* TZ, 2)
 
 // Per-tile precision flags: flag[ti] = 1 (FP64 algebra) when a point of tile ti
 // has chi below chi_fp64 in buffer slot `sel` (or a non-finite chi), else 0.
-__global__ void __launch_bounds__(128)
-    classify_tiles_kernel(const DevBlock* __restrict__ blocks, const Tile* __restrict__ tiles, int first, int sel,
-                          int tx, int ty, int tz, double chi_fp64, unsigned char* __restrict__ flag) {
-    const int ti = first + blockIdx.x;
+// One warp per tile, CLASSIFY_WARPS tiles per CTA (a CTA per tile made the
+// launch block-scheduling bound: ~16 k CTAs of one load per thread).
+constexpr int CLASSIFY_WARPS = 8;
+__global__ void __launch_bounds__(32 * CLASSIFY_WARPS)
+    classify_tiles_kernel(const DevBlock* __restrict__ blocks, const Tile* __restrict__ tiles, int first, int ntiles,
+                          int sel, int tx, int ty, int tz, double chi_fp64, unsigned char* __restrict__ flag) {
+    const int lane = threadIdx.x % 32;
+    const int tl = blockIdx.x * CLASSIFY_WARPS + (int)threadIdx.x / 32;
+    if (tl >= ntiles) return;  // whole warps
+    const int ti = first + tl;
     const Tile t = tiles[ti];
     const DevBlock& B = blocks[t.block];
     // global-load tiles: w x 128/w x 1; TMA x-remainder tiles (w < 0): -w x ty x 2 tz
@@ -199,13 +205,14 @@ __global__ void __launch_bounds__(128)
               d = t.w > 0 ? 1 : (t.w < 0 ? 2 * tz : tz);
     const double* chi = B.buf[sel] + (long long)CHI * B.stride;
     bool low = false;
-    for (int p = threadIdx.x; p < w * h * d; p += blockDim.x) {
+#pragma unroll 4
+    for (int p = lane; p < w * h * d; p += 32) {
         const int i = t.i0 + p % w, j = t.j0 + (p / w) % h, k = t.k0 + p / (w * h);
         if (i < B.n[0] && j < B.n[1] && k < B.n[2])
             low |= !(__ldg(chi + cell_index(B, i + NG, j + NG, k + NG)) >= chi_fp64);
     }
-    low = __syncthreads_or(low);
-    if (threadIdx.x == 0) flag[ti] = low ? 1 : 0;
+    low = __any_sync(0xffffffffu, low);
+    if (lane == 0) flag[ti] = low ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -391,7 +398,8 @@ cudaError_t launch_classify(int variant, int cfg, const DevBlock* blocks, const 
     if (ntiles <= 0) return cudaSuccess;
     int tx, ty, tz;
     if (stage_tile_dims(variant, cfg, &tx, &ty, &tz)) return cudaErrorInvalidValue;
-    classify_tiles_kernel<<<ntiles, 128, 0, stream>>>(blocks, tiles, first, sel, tx, ty, tz, chi_fp64, flag);
+    classify_tiles_kernel<<<(ntiles + CLASSIFY_WARPS - 1) / CLASSIFY_WARPS, 32 * CLASSIFY_WARPS, 0, stream>>>(
+        blocks, tiles, first, ntiles, sel, tx, ty, tz, chi_fp64, flag);
     return cudaGetLastError();
 }
 
