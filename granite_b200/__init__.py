@@ -34,7 +34,7 @@ KERNEL_STAGE, KERNEL_GHOST, KERNEL_TRANSFER, KERNEL_CONSTRAINTS = 0, 1, 2, 3
 VARIANT_GLOBAL, VARIANT_SMEM, VARIANT_GLOBAL_R168, VARIANT_GLOBAL_R128, VARIANT_TMA = 0, 1, 2, 3, 4
 VARIANT_NAMES = {"global": 0, "smem": 1, "global_r168": 2, "global_r128": 3, "tma": 4}
 # configurations of the TMA stage kernel and the block-size classes they are tuned for
-STAGE_CONFIGS = 16
+STAGE_CONFIGS = 18
 STAGE_CLASS_EDGES = (16, 24, 32, 48, 64, 96)
 
 _ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "no sm_100 device", -4: "out of memory",

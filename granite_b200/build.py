@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libgranite_ccz4.so")
 SOURCES = ["ccz4_rhs.cu", "ccz4_ghost.cu", "ccz4_constraints.cu", "ccz4_capi.cu", "ccz4_probe.cu", "ccz4_matter.cu",
-           "ccz4_psi4.cu", "ccz4_horizon.cu"] + [f"ccz4_tma_cfg{k}.cu" for k in range(16)]
+           "ccz4_psi4.cu", "ccz4_horizon.cu"] + [f"ccz4_tma_cfg{k}.cu" for k in range(18)]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xcompiler", "-fvisibility=hidden"]

@@ -42,19 +42,21 @@ struct TmaCfg {
     int bar;   // ring items per CTA barrier (1 or 2; the barrier frees that many slots)
     // x-remainder tiles: a block whose x extent leaves 8 cells after its
     // 16-wide tiles covers them with 8 x 4 x 2tz tiles (Tile::w = -8, every
-    // thread on a point) loaded with the 24 x 12 x (2tz + 8) box shape, instead
-    // of 16-wide tiles half outside the block
+    // thread on a point) instead of 16-wide tiles half outside the block;
+    // rem = 1 loads them with the 24 x 12 x (2tz + 8) box shape (ring slots
+    // sized for it), rem = 2 as two boxes of the configuration's own shape (one
+    // per half along z, two ring items; needs bar = 2)
     int rem;
     int pf;  // L2 prefetches of u^n and the next tile's pointwise cells without tin (tin implies them)
 };
-constexpr int NUM_TMA_CFGS = 16;
+constexpr int NUM_TMA_CFGS = 18;
 constexpr TmaCfg TMA_CFGS[NUM_TMA_CFGS] = {
     {4, 3, 0, 0, 0, 1, 1, 0, 0}, {4, 3, 1, 1, 0, 1, 1, 0, 0}, {2, 3, 1, 1, 0, 2, 1, 0, 0},
     {2, 2, 1, 1, 0, 2, 1, 0, 0}, {2, 3, 1, 0, 0, 2, 1, 0, 0}, {2, 3, 0, 0, 1, 2, 1, 0, 0},
     {2, 3, 0, 0, 0, 3, 1, 0, 0}, {2, 2, 1, 0, 0, 3, 1, 0, 0}, {2, 3, 1, 0, 0, 2, 2, 0, 0},
     {2, 4, 0, 0, 0, 2, 2, 0, 0}, {4, 4, 0, 0, 0, 1, 2, 0, 0}, {2, 3, 1, 0, 0, 2, 1, 1, 0},
     {2, 3, 0, 0, 0, 2, 1, 1, 0}, {2, 2, 1, 0, 0, 2, 1, 1, 0}, {2, 3, 0, 0, 0, 2, 1, 1, 1},
-    {4, 4, 0, 0, 0, 1, 2, 1, 0}};
+    {4, 4, 0, 0, 0, 1, 2, 1, 0}, {4, 4, 0, 0, 0, 1, 2, 2, 0}, {2, 4, 0, 0, 0, 2, 2, 2, 0}};
 // Points of an x-remainder tile along x.
 constexpr int TMA_REM_X = 8;
 // The box (cells incl. the 4-cell halo) one tensor-map load brings in per
@@ -68,7 +70,10 @@ constexpr int TMA_SHAPE_TZ[TMA_SHAPES] = {4, 2, 8};
 constexpr int tma_shape_for_tz(int tz) { return tz == 4 ? 0 : (tz == 2 ? 1 : (tz == 8 ? 2 : -1)); }
 constexpr int tma_shape_of(int cfg) { return tma_shape_for_tz(TMA_CFGS[cfg].tz); }
 // box shape of a configuration's x-remainder tiles (-1: none)
-constexpr int tma_rem_shape_of(int cfg) { return TMA_CFGS[cfg].rem ? tma_shape_for_tz(2 * TMA_CFGS[cfg].tz) : -1; }
+constexpr int tma_rem_shape_of(int cfg) {
+    return TMA_CFGS[cfg].rem == 1 ? tma_shape_for_tz(2 * TMA_CFGS[cfg].tz)
+                                  : (TMA_CFGS[cfg].rem == 2 ? tma_shape_of(cfg) : -1);
+}
 // Per-tile precision launches of the TMA kernel keep each CTA's selected tiles
 // in shared memory: at most TMA_SEL_CAP per CTA, i.e. ntiles <= grid x TMA_SEL_CAP.
 constexpr int TMA_SEL_CAP = 1024;

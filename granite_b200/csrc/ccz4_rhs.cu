@@ -277,6 +277,8 @@ cudaError_t configure_tma_cfg12(int, int[3][2][2]);
 cudaError_t configure_tma_cfg13(int, int[3][2][2]);
 cudaError_t configure_tma_cfg14(int, int[3][2][2]);
 cudaError_t configure_tma_cfg15(int, int[3][2][2]);
+cudaError_t configure_tma_cfg16(int, int[3][2][2]);
+cudaError_t configure_tma_cfg17(int, int[3][2][2]);
 cudaError_t launch_tma_cfg0(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
 cudaError_t launch_tma_cfg1(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
 cudaError_t launch_tma_cfg2(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
@@ -293,15 +295,18 @@ cudaError_t launch_tma_cfg12(int, int, bool, const DevBlock*, const Tile*, int, 
 cudaError_t launch_tma_cfg13(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
 cudaError_t launch_tma_cfg14(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
 cudaError_t launch_tma_cfg15(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
-static_assert(NUM_TMA_CFGS == 16, "one configure / launch pair per TMA configuration");
+cudaError_t launch_tma_cfg16(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
+cudaError_t launch_tma_cfg17(int, int, bool, const DevBlock*, const Tile*, int, const StageArgs&, cudaStream_t, int);
+static_assert(NUM_TMA_CFGS == 18, "one configure / launch pair per TMA configuration");
 static const TmaConfigure g_tma_configure[NUM_TMA_CFGS] = {
     configure_tma_cfg0, configure_tma_cfg1, configure_tma_cfg2, configure_tma_cfg3, configure_tma_cfg4, configure_tma_cfg5,
     configure_tma_cfg6, configure_tma_cfg7, configure_tma_cfg8, configure_tma_cfg9, configure_tma_cfg10,
-    configure_tma_cfg11, configure_tma_cfg12, configure_tma_cfg13, configure_tma_cfg14, configure_tma_cfg15};
+    configure_tma_cfg11, configure_tma_cfg12, configure_tma_cfg13, configure_tma_cfg14, configure_tma_cfg15,
+    configure_tma_cfg16, configure_tma_cfg17};
 static const TmaLaunch g_tma_launch[NUM_TMA_CFGS] = {
     launch_tma_cfg0, launch_tma_cfg1, launch_tma_cfg2, launch_tma_cfg3, launch_tma_cfg4, launch_tma_cfg5,
     launch_tma_cfg6, launch_tma_cfg7, launch_tma_cfg8, launch_tma_cfg9, launch_tma_cfg10, launch_tma_cfg11,
-    launch_tma_cfg12, launch_tma_cfg13, launch_tma_cfg14, launch_tma_cfg15};
+    launch_tma_cfg12, launch_tma_cfg13, launch_tma_cfg14, launch_tma_cfg15, launch_tma_cfg16, launch_tma_cfg17};
 
 // Persistent grid of each TMA configuration on each device: SMs x resident CTAs.
 constexpr int MAX_DEVICES = 64;

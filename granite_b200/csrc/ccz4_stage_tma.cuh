@@ -39,15 +39,20 @@ namespace granite_b200 {
 
 namespace {
 
-template <int TZ_, int NBUF_, bool TIN_, bool HS_, int MINB_, int BAR_ = 1, bool REM_ = false, bool PF_ = false>
+template <int TZ_, int NBUF_, bool TIN_, bool HS_, int MINB_, int BAR_ = 1, int REM_ = 0, bool PF_ = false>
 struct TmaCfgT {
     static constexpr int TZ = TZ_, NBUF = NBUF_, BAR = BAR_;
     // a tile round's first item starts a barrier group (the round's shared push
     // boxes rely on it), and at least one item is loaded ahead
     static_assert((BAR == 1 || BAR == 2) && NV % BAR == 0 && NBUF > BAR, "barrier grouping");
-    static constexpr bool TIN = TIN_, HS = HS_, REM = REM_;
+    static constexpr bool TIN = TIN_, HS = HS_;
+    // x-remainder tiles: REM, one box of the 2 TZ shape per field; REM2, two
+    // boxes of this configuration's own shape per field (one per half of the
+    // tile along z), two ring items that one barrier group frees together
+    static constexpr bool REM = REM_ == 1, REM2 = REM_ == 2;
     static constexpr bool PF = TIN || PF_;  // the L2 prefetches at the start of each tile
     static constexpr int TX = 16, TY = 4, NT = TX * TY * TZ;
+    static_assert(!REM2 || (BAR == 2 && TMA_REM_X * TY * 2 * TZ == NT), "two-box remainder tiles");
     static constexpr int MINB = MINB_;  // resident CTAs per SM asked of the register allocator
     static constexpr int BX = TX + 8, BY = TY + 8, BZ = TZ + 8;
     static constexpr int BOX = BX * BY * BZ;
@@ -152,6 +157,12 @@ struct TmaSource {
     unsigned int* err;
     int fail_q;
     int withhold;      // test switch: 1 + the item CTA 0 leaves unissued (0: none)
+    // REM2: the item stream has 2 NV items in a remainder tile's round (field
+    // FIELD_ORDER[p / 2], half p % 2), NV in the others; thread 0 keeps its issue
+    // position as a cursor (round, position, items issued)
+    int ic_round = 0, ic_pos = 0, issued = 0;
+    bool rem_round = false;  // REM2: the current round is a remainder tile
+    int half = 0;            // REM2: this thread's half of a remainder tile
 
     template <typename P>
     __device__ __forceinline__ P* hess_slots() const {
@@ -179,6 +190,25 @@ struct TmaSource {
         tma_load_box(smem_addr(ring + (size_t)s * C::SLOT), (rem ? maps_rem : maps) + (size_t)(3 * t.block + in_sel) * 128,
                      t.i0, t.j0, t.k0, FIELD_ORDER[q % NV], bar);
     }
+    // thread 0 only (REM2): issue the next item of the stream
+    __device__ __forceinline__ void issue_next() {
+        const int ti = round_tile(ic_round);
+        if (ti >= ntiles) return;  // nothing after the CTA's last tile
+        const Tile t = tiles[ti];
+        const bool rem = t.w < 0;
+        const int q = issued++;
+        const int fpos = rem ? ic_pos >> 1 : ic_pos, hf = rem ? ic_pos & 1 : 0;
+        if (++ic_pos == (rem ? 2 * NV : NV)) {
+            ++ic_round;
+            ic_pos = 0;
+        }
+        if (withhold != 0 && q == withhold - 1 && blockIdx.x == 0) return;  // test switch: never issued
+        const int s = q % C::NBUF;
+        const unsigned bar = bar0 + 8u * s;
+        mbar_expect_tx(bar, C::BYTES);
+        tma_load_box(smem_addr(ring + (size_t)s * C::SLOT), maps + (size_t)(3 * t.block + in_sel) * 128, t.i0, t.j0,
+                     t.k0 + hf * C::TZ, FIELD_ORDER[fpos], bar);
+    }
     __device__ __forceinline__ void wait(int q) {
         if (failed) return;
         const unsigned bar = bar0 + 8u * (q % C::NBUF), parity = (q / C::NBUF) & 1;
@@ -199,17 +229,32 @@ struct TmaSource {
     // which the next BAR loads overwrite).
     template <bool HESS, bool EXACT, typename P>
     __device__ __forceinline__ FieldDer<P> der(int v, const double beta[3], P w) {
-        if (next % C::BAR == 0) {
-            __syncthreads();
-            if (threadIdx.x == 0 && !failed)
+        int q = next;
+        if constexpr (C::REM2) {
+            // a remainder tile's field is two items (one per half): its der()
+            // always starts a barrier group and consumes both
+            if (next % 2 == 0) {
+                __syncthreads();
+                if (threadIdx.x == 0 && !failed) {
+                    issue_next();
+                    issue_next();
+                }
+            }
+            q = next + (rem_round ? half : 0);
+            next += rem_round ? 2 : 1;
+        } else {
+            if (next % C::BAR == 0) {
+                __syncthreads();
+                if (threadIdx.x == 0 && !failed)
 #pragma unroll
-                for (int j = C::NBUF - C::BAR; j < C::NBUF; ++j) issue(next + j);
+                    for (int j = C::NBUF - C::BAR; j < C::NBUF; ++j) issue(next + j);
+            }
+            ++next;
         }
-        wait(next);
-        const double* box = ring + (size_t)(next % C::NBUF) * C::SLOT + lin;
+        wait(q);
+        const double* box = ring + (size_t)(q % C::NBUF) * C::SLOT + lin;
         if constexpr (C::TIN) tin[v * NT] = box[0];
         const SharedLoad L{box};
-        ++next;
         const long long off[3] = {1, C::BX, C::BX * C::BY};
         return field_der_l<P, HESS, true, SharedLoad, EXACT>(*B, L, off, beta, w);
     }
@@ -271,7 +316,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     // this thread's point within a tile: 16 x 4 x TZ, or TMA_REM_X x 4 x 2 TZ
     // for an x-remainder tile (the box rows are the same, so is the stencil code)
     auto local = [&](const Tile& t, int& px, int& py, int& pz) {
-        if (C::REM && t.w < 0) {
+        if ((C::REM || C::REM2) && t.w < 0) {
             px = tid % TMA_REM_X;
             py = (tid / TMA_REM_X) % C::TY;
             pz = tid / (TMA_REM_X * C::TY);
@@ -286,8 +331,12 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     TmaSource<C, SEL> S{blocks, tiles, static_cast<const unsigned char*>(A.tmaps),
                         static_cast<const unsigned char*>(A.tmaps_rem), ntiles, A.in_sel, ring, bar0,
                         tin, hs, nullptr, 0, 0, false, A.errflag, 0, A.test_withhold};
-    if (tid == 0)
-        for (int q = 0; q < C::NBUF - C::BAR; ++q) S.issue(q);
+    if (tid == 0) {
+        if constexpr (C::REM2)
+            for (int q = 0; q < C::NBUF - C::BAR; ++q) S.issue_next();
+        else
+            for (int q = 0; q < C::NBUF - C::BAR; ++q) S.issue(q);
+    }
     for (int r = 0;; ++r) {
         const int ti = S.round_tile(r);
         if (ti >= ntiles) break;
@@ -296,7 +345,14 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
         S.B = &B;
         int lx, ly, lz;
         local(t, lx, ly, lz);
-        S.lin = (lx + 4) + C::BX * ((ly + 4) + C::BY * (lz + 4));
+        if constexpr (C::REM2) {
+            // a remainder tile's two halves along z each have their own box
+            S.rem_round = t.w < 0;
+            S.half = S.rem_round ? lz / C::TZ : 0;
+            S.lin = (lx + 4) + C::BX * ((ly + 4) + C::BY * (lz - S.half * C::TZ + 4));
+        } else {
+            S.lin = (lx + 4) + C::BX * ((ly + 4) + C::BY * (lz + 4));
+        }
         const int i = t.i0 + lx, j = t.j0 + ly, k = t.k0 + lz;
         const bool valid = i < B.n[0] && j < B.n[1] && k < B.n[2];
         // pointwise loads of threads outside the block use a valid cell; their results are dropped
@@ -349,10 +405,19 @@ __global__ void __launch_bounds__(C::NT, C::MINB)
     // CTA's shared memory outlives it.
     if (S.failed && tid == 0) {
         const int f = S.fail_q;
-        for (int q = f + 1; q < f - f % C::BAR + C::NBUF; ++q) {
-            if (S.round_tile(q / NV) >= ntiles) continue;
-            S.failed = false;
-            S.wait(q);
+        if constexpr (C::REM2) {
+            // the cursor counted every item issued (one the test switch withheld
+            // included: its wait runs out as that of item f did)
+            for (int q = f + 1; q < S.issued; ++q) {
+                S.failed = false;
+                S.wait(q);
+            }
+        } else {
+            for (int q = f + 1; q < f - f % C::BAR + C::NBUF; ++q) {
+                if (S.round_tile(q / NV) >= ntiles) continue;
+                S.failed = false;
+                S.wait(q);
+            }
         }
     }
 }
@@ -420,7 +485,7 @@ struct TmaConfigOps {
     namespace granite_b200 {                                                                                         \
     using TmaCfg##K =                                                                                                \
         TmaCfgT<TMA_CFGS[K].tz, TMA_CFGS[K].nbuf, TMA_CFGS[K].tin != 0, TMA_CFGS[K].hs != 0, TMA_CFGS[K].minb,      \
-                TMA_CFGS[K].bar, TMA_CFGS[K].rem != 0, TMA_CFGS[K].pf != 0>;                                         \
+                TMA_CFGS[K].bar, TMA_CFGS[K].rem, TMA_CFGS[K].pf != 0>;                                              \
     cudaError_t configure_tma_cfg##K(int nsm, int grids[3][2][2]) {                                                  \
         return TmaConfigOps<TmaCfg##K>::configure<STORE>(nsm, grids);                                                \
     }                                                                                                                \

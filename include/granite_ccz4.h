@@ -405,7 +405,7 @@ GRANITE_API int granite_ccz4_get_kernel_variant(const void* ctx, int* variant);
  * writes a table a caller can apply). A level's blocks of different
  * configurations run as one launch per configuration. Set before commit.
  * All configurations compute identical FP64 results. */
-#define GRANITE_STAGE_CONFIGS 16
+#define GRANITE_STAGE_CONFIGS 18
 #define GRANITE_STAGE_CLASSES 6
 #define GRANITE_STAGE_CLASS_EDGES 16, 24, 32, 48, 64, 96
 /* cls: class index (0 .. GRANITE_STAGE_CLASSES - 1) or -1 for every class;

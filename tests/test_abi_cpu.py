@@ -256,9 +256,10 @@ def test_stage_configs_and_classes_without_a_device():
             assert not info["shared_hessian"] and 3 * (dyn + 7680) <= 228 * 1024, (k, info)
     assert [gb.stage_config_info(k)["ctas_per_sm"] for k in (6, 7)] == [3, 3]
     assert [gb.stage_config_info(k)["items_per_barrier"] for k in range(gb.STAGE_CONFIGS)] == \
-        [1] * 8 + [2] * 3 + [1] * 4 + [2]
+        [1] * 8 + [2] * 3 + [1] * 4 + [2] * 3
     rem = [k for k in range(gb.STAGE_CONFIGS) if gb.stage_config_info(k)["x_remainder_tiles"]]
-    assert rem == [11, 12, 13, 14, 15] and [gb.stage_config_info(k)["tile"][2] for k in rem] == [2, 2, 2, 2, 4]
+    assert rem == [11, 12, 13, 14, 15, 16, 17]
+    assert [gb.stage_config_info(k)["tile"][2] for k in rem] == [2, 2, 2, 2, 4, 4, 2]
     with pytest.raises(gb.GraniteError):
         gb.stage_config_info(gb.STAGE_CONFIGS)
     assert [gb.block_stage_class((e, e, e)) for e in gb.STAGE_CLASS_EDGES] == list(range(6))

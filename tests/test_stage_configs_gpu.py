@@ -25,7 +25,7 @@ from test_parity_gpu import parity
 
 pytestmark = pytest.mark.gpu
 
-CONFIGS = list(range(16))
+CONFIGS = list(range(18))
 
 
 @pytest.fixture(scope="module")
