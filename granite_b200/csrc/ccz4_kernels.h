@@ -77,8 +77,9 @@ constexpr int tma_rem_shape_of(int cfg) {
 // Per-tile precision launches of the TMA kernel keep each CTA's selected tiles
 // in shared memory: at most TMA_SEL_CAP per CTA, i.e. ntiles <= grid x TMA_SEL_CAP.
 constexpr int TMA_SEL_CAP = 1024;
-// Grid of the FP64 pass of the per-tile precision, in resident grids.
-constexpr int TMA_FP64_SPREAD = 4;
+// Grid of the FP64 pass of the per-tile precision, in resident grids (on the
+// bench hierarchy 1: 76 us per level-stage, 4: 63 us, 8: 55 us).
+constexpr int TMA_FP64_SPREAD = 8;
 // The resident grid of a TMA configuration's per-tile precision passes on the
 // current device, the smaller of the two (0 before configure_stage_kernels).
 int tma_grid(int cfg);
