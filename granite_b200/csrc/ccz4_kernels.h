@@ -78,7 +78,8 @@ constexpr int tma_rem_shape_of(int cfg) {
 // in shared memory: at most TMA_SEL_CAP per CTA, i.e. ntiles <= grid x TMA_SEL_CAP.
 constexpr int TMA_SEL_CAP = 1024;
 // Grid of the FP64 pass of the per-tile precision, in resident grids (on the
-// bench hierarchy 1: 76 us per level-stage, 4: 63 us, 8: 55 us).
+// bench hierarchy 1: 76 us per level-stage, 4: 63 us, 8: 55 us, 16: 61 us, the
+// scans of the CTAs without a selected tile outweighing the spread).
 constexpr int TMA_FP64_SPREAD = 8;
 // The resident grid of a TMA configuration's per-tile precision passes on the
 // current device, the smaller of the two (0 before configure_stage_kernels).
